@@ -1,0 +1,307 @@
+#!/usr/bin/env python
+"""Benchmark of the MDFT engine: solutes/s converged at 64^3, mmax 3.
+
+Workload (one "step" = one solute solved end to end): a seeded 24-site neutral
+solute (random walk, 1.4-1.6 A bonds inside 6 A, sigma U[2.5,3.8], eps
+U[0.2,1.0], q ~ N(0,0.3) shifted to 0) in SPC/E-like 3-site water, 64^3 grid,
+32 A box, mmax 3, synthetic c(k); vext (LJ + Poisson) -> guess_density ->
+L-BFGS (m=5, stop at max|df| <= 1e-6 or an F decrease <= 1e-3) -> pressure
+correction -> dG.  Synthetic inputs stand in for the reference's data.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N>1 runs N independent replicas (each rank solves its own solutes; no
+collective on the data path, only a barrier and a max of the timings).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "mdft-dev_general_b200")]
+
+METRIC = "solutes/s to |ΔG−FP64|≤0.1 kJ/mol at 64³ mmax3: learned+mixed vs plain FP64"
+UNIT = "solutes/s"
+N_GRID, BOX, MMAX, NSITE = 64, 32.0, 3, 24
+RVDW = 10.0
+CK_SEED = 20260001
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel (FP64 path),
+# from the ncu captures summarised in profiles/ (None until captured for this kernel)
+NCU_TRAFFIC_BYTES = {}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="small grid smoke run (not a bench number)")
+    return ap.parse_args()
+
+
+def ck_file(mmax, kmax=12.0):
+    from mdft_b200 import synth
+    d = os.path.join(tempfile.gettempdir(), "mdft_b200_bench")
+    os.makedirs(d, exist_ok=True)
+    p = os.path.join(d, "ck_m%d_s%d_k%g.txt" % (mmax, CK_SEED, kmax))
+    if not os.path.exists(p):
+        tmp = p + ".%d" % os.getpid()
+        synth.make_ck_file(tmp, mmax, seed=CK_SEED, kmax=kmax, dk=0.01)
+        os.replace(tmp, p)
+    return p
+
+
+def solute(seed, box):
+    from mdft_b200 import synth
+    s = synth.random_walk_solute(NSITE, seed=seed)
+    s.xyz = synth.center_solute(s.xyz, (box,) * 3)
+    return s
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(MEASURED_PEAKS) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def stage_bytes(N, no, np_):
+    """Algorithmic bytes per evaluation of each stage (FP64)."""
+    c = 16
+    return {"project": N * (no * 8 + np_ * c), "fft_forward": 2 * np_ * N * c, "oz": 2 * np_ * N * c,
+            "fft_inverse": 2 * np_ * N * c, "gather": N * (np_ * c + 3 * no * 8)}
+
+
+def cpu_oracle_eval_seconds(n, box, mmax, ck, nevals, threads):
+    """Time nevals oracle evaluations of the workload on the host cores."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    from mdft_b200 import synth
+    sv = synth.Solvent()
+    o = O.Oracle(n, box, mmax, ck, sv.kT, sv.n0)
+    s = solute(1000, box)
+    o.compute_vext(s, sv, rvdw=RVDW)
+    xi = o.guess_density()
+    o.energy_grad(xi)  # first call
+    t0 = time.perf_counter()
+    for _ in range(nevals):
+        o.energy_grad(xi)
+    return (time.perf_counter() - t0) / nevals
+
+
+def reference_arm(args, rank, world):
+    """CPU implementation of the path on the host cores (the C restatement; the
+    Fortran reference cannot be compiled here)."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    ck = ck_file(MMAX)
+    evals_per_solve = EVALS_PER_SOLVE_FP64
+    times = []
+    for i in range(args.warmup + args.steps):
+        t = cpu_oracle_eval_seconds(N_GRID, BOX, MMAX, ck, 1, threads)
+        if i >= args.warmup:
+            times.append(t)
+    t_eval = float(np.mean(times))
+    v = 1.0 / (t_eval * evals_per_solve)
+    sample = ("one FP64 energy_and_gradient per step at 64^3 mmax3 (%d threads), x %d evaluations per solve "
+              "(count of the FP64 GPU solve of the same workload)" % (threads, evals_per_solve))
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_eval * evals_per_solve * 1e3,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": {"workload": "64^3 grid, 32 A box, mmax 3, 24-site solute, synthetic c(k)",
+                                                      "form": "CPU FP64 restatement (oracle), OpenMP"},
+                      "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+                      "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# evaluations per FP64 solve of the bench workload (updated from the GPU run; used only
+# to scale the CPU per-evaluation time to solutes/s)
+EVALS_PER_SOLVE_FP64 = 60
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    import torch
+    import torch.distributed as dist
+    from mdft_b200 import Engine, synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    n, box = (N_GRID, BOX) if not args.quick else (32, 16.0)
+    rvdw = RVDW if not args.quick else 7.9
+    ck = ck_file(MMAX)
+    sv = synth.Solvent()
+    eng = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    sols = [solute(10_000 * rank + i, box) for i in range(args.warmup + args.steps)]
+    opts = dict(m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=2000)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- value: solute in, dG out; density stays in HBM ----
+    results = []
+    for i in range(args.warmup):
+        results.append(eng.solve(sols[i], sv, rvdw=rvdw, **opts))
+    l0 = eng.launch_count
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for i in range(args.warmup, args.warmup + args.steps):
+            results.append(eng.solve(sols[i], sv, rvdw=rvdw, **opts))
+        ev1.record(stream)
+        barrier()
+    launches = eng.launch_count - l0
+    t_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    value = world * args.steps / (t_ms / 1e3)
+    timed = results[args.warmup:]
+    evals = [r["evaluations"] for r in timed]
+
+    # ---- e2e: the same call with the converged density returned to pinned host memory ----
+    xi_pinned = torch.empty(int(np.prod(eng.shape)), dtype=torch.float64, pin_memory=True)
+    xi_host = xi_pinned.numpy()
+    for i in range(min(2, args.warmup)):
+        eng.solve(sols[i], sv, rvdw=rvdw, xi_out=xi_host, **opts)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.warmup, args.warmup + args.steps):
+        eng.solve(sols[i], sv, rvdw=rvdw, xi_out=xi_host, **opts)
+    e1.record(stream)
+    barrier()
+    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / (float(te.item()) / 1e3)
+    s0 = sols[0]
+    h2d = 8 * (4 * s0.nsite + 4 * 3 * 2)  # solute q, sig, eps, xyz + solvent sites
+    d2h = xi_host.nbytes + 8 * 6
+
+    # ---- roofline of the dominant stage: per-stage CUDA events over evaluations at a converged density ----
+    xi_ref = xi_host.reshape(eng.shape).copy()
+    eng.set_timing(True)
+    for _ in range(5):
+        eng.energy_and_gradient(xi_ref)
+    st, cnt = eng.stage_times()
+    eng.set_timing(False)
+    per = {k: v / cnt for k, v in st.items()}
+    sb = stage_bytes(n ** 3, eng.no, eng.np)
+    dom = max(per, key=per.get)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = sb[dom] / (per[dom] * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC_BYTES.get(dom)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_kind, "stage_ms": per,
+            "algorithmic_bytes": sb[dom]}
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and not args.quick:
+            threads = os.cpu_count() or 1
+            te_cpu = cpu_oracle_eval_seconds(n, box, MMAX, ck, 2, threads)
+            epsolve = float(np.mean(evals))
+            cpu = {"value": 1.0 / (te_cpu * epsolve), "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": "2 FP64 evaluations of the workload on the host (oracle, %d OpenMP threads) x %.1f "
+                             "evaluations per solve (the GPU FP64 solves' mean)" % (threads, epsolve)}
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "%d^3 grid, %g A box, mmax %d, %d-site random-walk solute per step, synthetic c(k)"
+                                       % (n, box, MMAX, NSITE),
+                           "form": "plain FP64 (vext + guess + L-BFGS m=5 + pressure correction)",
+                           "stop": "max|df|<=1e-6 or F decrease<=1e-3", "l2": "inputs larger than L2 (176 MB per field)",
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "evaluations_per_solve": evals, "dG": [r["dG"] for r in timed],
+                           "dG_error_vs_fp64": 0.0},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

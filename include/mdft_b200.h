@@ -1,0 +1,183 @@
+/*
+ * mdft_b200.h -- C-ABI of the B200 MDFT energy-and-gradient engine.
+ *
+ * The engine replaces, behind plain pointers and sizes, the hot path of the
+ * Fortran program dborgis/mdft-dev_general:
+ *
+ *   subroutine energy_and_gradient(f, df)      src/module_energy_and_gradient.f90:36
+ *   procedure pointer excess_energy(ff, df)    src/module_proc_ptrs.f90:3-21
+ *
+ * and the set-up and callers those need (vext, guess_density, the L-BFGS
+ * loop of energy_minimization, pressure_correction).  A Fortran host binds
+ * these entry points with ISO_C_BINDING; the binding stubs are listed in
+ * INTEGRATION.md.
+ *
+ * Layout: every per-orientation field (xi, vext, df) is the reference's
+ * Fortran array (no, nx, ny, nz) with io fastest, i.e. the C index
+ * ((iz*ny + iy)*nx + ix)*no + io.  Units follow the reference: Angstrom,
+ * kJ/mol, molecules/Angstrom^3.  `df` is dF/dxi divided by the volume
+ * element dv, exactly as the reference returns it.
+ *
+ * Errors: every entry point returns 0 on success and a negative MDFT_E_*
+ * code on failure; mdft_last_error() gives the message of the last failure
+ * on the calling thread.  Nothing aborts the process.
+ *
+ * Threading: one host thread per handle; each handle owns one CUDA stream
+ * and all of its device memory.  Handles are independent.
+ */
+#ifndef MDFT_B200_H
+#define MDFT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDFT_OK 0
+#define MDFT_E_ARG (-1)     /* invalid argument or size                        */
+#define MDFT_E_IO (-2)      /* c(k) file missing or malformed                   */
+#define MDFT_E_CUDA (-3)    /* CUDA runtime error (message has the CUDA string) */
+#define MDFT_E_NUMERIC (-4) /* NaN/Inf in inputs or outputs                     */
+#define MDFT_E_STATE (-5)   /* call order (e.g. no vext yet)                    */
+#define MDFT_E_NOMEM (-6)   /* device allocation failed                         */
+
+/* Arithmetic of the excess-term pipeline. */
+#define MDFT_PREC_FP64 0  /* every stage in FP64 (parity path)                          */
+#define MDFT_PREC_MIXED 1 /* FP32 FFT + OZ, split-BF16 angular transforms, FP64 sums   */
+
+typedef struct mdft_handle mdft_handle;
+
+/* System description: grid (src/module_grid.f90:51-212), solvent and thermo
+ * (src/module_solvent.f90:209-226, src/module_thermo.f90:56-66), c(k) file
+ * (src/module_read_c_luc.f90:6-124). */
+typedef struct mdft_desc {
+    int nx, ny, nz;         /* grid nodes (boxnod); even                          */
+    double lx, ly, lz;      /* box lengths (boxlen), Angstrom                     */
+    int mmax;               /* angular order, 0..5                               */
+    int mrso;               /* molrotsymorder of the solvent (2 for water)       */
+    double temperature;     /* K                                                 */
+    double n0;              /* bulk number density, molecules/Angstrom^3         */
+    const char *ck_path;    /* c^{mn}_{mu nu khi}(q) table in Luc's file format  */
+    int precision;          /* MDFT_PREC_*                                       */
+    int device;             /* CUDA device ordinal                               */
+} mdft_desc;
+
+/* Sizes derived from the description (filled by mdft_get_sizes). */
+typedef struct mdft_sizes {
+    int ntheta, nphi, npsi; /* angular grid                                       */
+    int no;                 /* orientations  = ntheta*nphi*npsi                  */
+    int np;                 /* projections   = sum_m (2m+1)(m/mrso+1)            */
+    int ncoef;              /* c(k) coefficients used per k                      */
+    int nq;                 /* c(k) rows used                                    */
+    double dv;              /* volume element, Angstrom^3                        */
+    double rho0;            /* n0 / (8 pi^2 / mrso)                              */
+    double kT;              /* kJ/mol                                            */
+    double dq;              /* c(k) abscissa step                                */
+} mdft_sizes;
+
+/* Create / destroy: replaces init_simu's grid, thermo, c(k) and FFT set-up
+ * (src/module_init_simu.f90:24-36, src/module_energy_cproj_mrso.f90:151-267,362-431). */
+int mdft_create(const mdft_desc *desc, mdft_handle **out);
+int mdft_destroy(mdft_handle *h);
+const char *mdft_last_error(void);
+int mdft_get_sizes(const mdft_handle *h, mdft_sizes *out);
+
+/* Stream of the handle (a cudaStream_t); every device call runs on it. */
+int mdft_get_stream(const mdft_handle *h, void **stream);
+
+/* Quadrature weights w(io) (src/module_grid.f90:116-139), host buffer of no doubles. */
+int mdft_get_weights(const mdft_handle *h, double *w);
+
+/* External potential vext(no,nx,ny,nz), host buffer: replaces the module state
+ * solvent(1)%vext that energy_and_gradient reads (src/module_vext.f90:14-115). */
+int mdft_set_vext(mdft_handle *h, const double *vext_host);
+int mdft_get_vext(const mdft_handle *h, double *vext_host);
+
+/* Constant added to F: the charged-solute corrections of
+ * src/module_energy_and_gradient.f90:191-204,281-344 (0 for a neutral solute). */
+int mdft_set_constant_correction(mdft_handle *h, double c);
+
+/* energy_and_gradient(f, df): src/module_energy_and_gradient.f90:36-240.
+ * xi, df: host arrays of no*nx*ny*nz doubles; df may be NULL (energy only).
+ * terms (may be NULL) receives {F_id, F_ext, F_exc, constant correction}. */
+int mdft_energy_and_gradient(mdft_handle *h, const double *xi, double *f, double *df, double *terms);
+
+/* Same with device pointers (on the handle's stream); d_df may be NULL. */
+int mdft_energy_and_gradient_device(mdft_handle *h, const double *d_xi, double *d_df, double *f, double *terms);
+
+/* excess_energy(ff, df): the procedure-pointer seam bound to energy_cproj_mrso
+ * (src/module_proc_ptrs.f90:3-21, src/module_energy_cproj_mrso.f90:61-782).
+ * df (may be NULL) is ACCUMULATED into, as the reference does. */
+int mdft_excess_energy(mdft_handle *h, const double *xi, double *fexc, double *df);
+
+/* External potential from a solute (src/module_vext.f90:14-115,600-669):
+ * Lennard-Jones (src/module_lennardjones.f90:9-226) plus the Poisson-solved
+ * electrostatics (src/module_fastpoissonsolver.f90:121-288,
+ * src/module_solvent.f90:367-438), clipped at qfact/2.  Solute sites are used
+ * as given (callers apply mv_solute_to_center first, src/module_solute.f90:146-187).
+ * The result becomes the handle's vext; lj_tail receives LJ_energy_correction. */
+int mdft_compute_vext(mdft_handle *h, int nsite, const double *q, const double *sig, const double *eps,
+                      const double *xyz, int nsolvsite, const double *sq, const double *ssig,
+                      const double *seps, const double *sxyz, double rvdw, double *lj_tail);
+
+/* guess_density (src/module_density.f90:267-284) into a host xi. */
+int mdft_guess_density(const mdft_handle *h, double *xi);
+
+/* Minimiser settings and result for mdft_minimize. */
+typedef struct mdft_minimize_opts {
+    int m;           /* L-BFGS history (lbfgsb%m)                                 */
+    double pgtol;    /* stop when max|df| <= pgtol (lbfgsb%pgtol)                  */
+    double ftol_abs; /* stop when f_old - f <= ftol_abs (factr*epsmch)             */
+    int itermax;     /* maximum iterations (maximum_iteration_nbr)                 */
+    int precision;   /* MDFT_PREC_* of the evaluations used by this solve          */
+} mdft_minimize_opts;
+
+typedef struct mdft_minimize_result {
+    double f;        /* functional at the returned xi                             */
+    double pgnorm;   /* max|df| at the returned xi                                */
+    int iterations;  /* L-BFGS iterations                                        */
+    int evaluations; /* energy_and_gradient calls                                 */
+    int status;      /* 0 pgtol, 1 f-reduction, 2 line-search failure, 3 itermax   */
+} mdft_minimize_result;
+
+/* minimization_using_lbfgs (src/energy_minimization.f90:232-290) with the
+ * unconstrained L-BFGS-B of src/module_lbfgs_nocedal_mdft.f90:136-534, run on
+ * the device: xi is read from and written to the host buffer. */
+int mdft_minimize(mdft_handle *h, double *xi, const mdft_minimize_opts *opts, mdft_minimize_result *res);
+
+/* Device-pointer variants (on the handle's stream): d_xi is a device array of
+ * no*nx*ny*nz doubles, read and overwritten. */
+int mdft_guess_density_device(mdft_handle *h, double *d_xi);
+int mdft_minimize_device(mdft_handle *h, double *d_xi, const mdft_minimize_opts *opts, mdft_minimize_result *res);
+
+/* pressure_correction (src/module_pressure_correction.f90:7-156):
+ * out = {dG_SFE, PMV correction, P_bulk, deltaN} for the density xi (host)
+ * whose functional value is ftot; lj_tail as returned by mdft_compute_vext. */
+int mdft_pressure_correction(mdft_handle *h, const double *xi, double ftot, double lj_tail, double *out);
+
+/* One solute, end to end, as main.f90 runs it (src/main.f90:20-40): init_vext,
+ * guess_density, the L-BFGS minimisation and pressure_correction.  Solute and
+ * solvent sites are host arrays as in mdft_compute_vext; charged solutes get
+ * the constant corrections of src/module_energy_and_gradient.f90:281-344 from
+ * eps_r and the solvent quadrupole trace.  xi_out (host, may be NULL) receives
+ * the converged density; out = {dG_SFE, F at the minimum, PMV correction,
+ * LJ tail, P_bulk, deltaN}. */
+int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, const double *eps, const double *xyz,
+               int nsolvsite, const double *sq, const double *ssig, const double *seps, const double *sxyz, double rvdw,
+               double eps_r, const mdft_minimize_opts *opts, double *xi_out, double *out, mdft_minimize_result *res);
+
+int mdft_pressure_correction_device(mdft_handle *h, const double *d_xi, double ftot, double lj_tail, double *out);
+
+/* Per-stage device time (ms) of the last evaluations, when timing is on:
+ * stage order {project, fft_forward, oz, fft_inverse, gather}; count = calls. */
+int mdft_set_timing(mdft_handle *h, int on);
+int mdft_get_stage_times(const mdft_handle *h, double *ms5, int *count);
+
+/* Number of kernels this handle has launched since creation. */
+int mdft_get_launch_count(const mdft_handle *h, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDFT_B200_H */

@@ -1,0 +1,481 @@
+// C-ABI of the B200 MDFT engine (declared in include/mdft_b200.h).
+#include "../../include/mdft_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "common.cuh"
+#include "setup_host.cuh"
+#include "k_angular.cuh"
+#include "k_fft.cuh"
+#include "k_oz.cuh"
+#include "k_vec.cuh"
+#include "k_vext.cuh"
+
+namespace mdft {
+
+static thread_local std::string g_error;
+void set_error(const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+}
+const char *last_error() { return g_error.c_str(); }
+
+constexpr double kBoltz = 1.3806488e-23;  // src/module_constants.f90:26
+constexpr double kNavo = 6.02214129e23;   // src/module_constants.f90:24
+
+enum Stage { ST_PROJECT = 0, ST_FFT_FWD, ST_OZ, ST_FFT_INV, ST_GATHER, ST_COUNT };
+
+struct FftAxis {
+    FftAxisArgs args;
+    int grid;
+    size_t smem;
+    const void *tw;  // device twiddles (double2 or float2) of this length
+};
+
+}  // namespace mdft
+
+using namespace mdft;
+
+struct mdft_handle {
+    Grid g;
+    CTable ct;
+    int precision = MDFT_PREC_FP64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double const_corr = 0.0;
+    bool have_vext = false;
+    // device state
+    DevBuf<double> xi, vext, df, w, A, B, partial, sums;
+    DevBuf<double2> planes, ctab;
+    DevBuf<double2> tw64[3];
+    double *h_sums = nullptr;  // pinned {F_id, F_ext, sum_exc}
+    int bm_project = 64, bm_gather = 64;
+    long long nblk_project = 0, nblk_gather = 0;
+    FftAxis fft[3];
+    OzArgs oz{};
+    int oz_grid = 0;
+    size_t oz_smem = 0;
+    // timing
+    bool timing = false;
+    cudaEvent_t ev[ST_COUNT + 1] = {};
+    double stage_ms[ST_COUNT] = {0};
+    int stage_count = 0;
+    long long launches = 0;  // kernels launched by this handle
+    // vector reductions
+    DevBuf<double> vpart, vsc;
+    double *h_vsc = nullptr;
+    // minimiser work (allocated on first use)
+    LbfgsState lb;
+};
+
+namespace {
+
+int check_cuda(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return MDFT_E_CUDA;
+    }
+    return 0;
+}
+
+int alloc_check(cudaError_t e, const char *what, size_t bytes) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        set_error("device allocation of %zu bytes for %s failed", bytes, what);
+        return MDFT_E_NOMEM;
+    }
+    return check_cuda(e, what);
+}
+
+int upload_twiddles(DevBuf<double2> &buf, int n) {
+    std::vector<double2> h(n);
+    for (int t = 0; t < n; ++t) {
+        long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)n;
+        h[t] = make_double2((double)cosl(ang), (double)sinl(ang));
+    }
+    int rc = alloc_check(buf.alloc(n), "fft twiddles", n * sizeof(double2));
+    if (rc) return rc;
+    return check_cuda(cudaMemcpy(buf.p, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice), "twiddle upload");
+}
+
+int pick_tl(long long lines_divisor, int n) {
+    int best = 1;
+    const int cands[] = {32, 16, 8, 4, 2, 1};
+    for (int c : cands) {
+        if (lines_divisor % c) continue;
+        if (c == 32 && n > 32) continue;
+        best = c;
+        break;
+    }
+    return best;
+}
+
+int setup_fft(mdft_handle *h) {
+    const Grid &g = h->g;
+    const int dims[3] = {g.nx, g.ny, g.nz};
+    for (int ax = 0; ax < 3; ++ax) {
+        FftAxis &F = h->fft[ax];
+        F.args.axis = ax;
+        F.args.nx = g.nx;
+        F.args.ny = g.ny;
+        F.args.nz = g.nz;
+        F.args.nplanes = g.np;
+        if (!make_plan1d(dims[ax], F.args.plan)) {
+            set_error("grid size %d is not of the form 2^a 3^b", dims[ax]);
+            return MDFT_E_ARG;
+        }
+        long long lines_div = (ax == 0) ? (long long)g.np * g.ny * g.nz : g.nx;
+        F.args.TL = pick_tl(lines_div, dims[ax]);
+        long long nlines = (long long)g.np * g.N / dims[ax];
+        F.grid = (int)(nlines / F.args.TL);
+        F.smem = fft_smem_bytes<double>(dims[ax], F.args.TL);
+        int rc = upload_twiddles(h->tw64[ax], dims[ax]);
+        if (rc) return rc;
+        F.tw = h->tw64[ax].p;
+    }
+    return 0;
+}
+
+int launch_fft(mdft_handle *h, int sign) {
+    for (int ax = 0; ax < 3; ++ax) {
+        FftAxis &F = h->fft[ax];
+        F.args.sign = sign;
+        k_fft_axis<double><<<F.grid, kFftThreads, F.smem, h->stream>>>(h->planes.p, (const double2 *)F.tw, F.args);
+    }
+    return check_cuda(cudaGetLastError(), "fft launch");
+}
+
+void stage_mark(mdft_handle *h, int i) {
+    if (h->timing) cudaEventRecord(h->ev[i], h->stream);
+}
+
+// The excess-term pipeline plus (optionally) the ideal/external term on device
+// arrays; leaves {F_id, F_ext, sum_exc} in h->sums.
+int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode) {
+    const Grid &g = h->g;
+    stage_mark(h, 0);
+    AngularArgs aa{g.N, g.no, g.np, g.rho0};
+    if (h->bm_project == 64)
+        k_project_f64<64><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes(64, g.no), h->stream>>>(d_xi, h->A.p, h->planes.p, aa);
+    else
+        k_project_f64<32><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes(32, g.no), h->stream>>>(d_xi, h->A.p, h->planes.p, aa);
+    int rc = check_cuda(cudaGetLastError(), "project launch");
+    if (rc) return rc;
+    stage_mark(h, 1);
+    if ((rc = launch_fft(h, +1))) return rc;
+    stage_mark(h, 2);
+    k_oz_f64<<<h->oz_grid, 256, h->oz_smem, h->stream>>>(h->planes.p, h->ctab.p, h->oz);
+    if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
+    stage_mark(h, 3);
+    if ((rc = launch_fft(h, -1))) return rc;
+    stage_mark(h, 4);
+    GatherArgs ga;
+    ga.N = g.N;
+    ga.no = g.no;
+    ga.np = g.np;
+    ga.rho0 = g.rho0;
+    ga.kT = g.kT;
+    ga.dv = g.dv;
+    const double fourpisq = 4.0 * kPi * kPi;
+    ga.prefactor = -g.kT * 2.0 * fourpisq / g.mrso / g.n0;
+    ga.cst = 1.0 / (double)(g.nx * g.ny * g.nz);
+    ga.do_ideal = do_ideal;
+    ga.df_mode = d_df ? df_mode : 0;
+    if (h->bm_gather == 64)
+        k_gather_f64<64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes(64, g.np), h->stream>>>(
+            h->planes.p, h->B.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+    else
+        k_gather_f64<32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes(32, g.np), h->stream>>>(
+            h->planes.p, h->B.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+    if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
+    k_reduce3<<<1, 256, 0, h->stream>>>(h->partial.p, h->nblk_gather, h->sums.p);
+    h->launches += 10;
+    stage_mark(h, 5);
+    return check_cuda(cudaGetLastError(), "reduce launch");
+}
+
+int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
+    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "evaluation"))) return rc;
+    if (h->timing) {
+        for (int i = 0; i < ST_COUNT; ++i) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->ev[i], h->ev[i + 1]);
+            h->stage_ms[i] += ms;
+        }
+        h->stage_count++;
+    }
+    *fid = h->h_sums[0];
+    *fext = h->h_sums[1];
+    *fexc = h->h_sums[2] * 0.5 * h->g.dv;
+    if (!std::isfinite(*fid) || !std::isfinite(*fext) || !std::isfinite(*fexc)) {
+        set_error("non-finite functional (F_id=%g F_ext=%g F_exc=%g)", *fid, *fext, *fexc);
+        return MDFT_E_NUMERIC;
+    }
+    return 0;
+}
+
+double combine(const mdft_handle *h, double fid, double fext, double fexc) {
+    // src/module_energy_and_gradient.f90:89-217
+    double f = 0.0;
+    f = f + fid + fext;
+    f = f + fexc;
+    f = f + 0.0;  // bridge "no"
+    f = f + h->const_corr;
+    return f;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------------------
+extern "C" {
+
+const char *mdft_last_error(void) { return last_error(); }
+
+int mdft_create(const mdft_desc *d, mdft_handle **out) {
+    if (!d || !out) { set_error("null argument"); return MDFT_E_ARG; }
+    *out = nullptr;
+    if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0 || (d->nx & 1) || (d->ny & 1) || (d->nz & 1)) {
+        set_error("grid sizes must be positive and even (got %d %d %d)", d->nx, d->ny, d->nz);
+        return MDFT_E_ARG;
+    }
+    if (!(d->lx > 0 && d->ly > 0 && d->lz > 0)) { set_error("box lengths must be positive"); return MDFT_E_ARG; }
+    if (d->mmax < 0 || d->mmax > kMaxMmax) { set_error("mmax must be in [0, %d]", kMaxMmax); return MDFT_E_ARG; }
+    if (d->mrso < 1) { set_error("mrso must be >= 1"); return MDFT_E_ARG; }
+    if (!(d->temperature > 0) || !(d->n0 > 0)) { set_error("temperature and n0 must be positive"); return MDFT_E_ARG; }
+    if (d->precision != MDFT_PREC_FP64 && d->precision != MDFT_PREC_MIXED) { set_error("unknown precision %d", d->precision); return MDFT_E_ARG; }
+    std::unique_ptr<mdft_handle> h(new mdft_handle());
+    h->precision = d->precision;
+    h->device = d->device;
+    // host-side set-up first: argument and c(k) errors do not depend on the device
+    const double kT = kBoltz * kNavo * d->temperature * 1.0e-3;  // src/module_thermo.f90:62
+    if (build_grid(h->g, d->nx, d->ny, d->nz, d->lx, d->ly, d->lz, d->mmax, d->mrso, kT, d->n0)) return MDFT_E_ARG;
+    const Grid &g = h->g;
+    if (g.np > kMaxNpConst) { set_error("too many projections (%d)", g.np); return MDFT_E_ARG; }
+    {
+        FftPlan1D tmp;
+        const int dims[3] = {d->nx, d->ny, d->nz};
+        for (int ax = 0; ax < 3; ++ax)
+            if (!make_plan1d(dims[ax], tmp)) { set_error("grid size %d is not of the form 2^a 3^b", dims[ax]); return MDFT_E_ARG; }
+    }
+    if (read_ctable(g, d->ck_path, h->ct)) return MDFT_E_IO;
+    int rc = check_cuda(cudaSetDevice(d->device), "cudaSetDevice");
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"))) return rc;
+    for (int i = 0; i <= ST_COUNT; ++i)
+        if ((rc = check_cuda(cudaEventCreate(&h->ev[i]), "event"))) return rc;
+    const size_t nf = (size_t)g.N * g.no;
+    if ((rc = alloc_check(h->xi.alloc(nf), "xi", nf * 8))) return rc;
+    if ((rc = alloc_check(h->vext.alloc(nf), "vext", nf * 8))) return rc;
+    if ((rc = alloc_check(h->df.alloc(nf), "df", nf * 8))) return rc;
+    if ((rc = alloc_check(h->planes.alloc((size_t)g.np * g.N), "projection planes", (size_t)g.np * g.N * 16))) return rc;
+    if ((rc = check_cuda(cudaMemsetAsync(h->vext.p, 0, nf * 8, h->stream), "vext clear"))) return rc;
+    std::vector<double> A, B;
+    build_angular_matrices(g, A, B);
+    if ((rc = alloc_check(h->A.alloc(A.size()), "A", A.size() * 8))) return rc;
+    if ((rc = alloc_check(h->B.alloc(B.size()), "B", B.size() * 8))) return rc;
+    if ((rc = alloc_check(h->w.alloc(g.no), "w", g.no * 8))) return rc;
+    cudaMemcpy(h->A.p, A.data(), A.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->B.p, B.data(), B.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->w.p, g.w.data(), g.no * 8, cudaMemcpyHostToDevice);
+    if ((rc = alloc_check(h->ctab.alloc((size_t)h->ct.nq * h->ct.ncoef), "c table", h->ct.c.size() * 8))) return rc;
+    cudaMemcpy(h->ctab.p, h->ct.c.data(), h->ct.c.size() * 8, cudaMemcpyHostToDevice);
+    // constant tables
+    RotCoef rcf;
+    build_rot_coef(rcf);
+    std::vector<int> pm(kMaxNpConst, 0), pmup(kMaxNpConst, 0), pmu2(kMaxNpConst, 0), ias(kMaxNpConst, 0);
+    for (int i = 0; i < g.np; ++i) {
+        pm[i] = g.pm[i];
+        pmup[i] = g.pmup[i];
+        pmu2[i] = g.pmu[i] / g.mrso;
+        ias[i] = h->ct.ia_start[i];
+    }
+    cudaMemcpyToSymbol(c_rot, &rcf, sizeof rcf);
+    cudaMemcpyToSymbol(c_pm, pm.data(), kMaxNpConst * sizeof(int));
+    cudaMemcpyToSymbol(c_pmup, pmup.data(), kMaxNpConst * sizeof(int));
+    cudaMemcpyToSymbol(c_pmu2, pmu2.data(), kMaxNpConst * sizeof(int));
+    cudaMemcpyToSymbol(c_ia_start, ias.data(), kMaxNpConst * sizeof(int));
+    if ((rc = check_cuda(cudaGetLastError(), "table upload"))) return rc;
+    // launch shapes
+    int maxsmem = 0;
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device);
+    h->bm_project = project_smem_bytes(64, g.no) <= (size_t)maxsmem ? 64 : 32;
+    h->bm_gather = gather_smem_bytes(64, g.np) <= (size_t)maxsmem ? 64 : 32;
+    if (project_smem_bytes(h->bm_project, g.no) > (size_t)maxsmem || gather_smem_bytes(h->bm_gather, g.np) > (size_t)maxsmem) {
+        set_error("angular transform tiles do not fit in shared memory");
+        return MDFT_E_ARG;
+    }
+    cudaFuncSetAttribute(k_project_f64<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    cudaFuncSetAttribute(k_project_f64<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    cudaFuncSetAttribute(k_gather_f64<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    cudaFuncSetAttribute(k_gather_f64<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    cudaFuncSetAttribute(k_oz_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
+    h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
+    if ((rc = alloc_check(h->partial.alloc(3 * (size_t)h->nblk_gather), "partials", 24 * h->nblk_gather))) return rc;
+    if ((rc = alloc_check(h->sums.alloc(8), "sums", 64))) return rc;
+    if ((rc = check_cuda(cudaMallocHost(&h->h_sums, 8 * sizeof(double)), "pinned sums"))) return rc;
+    if ((rc = alloc_check(h->vpart.alloc(2 * kRedBlocks), "reduction partials", 16 * kRedBlocks))) return rc;
+    if ((rc = alloc_check(h->vsc.alloc(kScalarSlots), "reduction scalars", 8 * kScalarSlots))) return rc;
+    if ((rc = check_cuda(cudaMallocHost(&h->h_vsc, sizeof(double) * kScalarSlots), "pinned scalars"))) return rc;
+    if ((rc = setup_fft(h.get()))) return rc;
+    for (int ax = 0; ax < 3; ++ax)
+        if (h->fft[ax].smem > (size_t)maxsmem) { set_error("FFT tile does not fit in shared memory"); return MDFT_E_ARG; }
+    OzArgs &oz = h->oz;
+    oz.nx = g.nx; oz.ny = g.ny; oz.nz = g.nz; oz.N = g.N;
+    oz.mmax = g.mmax; oz.mrso = g.mrso; oz.np = g.np;
+    oz.ncoef = h->ct.ncoef; oz.nq = h->ct.nq; oz.dq = h->ct.dq;
+    oz.twopi_lx = 2.0 * kPi / g.lx;
+    oz.twopi_ly = 2.0 * kPi / g.ly;
+    oz.twopi_lz = 2.0 * kPi / g.lz;
+    oz.quirks = 1;
+    oz.nk = (long long)g.nx * g.ny * (g.nz / 2 + 1);
+    h->oz_grid = (int)((oz.nk + 7) / 8);
+    h->oz_smem = oz_smem_bytes(g.mmax, g.np, 8);
+    if (h->oz_smem > (size_t)maxsmem) { set_error("OZ tile does not fit in shared memory"); return MDFT_E_ARG; }
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "create"))) return rc;
+    *out = h.release();
+    return MDFT_OK;
+}
+
+int mdft_destroy(mdft_handle *h) {
+    if (!h) return MDFT_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->xi.free(); h->vext.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
+    h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free();
+    for (int i = 0; i < 3; ++i) h->tw64[i].free();
+    lbfgs_free(h->lb);
+    h->vpart.free();
+    h->vsc.free();
+    if (h->h_vsc) cudaFreeHost(h->h_vsc);
+    if (h->h_sums) cudaFreeHost(h->h_sums);
+    for (int i = 0; i <= ST_COUNT; ++i)
+        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MDFT_OK;
+}
+
+int mdft_get_sizes(const mdft_handle *h, mdft_sizes *o) {
+    if (!h || !o) { set_error("null argument"); return MDFT_E_ARG; }
+    o->ntheta = h->g.ntheta; o->nphi = h->g.nphi; o->npsi = h->g.npsi;
+    o->no = h->g.no; o->np = h->g.np;
+    o->ncoef = h->ct.ncoef; o->nq = h->ct.nq;
+    o->dv = h->g.dv; o->rho0 = h->g.rho0; o->kT = h->g.kT; o->dq = h->ct.dq;
+    return MDFT_OK;
+}
+
+int mdft_get_stream(const mdft_handle *h, void **s) {
+    if (!h || !s) { set_error("null argument"); return MDFT_E_ARG; }
+    *s = (void *)h->stream;
+    return MDFT_OK;
+}
+
+int mdft_get_weights(const mdft_handle *h, double *w) {
+    if (!h || !w) { set_error("null argument"); return MDFT_E_ARG; }
+    std::memcpy(w, h->g.w.data(), sizeof(double) * h->g.no);
+    return MDFT_OK;
+}
+
+int mdft_set_vext(mdft_handle *h, const double *v) {
+    if (!h || !v) { set_error("null argument"); return MDFT_E_ARG; }
+    size_t n = (size_t)h->g.N * h->g.no;
+    int rc = check_cuda(cudaMemcpyAsync(h->vext.p, v, n * 8, cudaMemcpyHostToDevice, h->stream), "vext upload");
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "vext upload"))) return rc;
+    h->have_vext = true;
+    return MDFT_OK;
+}
+
+int mdft_get_vext(const mdft_handle *h, double *v) {
+    if (!h || !v) { set_error("null argument"); return MDFT_E_ARG; }
+    size_t n = (size_t)h->g.N * h->g.no;
+    int rc = check_cuda(cudaMemcpyAsync(v, h->vext.p, n * 8, cudaMemcpyDeviceToHost, h->stream), "vext download");
+    if (rc) return rc;
+    return check_cuda(cudaStreamSynchronize(h->stream), "vext download");
+}
+
+int mdft_set_constant_correction(mdft_handle *h, double c) {
+    if (!h) { set_error("null argument"); return MDFT_E_ARG; }
+    h->const_corr = c;
+    return MDFT_OK;
+}
+
+int mdft_energy_and_gradient_device(mdft_handle *h, const double *d_xi, double *d_df, double *f, double *terms) {
+    if (!h || !d_xi || !f) { set_error("null argument"); return MDFT_E_ARG; }
+    int rc = run_pipeline(h, d_xi, d_df, 1, 1);
+    if (rc) return rc;
+    double fid, fext, fexc;
+    if ((rc = finish_sums(h, &fid, &fext, &fexc))) return rc;
+    *f = combine(h, fid, fext, fexc);
+    if (terms) {
+        terms[0] = fid;
+        terms[1] = fext;
+        terms[2] = fexc;
+        terms[3] = h->const_corr;
+    }
+    return MDFT_OK;
+}
+
+int mdft_energy_and_gradient(mdft_handle *h, const double *xi, double *f, double *df, double *terms) {
+    if (!h || !xi || !f) { set_error("null argument"); return MDFT_E_ARG; }
+    size_t n = (size_t)h->g.N * h->g.no;
+    int rc = check_cuda(cudaMemcpyAsync(h->xi.p, xi, n * 8, cudaMemcpyHostToDevice, h->stream), "xi upload");
+    if (rc) return rc;
+    if ((rc = mdft_energy_and_gradient_device(h, h->xi.p, df ? h->df.p : nullptr, f, terms))) return rc;
+    if (df) {
+        if ((rc = check_cuda(cudaMemcpyAsync(df, h->df.p, n * 8, cudaMemcpyDeviceToHost, h->stream), "df download"))) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "df download"))) return rc;
+    }
+    return MDFT_OK;
+}
+
+int mdft_excess_energy(mdft_handle *h, const double *xi, double *fexc, double *df) {
+    if (!h || !xi || !fexc) { set_error("null argument"); return MDFT_E_ARG; }
+    size_t n = (size_t)h->g.N * h->g.no;
+    int rc = check_cuda(cudaMemcpyAsync(h->xi.p, xi, n * 8, cudaMemcpyHostToDevice, h->stream), "xi upload");
+    if (rc) return rc;
+    if (df && (rc = check_cuda(cudaMemcpyAsync(h->df.p, df, n * 8, cudaMemcpyHostToDevice, h->stream), "df upload"))) return rc;
+    if ((rc = run_pipeline(h, h->xi.p, df ? h->df.p : nullptr, 0, 2))) return rc;
+    double a, b;
+    if ((rc = finish_sums(h, &a, &b, fexc))) return rc;
+    if (df) {
+        if ((rc = check_cuda(cudaMemcpyAsync(df, h->df.p, n * 8, cudaMemcpyDeviceToHost, h->stream), "df download"))) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "df download"))) return rc;
+    }
+    return MDFT_OK;
+}
+
+int mdft_set_timing(mdft_handle *h, int on) {
+    if (!h) { set_error("null argument"); return MDFT_E_ARG; }
+    h->timing = on != 0;
+    for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = 0;
+    h->stage_count = 0;
+    return MDFT_OK;
+}
+
+int mdft_get_launch_count(const mdft_handle *h, long long *count) {
+    if (!h || !count) { set_error("null argument"); return MDFT_E_ARG; }
+    *count = h->launches;
+    return MDFT_OK;
+}
+
+int mdft_get_stage_times(const mdft_handle *h, double *ms5, int *count) {
+    if (!h || !ms5) { set_error("null argument"); return MDFT_E_ARG; }
+    for (int i = 0; i < ST_COUNT; ++i) ms5[i] = h->stage_ms[i];
+    if (count) *count = h->stage_count;
+    return MDFT_OK;
+}
+
+}  // extern "C"
+
+#include "solve.cuh"

@@ -1,0 +1,666 @@
+// Solve-level entry points: external potential, initial guess, the L-BFGS
+// minimisation on the device and the pressure-corrected solvation free
+// energy.  Included by mdft_b200.cu after the handle definition.
+#pragma once
+
+namespace {
+
+constexpr double kQfact = 1.602176565e-19 * 1.602176565e-19 * 1.0e-3 * 6.02214129e23 /
+                          (4.0 * 3.14159265358979323846 * 8.854187817e-12 * 1.0e-10);  // src/module_constants.f90:25
+
+inline unsigned vec_grid() { return kRedBlocks; }
+
+// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.
+int eval_fg(mdft_handle *h, const double *x, double *g, const double *dvec, double *f, double *gd, double *gmax) {
+    LbfgsState &L = h->lb;
+    int rc = run_pipeline(h, x, g, 1, 1);
+    if (rc) return rc;
+    k_dot_max<<<vec_grid(), kRedThreads, 0, h->stream>>>(g, dvec, L.n, h->vpart.p);
+    k_finish_dot_max<<<1, 256, 0, h->stream>>>(h->vpart.p, vec_grid(), h->vsc.p, 0);
+    h->launches += 2;
+    if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc, h->vsc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "scalars"))) return rc;
+    double fid, fext, fexc;
+    if ((rc = finish_sums(h, &fid, &fext, &fexc))) return rc;
+    *f = combine(h, fid, fext, fexc);
+    if (gd) *gd = h->h_vsc[0];
+    if (gmax) *gmax = h->h_vsc[1];
+    if (!std::isfinite(h->h_vsc[0]) || !std::isfinite(h->h_vsc[1])) {
+        set_error("non-finite gradient");
+        return MDFT_E_NUMERIC;
+    }
+    return 0;
+}
+
+// host value of a.b (a, b device)
+int dev_dot(mdft_handle *h, const double *a, const double *b, double *out) {
+    LbfgsState &L = h->lb;
+    k_dot_max<<<vec_grid(), kRedThreads, 0, h->stream>>>(a, b, L.n, h->vpart.p);
+    k_finish_dot_max<<<1, 256, 0, h->stream>>>(h->vpart.p, vec_grid(), h->vsc.p, 2);
+    h->launches += 2;
+    int rc = check_cuda(cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "dot");
+    (void)L;
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "dot"))) return rc;
+    *out = h->h_vsc[2];
+    return 0;
+}
+
+int lbfgs_alloc(mdft_handle *h, int m) {
+    LbfgsState &L = h->lb;
+    const long long n = h->g.N * h->g.no;
+    if (L.n == n && L.m == m) return 0;
+    lbfgs_free(L);
+    L.n = n;
+    L.m = m;
+    int rc;
+    DevBuf<double> *v[] = {&L.x, &L.z, &L.d, &L.t, &L.r, &L.q};
+    for (auto *b : v)
+        if ((rc = alloc_check(b->alloc(n), "L-BFGS vector", n * 8))) return rc;
+    if ((rc = alloc_check(L.S.alloc((size_t)m * n), "L-BFGS s history", (size_t)m * n * 8))) return rc;
+    return alloc_check(L.Y.alloc((size_t)m * n), "L-BFGS y history", (size_t)m * n * 8);
+}
+
+// Moré-Thuente search of src/module_lbfgs_nocedal_mdft.f90:1653-1959 (dcsrch/dcstep),
+// with the reference's single-precision constants.
+struct LineSearch {
+    int brackt = 0, stage = 1;
+    double ginit = 0, gtest = 0, gx = 0, gy = 0, finit = 0, fx = 0, fy = 0, stx = 0, sty = 0, stmin = 0, stmax = 0,
+           width = 0, width1 = 0;
+};
+enum { LS_FG = 0, LS_CONV = 1, LS_WARN = 2, LS_ERROR = 3 };
+
+void dcstep(double &stx, double &fx, double &dx, double &sty, double &fy, double &dy, double &stp, double fp, double dp,
+            int &brackt, double stpmin, double stpmax) {
+    const double p66 = (double)0.66f;
+    double gamma, p, q, r, s, stpc, stpf, stpq, theta;
+    double sgnd = dp * (dx / std::fabs(dx));
+    if (fp > fx) {
+        theta = 3.0 * (fx - fp) / (stp - stx) + dx + dp;
+        s = std::max(std::max(std::fabs(theta), std::fabs(dx)), std::fabs(dp));
+        gamma = s * std::sqrt((theta / s) * (theta / s) - (dx / s) * (dp / s));
+        if (stp < stx) gamma = -gamma;
+        p = (gamma - dx) + theta;
+        q = ((gamma - dx) + gamma) + dp;
+        r = p / q;
+        stpc = stx + r * (stp - stx);
+        stpq = stx + ((dx / ((fx - fp) / (stp - stx) + dx)) / 2.0) * (stp - stx);
+        stpf = (std::fabs(stpc - stx) < std::fabs(stpq - stx)) ? stpc : stpc + (stpq - stpc) / 2.0;
+        brackt = 1;
+    } else if (sgnd < 0.0) {
+        theta = 3.0 * (fx - fp) / (stp - stx) + dx + dp;
+        s = std::max(std::max(std::fabs(theta), std::fabs(dx)), std::fabs(dp));
+        gamma = s * std::sqrt((theta / s) * (theta / s) - (dx / s) * (dp / s));
+        if (stp > stx) gamma = -gamma;
+        p = (gamma - dp) + theta;
+        q = ((gamma - dp) + gamma) + dx;
+        r = p / q;
+        stpc = stp + r * (stx - stp);
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        stpf = (std::fabs(stpc - stp) > std::fabs(stpq - stp)) ? stpc : stpq;
+        brackt = 1;
+    } else if (std::fabs(dp) < std::fabs(dx)) {
+        theta = 3.0 * (fx - fp) / (stp - stx) + dx + dp;
+        s = std::max(std::max(std::fabs(theta), std::fabs(dx)), std::fabs(dp));
+        gamma = s * std::sqrt(std::max(0.0, (theta / s) * (theta / s) - (dx / s) * (dp / s)));
+        if (stp > stx) gamma = -gamma;
+        p = (gamma - dp) + theta;
+        q = (gamma + (dx - dp)) + gamma;
+        r = p / q;
+        if (r < 0.0 && gamma != 0.0) stpc = stp + r * (stx - stp);
+        else if (stp > stx) stpc = stpmax;
+        else stpc = stpmin;
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        if (brackt) {
+            stpf = (std::fabs(stpc - stp) < std::fabs(stpq - stp)) ? stpc : stpq;
+            if (stp > stx) stpf = std::min(stp + p66 * (sty - stp), stpf);
+            else stpf = std::max(stp + p66 * (sty - stp), stpf);
+        } else {
+            stpf = (std::fabs(stpc - stp) > std::fabs(stpq - stp)) ? stpc : stpq;
+            stpf = std::min(stpmax, stpf);
+            stpf = std::max(stpmin, stpf);
+        }
+    } else {
+        if (brackt) {
+            theta = 3.0 * (fp - fy) / (sty - stp) + dy + dp;
+            s = std::max(std::max(std::fabs(theta), std::fabs(dy)), std::fabs(dp));
+            gamma = s * std::sqrt((theta / s) * (theta / s) - (dy / s) * (dp / s));
+            if (stp > sty) gamma = -gamma;
+            p = (gamma - dp) + theta;
+            q = ((gamma - dp) + gamma) + dy;
+            r = p / q;
+            stpc = stp + r * (sty - stp);
+            stpf = stpc;
+        } else if (stp > stx) stpf = stpmax;
+        else stpf = stpmin;
+    }
+    if (fp > fx) {
+        sty = stp; fy = fp; dy = dp;
+    } else {
+        if (sgnd < 0.0) { sty = stx; fy = fx; dy = dx; }
+        stx = stp; fx = fp; dx = dp;
+    }
+    stp = stpf;
+}
+
+int dcsrch(double f, double g, double &stp, double ftol, double gtol, double xtol, double stpmin, double stpmax, bool start,
+           LineSearch &S) {
+    const double p5 = 0.5, p66 = (double)0.66f, xtrapl = (double)1.1f, xtrapu = 4.0;
+    if (start) {
+        if (stp < stpmin || stp > stpmax || g >= 0.0 || ftol < 0.0 || gtol < 0.0 || xtol < 0.0 || stpmin < 0.0 ||
+            stpmax < stpmin)
+            return LS_ERROR;
+        S = LineSearch();
+        S.brackt = 0; S.stage = 1; S.finit = f; S.ginit = g; S.gtest = ftol * S.ginit;
+        S.width = stpmax - stpmin; S.width1 = S.width / p5;
+        S.stx = 0.0; S.fx = S.finit; S.gx = S.ginit;
+        S.sty = 0.0; S.fy = S.finit; S.gy = S.ginit;
+        S.stmin = 0.0; S.stmax = stp + xtrapu * stp;
+        return LS_FG;
+    }
+    int task = LS_FG;
+    double ftest = S.finit + stp * S.gtest;
+    if (S.stage == 1 && f <= ftest && g >= 0.0) S.stage = 2;
+    if (S.brackt && (stp <= S.stmin || stp >= S.stmax)) task = LS_WARN;
+    if (S.brackt && S.stmax - S.stmin <= xtol * S.stmax) task = LS_WARN;
+    if (stp == stpmax && f <= ftest && g <= S.gtest) task = LS_WARN;
+    if (stp == stpmin && (f > ftest || g >= S.gtest)) task = LS_WARN;
+    if (f <= ftest && std::fabs(g) <= gtol * (-S.ginit)) task = LS_CONV;
+    if (task != LS_FG) return task;
+    if (S.stage == 1 && f <= S.fx && f > ftest) {
+        double fm = f - stp * S.gtest, fxm = S.fx - S.stx * S.gtest, fym = S.fy - S.sty * S.gtest;
+        double gm = g - S.gtest, gxm = S.gx - S.gtest, gym = S.gy - S.gtest;
+        dcstep(S.stx, fxm, gxm, S.sty, fym, gym, stp, fm, gm, S.brackt, S.stmin, S.stmax);
+        S.fx = fxm + S.stx * S.gtest;
+        S.fy = fym + S.sty * S.gtest;
+        S.gx = gxm + S.gtest;
+        S.gy = gym + S.gtest;
+    } else {
+        dcstep(S.stx, S.fx, S.gx, S.sty, S.fy, S.gy, stp, f, g, S.brackt, S.stmin, S.stmax);
+    }
+    if (S.brackt) {
+        if (std::fabs(S.sty - S.stx) >= p66 * S.width1) stp = S.stx + p5 * (S.sty - S.stx);
+        S.width1 = S.width;
+        S.width = std::fabs(S.sty - S.stx);
+    }
+    if (S.brackt) { S.stmin = std::min(S.stx, S.sty); S.stmax = std::max(S.stx, S.sty); }
+    else { S.stmin = stp + xtrapl * (stp - S.stx); S.stmax = stp + xtrapu * (stp - S.stx); }
+    stp = std::max(stp, stpmin);
+    stp = std::min(stp, stpmax);
+    if ((S.brackt && (stp <= S.stmin || stp >= S.stmax)) || (S.brackt && S.stmax - S.stmin <= xtol * S.stmax)) stp = S.stx;
+    return LS_FG;
+}
+
+// Launch a batched FFT over `nplanes` planes starting at `data`.
+int launch_fft_planes(mdft_handle *h, double2 *data, int nplanes, int sign) {
+    const Grid &g = h->g;
+    const int dims[3] = {g.nx, g.ny, g.nz};
+    for (int ax = 0; ax < 3; ++ax) {
+        FftAxisArgs a = h->fft[ax].args;
+        a.nplanes = nplanes;
+        a.sign = sign;
+        long long lines_div = (ax == 0) ? (long long)nplanes * g.ny * g.nz : g.nx;
+        a.TL = pick_tl(lines_div, dims[ax]);
+        long long nlines = (long long)nplanes * g.N / dims[ax];
+        size_t smem = fft_smem_bytes<double>(dims[ax], a.TL);
+        k_fft_axis<double><<<(unsigned)(nlines / a.TL), kFftThreads, smem, h->stream>>>(data, (const double2 *)h->fft[ax].tw, a);
+        h->launches += 1;
+    }
+    return check_cuda(cudaGetLastError(), "fft launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdft_compute_vext(mdft_handle *h, int nsite, const double *q, const double *sig, const double *eps, const double *xyz,
+                      int nsv, const double *sq, const double *ssig, const double *seps, const double *sxyz, double rvdw,
+                      double *lj_tail) {
+    if (!h || nsite < 0 || (nsite > 0 && (!q || !sig || !eps || !xyz)) || nsv <= 0 || !sq || !ssig || !seps || !sxyz) {
+        set_error("null or invalid argument");
+        return MDFT_E_ARG;
+    }
+    const Grid &g = h->g;
+    const long long N = g.N;
+    const size_t nf = (size_t)N * g.no;
+    int rc;
+    // ---- electrostatics (vextq kept apart in the df buffer until the sum) ----
+    bool charged = false;
+    for (int s = 0; s < nsite; ++s)
+        if (std::fabs(q[s]) > kEpsDp) charged = true;
+    bool have_vq = false;
+    if (charged) {
+        std::vector<double> rho(N, 0.0);
+        const int n3[3] = {g.nx, g.ny, g.nz};
+        const double L3[3] = {g.lx, g.ly, g.lz};
+        const double d3[3] = {g.lx / g.nx, g.ly / g.ny, g.lz / g.nz};
+        for (int s = 0; s < nsite; ++s) {  // src/module_solute.f90:193-236
+            if (!(std::fabs(q[s]) > kEpsDp)) continue;
+            int mi[3], pi[3];
+            double wp[3], wm[3];
+            for (int d = 0; d < 3; ++d) {
+                double x = xyz[3 * s + d];
+                double r = std::fabs(x / d3[d] - std::floor(x / d3[d]));
+                double md = std::fmod(x, L3[d]);
+                if (md < 0) md += L3[d];
+                mi[d] = (int)std::floor(md / d3[d]);
+                if (mi[d] >= n3[d]) mi[d] = n3[d] - 1;
+                pi[d] = (mi[d] + 1) % n3[d];
+                wp[d] = r;
+                wm[d] = 1.0 - r;
+            }
+            auto at = [&](int a, int b, int c) -> double & { return rho[((size_t)c * g.ny + b) * g.nx + a]; };
+            at(mi[0], mi[1], mi[2]) += q[s] * wm[0] * wm[1] * wm[2];
+            at(pi[0], mi[1], mi[2]) += q[s] * wp[0] * wm[1] * wm[2];
+            at(mi[0], pi[1], mi[2]) += q[s] * wm[0] * wp[1] * wm[2];
+            at(mi[0], mi[1], pi[2]) += q[s] * wm[0] * wm[1] * wp[2];
+            at(pi[0], pi[1], mi[2]) += q[s] * wp[0] * wp[1] * wm[2];
+            at(pi[0], mi[1], pi[2]) += q[s] * wp[0] * wm[1] * wp[2];
+            at(mi[0], pi[1], pi[2]) += q[s] * wm[0] * wp[1] * wp[2];
+            at(pi[0], pi[1], pi[2]) += q[s] * wp[0] * wp[1] * wp[2];
+        }
+        const double vol = d3[0] * d3[1] * d3[2];
+        bool allzero = true;
+        for (auto &v : rho) {
+            v /= vol;
+            if (std::fabs(v) > kEpsDp) allzero = false;
+        }
+        if (!allzero) {
+            DevBuf<double> drho, dsq, dsx, drot;
+            DevBuf<double2> vk;
+            std::vector<double> cq, cx;
+            for (int s = 0; s < nsv; ++s)
+                if (std::fabs(sq[s]) > kEpsDp) {
+                    cq.push_back(sq[s]);
+                    cx.insert(cx.end(), sxyz + 3 * s, sxyz + 3 * s + 3);
+                }
+            if ((rc = alloc_check(drho.alloc(N), "charge density", N * 8))) return rc;
+            if ((rc = alloc_check(vk.alloc(N), "V(k)", N * 16))) return rc;
+            if ((rc = alloc_check(dsq.alloc(std::max<size_t>(1, cq.size())), "solvent charges", 64))) return rc;
+            if ((rc = alloc_check(dsx.alloc(std::max<size_t>(3, cx.size())), "solvent sites", 64))) return rc;
+            if ((rc = alloc_check(drot.alloc(9 * (size_t)g.no), "orientations", 72 * g.no))) return rc;
+            cudaMemcpyAsync(drho.p, rho.data(), N * 8, cudaMemcpyHostToDevice, h->stream);
+            if (!cq.empty()) {
+                cudaMemcpyAsync(dsq.p, cq.data(), cq.size() * 8, cudaMemcpyHostToDevice, h->stream);
+                cudaMemcpyAsync(dsx.p, cx.data(), cx.size() * 8, cudaMemcpyHostToDevice, h->stream);
+            }
+            cudaMemcpyAsync(drot.p, g.rotm.data(), 72 * (size_t)g.no, cudaMemcpyHostToDevice, h->stream);
+            k_real_to_cplx<<<vec_grid(), 256, 0, h->stream>>>(drho.p, h->planes.p, N);
+            if ((rc = launch_fft_planes(h, h->planes.p, 1, -1))) return rc;
+            k_poisson<<<vec_grid(), 256, 0, h->stream>>>(h->planes.p, vk.p, g.nx, g.ny, g.nz, g.lx, g.ly, g.lz);
+            const int batch = g.np;
+            for (int io0 = 0; io0 < g.no; io0 += batch) {
+                SigmaArgs sa{g.nx, g.ny, g.nz, g.no, 2.0 * kPi / g.lx, 2.0 * kPi / g.ly, 2.0 * kPi / g.lz, (int)cq.size(), io0,
+                             std::min(batch, g.no - io0)};
+                k_sigma_product<<<vec_grid(), 256, 0, h->stream>>>(vk.p, h->planes.p, drot.p, dsq.p, dsx.p, sa);
+                if ((rc = launch_fft_planes(h, h->planes.p, sa.nbatch, +1))) return rc;
+                k_sigma_store<<<vec_grid(), 256, 0, h->stream>>>(h->planes.p, h->df.p, g.no, io0, sa.nbatch, N, kQfact / (double)N);
+            }
+            if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "electrostatics"))) return rc;
+            have_vq = true;
+        }
+    }
+    // ---- Lennard-Jones (src/module_lennardjones.f90:9-226) ----
+    const double cutoff = rvdw;
+    if (cutoff > g.lx * 0.5 || cutoff > g.ly * 0.5 || cutoff > g.lz * 0.5) {
+        set_error("LJ cut-off %g larger than half the box", cutoff);
+        return MDFT_E_ARG;
+    }
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    const double L3[3] = {g.lx, g.ly, g.lz}, D3[3] = {g.dx, g.dy, g.dz};
+    int tabsize[3];
+    for (int d = 0; d < 3; ++d) tabsize[d] = (int)std::floor(2 * cutoff / D3[d]) + 1;
+    bool only_origin = true;
+    for (int s = 0; s < nsv; ++s)
+        if (seps[s] != 0.0 && (sxyz[3 * s] != 0.0 || sxyz[3 * s + 1] != 0.0 || sxyz[3 * s + 2] != 0.0)) only_origin = false;
+    std::vector<LJTerm> terms;
+    double ljcorr = 0.0;
+    for (int u = 0; u < nsite; ++u) {
+        if (eps[u] <= kEpsDp) continue;
+        LJTerm base{};
+        base.px = xyz[3 * u]; base.py = xyz[3 * u + 1]; base.pz = xyz[3 * u + 2];
+        for (int d = 0; d < 3; ++d) {
+            double r = xyz[3 * u + d];
+            int mn = (int)std::floor(std::fmod(r - cutoff + L3[d], L3[d]) / D3[d]) + 1;
+            int mx = (int)std::floor(std::fmod(r + cutoff, L3[d]) / D3[d]) + 1;
+            if (mn < 1 || mx > n3[d]) {
+                set_error("LJ node range check failed for site %d", u + 1);
+                return MDFT_E_ARG;
+            }
+            // the reference loops over the first tabsize entries of the realised table
+            int ts = tabsize[d];
+            base.lo[d][1] = 1; base.hi[d][1] = 0;  // empty
+            if (mn < mx) {
+                base.lo[d][0] = mn - 1;
+                base.hi[d][0] = std::min(mx, mn + ts - 1) - 1;
+            } else {
+                int first = std::min(mx, ts);
+                base.lo[d][0] = 0;
+                base.hi[d][0] = first - 1;
+                int rest = ts - first;
+                if (rest > 0) {
+                    base.lo[d][1] = mn - 1;
+                    base.hi[d][1] = std::min(n3[d], mn + rest - 1) - 1;
+                }
+            }
+        }
+        for (int ss = 0; ss < nsv; ++ss) {
+            if (seps[ss] <= kEpsDp) continue;
+            LJTerm t = base;
+            t.epsuv = std::sqrt(eps[u] * seps[ss]);
+            t.siguv6 = powi((sig[u] + ssig[ss]) * 0.5, 6);
+            t.sx = sxyz[3 * ss]; t.sy = sxyz[3 * ss + 1]; t.sz = sxyz[3 * ss + 2];
+            ljcorr = ljcorr - (16.0 * 3.14159 / 3.0) * t.epsuv * t.siguv6 * g.n0 / powi(cutoff, 3);
+            terms.push_back(t);
+        }
+    }
+    if ((rc = check_cuda(cudaMemsetAsync(h->vext.p, 0, nf * 8, h->stream), "vext clear"))) return rc;
+    if (!terms.empty()) {
+        DevBuf<LJTerm> dt;
+        DevBuf<double> drot;
+        if ((rc = alloc_check(dt.alloc(terms.size()), "LJ terms", terms.size() * sizeof(LJTerm)))) return rc;
+        if ((rc = alloc_check(drot.alloc(9 * (size_t)g.no), "orientations", 72 * g.no))) return rc;
+        cudaMemcpyAsync(dt.p, terms.data(), terms.size() * sizeof(LJTerm), cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(drot.p, g.rotm.data(), 72 * (size_t)g.no, cudaMemcpyHostToDevice, h->stream);
+        LJArgs la{g.nx, g.ny, g.nz, g.no, g.dx, g.dy, g.dz, g.lx, g.ly, g.lz, cutoff * cutoff, (int)terms.size(), only_origin ? 1 : 0};
+        k_lj<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, dt.p, drot.p, la);
+        if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "Lennard-Jones"))) return rc;
+    }
+    // ---- vext_total_sum ----
+    DevBuf<int> flag;
+    if ((rc = alloc_check(flag.alloc(1), "flag", 4))) return rc;
+    cudaMemsetAsync(flag.p, 0, 4, h->stream);
+    k_vext_total<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, have_vq ? h->df.p : nullptr, kQfact / 2.0, (long long)nf, flag.p);
+    int hflag = 0;
+    cudaMemcpyAsync(&hflag, flag.p, 4, cudaMemcpyDeviceToHost, h->stream);
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "vext sum"))) return rc;
+    if (hflag & 1) { set_error("NaN or Inf in vext"); return MDFT_E_NUMERIC; }
+    if (hflag & 2) { set_error("vext below -qfact/2 somewhere"); return MDFT_E_NUMERIC; }
+    h->have_vext = true;
+    if (lj_tail) *lj_tail = ljcorr;
+    return MDFT_OK;
+}
+
+int mdft_guess_density(const mdft_handle *h, double *xi) {
+    if (!h || !xi) { set_error("null argument"); return MDFT_E_ARG; }
+    const size_t nf = (size_t)h->g.N * h->g.no;
+    const double vmax = (-std::log(kEpsDp) - (double)0.05f) * h->g.kT;
+    mdft_handle *hh = const_cast<mdft_handle *>(h);
+    k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, hh->xi.p, vmax, (long long)nf);
+    int rc = check_cuda(cudaMemcpyAsync(xi, h->xi.p, nf * 8, cudaMemcpyDeviceToHost, h->stream), "guess download");
+    if (rc) return rc;
+    return check_cuda(cudaStreamSynchronize(h->stream), "guess");
+}
+
+}  // extern "C"
+
+namespace {
+
+// The L-BFGS loop on L.x (already holding the start point).
+int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_result *res) {
+    int rc;
+    LbfgsState &L = h->lb;
+    const long long n = L.n;
+    const int m = o->m;
+    const unsigned G = vec_grid();
+    cudaStream_t st = h->stream;
+    const long long l0 = h->launches;
+    long long vec_launches = 0;
+    double *g = h->df.p;  // gradient lives in the handle's df buffer
+    const double epsmch = kEpsDp;
+    const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
+    std::vector<double> rho(m, 0.0);
+    double f = 0, fold = 0, theta = 1.0, stp = 0, gd = 0, gdold = 0, gmax = 0;
+    int col = 0, head = 0, itail = 0, iupdat = 0, iter = 0, nfgv = 0, status = 3;
+    if ((rc = eval_fg(h, L.x.p, g, nullptr, &f, nullptr, &gmax))) return rc;
+    nfgv = 1;
+    double sbgnrm = gmax;
+    if (sbgnrm <= o->pgtol) { status = 0; goto done; }
+    while (iter < o->itermax) {
+        // ---- search direction ----
+        if (col == 0) {
+            k_sd_step<<<G, 256, 0, st>>>(L.x.p, g, L.z.p, L.d.p, n); ++vec_launches;
+        } else {
+            // two-loop recursion for q = -H g, H0 = I/theta (equal to the compact L-BFGS-B step
+            // of formk/cmprlb/subsm for an unconstrained problem)
+            double *q = L.q.p, *sc = h->vsc.p;
+            auto aslot = [](int j) { return 8 + 2 * j; };
+            auto bslot = [m](int j) { return 8 + 2 * m + 2 * j; };
+            k_neg<<<G, 256, 0, st>>>(g, q, n); ++vec_launches;
+            int jn = (head + col - 1) % m;
+            k_dot_max<<<G, kRedThreads, 0, st>>>(L.S.p + (size_t)jn * n, q, n, h->vpart.p); ++vec_launches;
+            k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, aslot(jn)); ++vec_launches;
+            for (int k = col - 1; k >= 0; --k) {
+                int j = (head + k) % m;
+                int jnext = (k > 0) ? (head + k - 1) % m : -1;
+                k_axpy_dot<<<G, kRedThreads, 0, st>>>(q, L.Y.p + (size_t)j * n, jnext >= 0 ? L.S.p + (size_t)jnext * n : nullptr,
+                                                       n, sc, aslot(j), -rho[j], -1, 0.0, 1.0, jnext >= 0 ? h->vpart.p : nullptr); ++vec_launches;
+                if (jnext >= 0) k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, aslot(jnext)); ++vec_launches;
+            }
+            int j0 = head % m;
+            k_axpy_dot<<<G, kRedThreads, 0, st>>>(q, nullptr, L.Y.p + (size_t)j0 * n, n, sc, -1, 0.0, -1, 0.0, 1.0 / theta, h->vpart.p); ++vec_launches;
+            k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, bslot(j0)); ++vec_launches;
+            for (int k = 0; k < col; ++k) {
+                int j = (head + k) % m;
+                int jnext = (k + 1 < col) ? (head + k + 1) % m : -1;
+                k_axpy_dot<<<G, kRedThreads, 0, st>>>(q, L.S.p + (size_t)j * n, jnext >= 0 ? L.Y.p + (size_t)jnext * n : nullptr, n,
+                                                       sc, aslot(j), rho[j], bslot(j), rho[j], 1.0, jnext >= 0 ? h->vpart.p : nullptr); ++vec_launches;
+                if (jnext >= 0) k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, bslot(jnext)); ++vec_launches;
+            }
+            k_qn_step<<<G, 256, 0, st>>>(L.x.p, q, L.z.p, L.d.p, n); ++vec_launches;
+        }
+        if ((rc = check_cuda(cudaGetLastError(), "direction"))) return rc;
+        // ---- line search (lnsrlb) ----
+        const double stpmx = big;
+        if (iter == 0) {
+            double dtd;
+            if ((rc = dev_dot(h, L.d.p, L.d.p, &dtd))) return rc;
+            stp = std::min(1.0 / std::sqrt(dtd), stpmx);
+        } else {
+            stp = 1.0;
+        }
+        cudaMemcpyAsync(L.t.p, L.x.p, n * 8, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(L.r.p, g, n * 8, cudaMemcpyDeviceToDevice, st);
+        fold = f;
+        int ifun = 0, iback = 0, info = 0;
+        if ((rc = dev_dot(h, g, L.d.p, &gd))) return rc;
+        gdold = gd;
+        LineSearch LS;
+        if (gd >= 0.0) {
+            info = -4;
+        } else {
+            int task = dcsrch(f, gd, stp, ftol, gtol, xtol, 0.0, stpmx, true, LS);
+            while (task == LS_FG) {
+                ++ifun;
+                ++nfgv;
+                iback = ifun - 1;
+                if (iback >= 20) break;
+                k_trial_point<<<G, 256, 0, st>>>(L.x.p, L.z.p, L.d.p, L.t.p, stp, n); ++vec_launches;
+                if ((rc = eval_fg(h, L.x.p, g, L.d.p, &f, &gd, &gmax))) return rc;
+                task = dcsrch(f, gd, stp, ftol, gtol, xtol, 0.0, stpmx, false, LS);
+            }
+            if (task == LS_ERROR) info = -1;
+        }
+        if (info != 0 || iback >= 20) {
+            cudaMemcpyAsync(L.x.p, L.t.p, n * 8, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(g, L.r.p, n * 8, cudaMemcpyDeviceToDevice, st);
+            f = fold;
+            if (col == 0) {
+                status = 2;
+                ++iter;
+                goto done;
+            }
+            col = 0; head = 0; itail = 0; theta = 1.0; iupdat = 0;
+            continue;
+        }
+        ++iter;
+        sbgnrm = gmax;
+        if (sbgnrm <= o->pgtol) { status = 0; goto done; }
+        if ((fold - f) <= o->ftol_abs) { status = 1; goto done; }
+        // ---- BFGS update (matupd) ----
+        k_diff_norm<<<G, kRedThreads, 0, st>>>(g, L.r.p, n, h->vpart.p); ++vec_launches;
+        k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, h->vsc.p, 2); ++vec_launches;
+        if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, 8, cudaMemcpyDeviceToHost, st), "rr"))) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(st), "rr"))) return rc;
+        double rr = h->h_vsc[2], dr, ddum;
+        if (stp == 1.0) { dr = gd - gdold; ddum = -gdold; }
+        else { dr = (gd - gdold) * stp; ddum = -gdold * stp; }
+        if (dr <= epsmch * ddum) continue;  // update skipped
+        ++iupdat;
+        if (iupdat <= m) { col = iupdat; itail = (head + iupdat - 1) % m; }
+        else { itail = (itail + 1) % m; head = (head + 1) % m; }
+        k_scale_copy<<<G, 256, 0, st>>>(L.S.p + (size_t)itail * n, L.d.p, stp, n); ++vec_launches;
+        cudaMemcpyAsync(L.Y.p + (size_t)itail * n, L.r.p, n * 8, cudaMemcpyDeviceToDevice, st);
+        rho[itail] = 1.0 / dr;
+        theta = rr / dr;
+    }
+done:
+    if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;
+    h->launches += vec_launches;
+    (void)l0;
+    res->f = f;
+    res->pgnorm = sbgnrm;
+    res->iterations = iter;
+    res->evaluations = nfgv;
+    res->status = status;
+    return MDFT_OK;
+}
+
+int check_min_opts(const mdft_minimize_opts *o) {
+    if (o->m < 1 || o->m > 64 || o->itermax < 1) { set_error("invalid minimiser options"); return MDFT_E_ARG; }
+    if (o->precision != MDFT_PREC_FP64) { set_error("only the FP64 minimiser is available in this build"); return MDFT_E_ARG; }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdft_minimize(mdft_handle *h, double *xi, const mdft_minimize_opts *o, mdft_minimize_result *res) {
+    if (!h || !xi || !o || !res) { set_error("null argument"); return MDFT_E_ARG; }
+    int rc = check_min_opts(o);
+    if (rc) return rc;
+    if ((rc = lbfgs_alloc(h, o->m))) return rc;
+    LbfgsState &L = h->lb;
+    if ((rc = check_cuda(cudaMemcpyAsync(L.x.p, xi, L.n * 8, cudaMemcpyHostToDevice, h->stream), "xi upload"))) return rc;
+    if ((rc = minimize_impl(h, o, res))) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(xi, L.x.p, L.n * 8, cudaMemcpyDeviceToHost, h->stream), "xi download"))) return rc;
+    return check_cuda(cudaStreamSynchronize(h->stream), "xi download");
+}
+
+int mdft_minimize_device(mdft_handle *h, double *d_xi, const mdft_minimize_opts *o, mdft_minimize_result *res) {
+    if (!h || !d_xi || !o || !res) { set_error("null argument"); return MDFT_E_ARG; }
+    int rc = check_min_opts(o);
+    if (rc) return rc;
+    if ((rc = lbfgs_alloc(h, o->m))) return rc;
+    LbfgsState &L = h->lb;
+    if ((rc = check_cuda(cudaMemcpyAsync(L.x.p, d_xi, L.n * 8, cudaMemcpyDeviceToDevice, h->stream), "xi copy"))) return rc;
+    if ((rc = minimize_impl(h, o, res))) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(d_xi, L.x.p, L.n * 8, cudaMemcpyDeviceToDevice, h->stream), "xi copy"))) return rc;
+    return check_cuda(cudaStreamSynchronize(h->stream), "xi copy");
+}
+
+int mdft_guess_density_device(mdft_handle *h, double *d_xi) {
+    if (!h || !d_xi) { set_error("null argument"); return MDFT_E_ARG; }
+    const double vmax = (-std::log(kEpsDp) - (double)0.05f) * h->g.kT;
+    k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, d_xi, vmax, (long long)h->g.N * h->g.no);
+    h->launches += 1;
+    return check_cuda(cudaGetLastError(), "guess launch");
+}
+
+}  // extern "C"
+
+namespace {
+
+// d_xi device; h->xi is overwritten (it holds the empty box afterwards)
+int pressure_impl(mdft_handle *h, const double *d_xi, double ftot, double lj_tail, double *out) {
+    const Grid &g = h->g;
+    const size_t nf = (size_t)g.N * g.no;
+    int rc;
+    cudaStream_t st = h->stream;
+    k_density_sum<<<vec_grid(), 256, 0, st>>>(d_xi, h->w.p, g.no, (long long)nf, g.rho0, h->vpart.p);
+    h->launches += 2;
+    k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, vec_grid(), h->vsc.p, 2);
+    cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, 8, cudaMemcpyDeviceToHost, st);
+    if ((rc = check_cuda(cudaStreamSynchronize(st), "density integral"))) return rc;
+    const double nwith = h->h_vsc[2] * g.dv;
+    const double nwithout = g.n0 * (g.lx * g.ly * g.lz);
+    const double deltaN = nwithout - nwith;
+    // empty box: xi = 0, no charged-solute corrections (src/module_pressure_correction.f90:117-126)
+    if ((rc = check_cuda(cudaMemsetAsync(h->xi.p, 0, nf * 8, st), "xi clear"))) return rc;
+    h->launches += 0;
+    if ((rc = run_pipeline(h, h->xi.p, nullptr, 1, 0))) return rc;
+    double fid, fext, fexc;
+    if ((rc = finish_sums(h, &fid, &fext, &fexc))) return rc;
+    double f0 = 0.0;
+    f0 = f0 + fid + fext;
+    f0 = f0 + fexc;
+    const double pbulk = f0 / (g.lx * g.ly * g.lz);
+    const double pmv = -deltaN / g.n0 * pbulk;
+    out[0] = ftot + pmv + lj_tail;
+    out[1] = pmv;
+    out[2] = pbulk;
+    out[3] = deltaN;
+    return MDFT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdft_pressure_correction(mdft_handle *h, const double *xi, double ftot, double lj_tail, double *out) {
+    if (!h || !xi || !out) { set_error("null argument"); return MDFT_E_ARG; }
+    const size_t nf = (size_t)h->g.N * h->g.no;
+    int rc = lbfgs_alloc(h, h->lb.m > 0 ? h->lb.m : 1);
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(h->lb.x.p, xi, nf * 8, cudaMemcpyHostToDevice, h->stream), "xi upload"))) return rc;
+    return pressure_impl(h, h->lb.x.p, ftot, lj_tail, out);
+}
+
+int mdft_pressure_correction_device(mdft_handle *h, const double *d_xi, double ftot, double lj_tail, double *out) {
+    if (!h || !d_xi || !out) { set_error("null argument"); return MDFT_E_ARG; }
+    return pressure_impl(h, d_xi, ftot, lj_tail, out);
+}
+
+int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, const double *eps, const double *xyz, int nsv,
+               const double *sq, const double *ssig, const double *seps, const double *sxyz, double rvdw, double eps_r,
+               const mdft_minimize_opts *o, double *xi_out, double *out, mdft_minimize_result *res) {
+    if (!h || !o || !out || !res || nsv <= 0 || !sq || !sxyz) { set_error("null argument"); return MDFT_E_ARG; }
+    int rc = check_min_opts(o);
+    if (rc) return rc;
+    double lj = 0.0;
+    if ((rc = mdft_compute_vext(h, nsite, q, sig, eps, xyz, nsv, sq, ssig, seps, sxyz, rvdw, &lj))) return rc;
+    // charged-solute corrections (src/module_energy_and_gradient.f90:191-204,281-344)
+    double qnet = 0.0, quad = 0.0;
+    for (int s = 0; s < nsite; ++s) qnet += q[s];
+    for (int s = 0; s < nsv; ++s)
+        quad += sq[s] * (sxyz[3 * s] * sxyz[3 * s] + sxyz[3 * s + 1] * sxyz[3 * s + 1] + sxyz[3 * s + 2] * sxyz[3 * s + 2]);
+    double corr = 0.0;
+    if (std::fabs(qnet) > 1e-7) {
+        const Grid &g = h->g;
+        double L = (g.lx == g.ly && g.ly == g.lz) ? g.lx : (g.lx + g.ly + g.lz) / 3.0;
+        corr = -1971.01 * qnet * qnet / L * (1 - 1.0 / eps_r);
+        corr = corr + (0.0 - quad * g.n0 * 2909.857 * qnet);
+    }
+    h->const_corr = corr;
+    if ((rc = lbfgs_alloc(h, o->m))) return rc;
+    LbfgsState &L = h->lb;
+    const double vmax = (-std::log(kEpsDp) - (double)0.05f) * h->g.kT;
+    k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, L.x.p, vmax, L.n);
+    h->launches += 1;
+    if ((rc = minimize_impl(h, o, res))) return rc;
+    double pc[4];
+    if ((rc = pressure_impl(h, L.x.p, res->f, lj, pc))) return rc;
+    out[0] = pc[0];
+    out[1] = res->f;
+    out[2] = pc[1];
+    out[3] = lj;
+    out[4] = pc[2];
+    out[5] = pc[3];
+    if (xi_out) {
+        if ((rc = check_cuda(cudaMemcpyAsync(xi_out, L.x.p, L.n * 8, cudaMemcpyDeviceToHost, h->stream), "xi download"))) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "xi download"))) return rc;
+    }
+    return MDFT_OK;
+}
+
+}  // extern "C"

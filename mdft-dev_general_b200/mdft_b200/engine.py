@@ -1,0 +1,287 @@
+"""ctypes binding of libmdft_b200.so, mirroring the reference's host calls.
+
+Reference interface (Fortran, dborgis/mdft-dev_general):
+  energy_and_gradient(f, df)            src/module_energy_and_gradient.f90:36
+  excess_energy(ff, df, print_timers)   src/module_proc_ptrs.f90:3-21
+  init_vext                             src/module_vext.f90:14-115
+  guess_density                         src/module_density.f90:267-284
+  minimization_using_lbfgs              src/energy_minimization.f90:232-290
+  pressure_correction                   src/module_pressure_correction.f90:7-156
+
+Arrays use the reference layout xi(no, nx, ny, nz) with io fastest, i.e. numpy
+shape (nz, ny, nx, no) in C order.  Errors raise MdftError carrying the
+library's message (the reference would `error stop`).  There is no CPU path:
+without the compiled library (or without a GPU) construction fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def library_path() -> str:
+    return os.path.join(_PKG, "libmdft_b200.so")
+
+
+class MdftError(RuntimeError):
+    pass
+
+
+class _Desc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("mmax", C.c_int), ("mrso", C.c_int), ("temperature", C.c_double), ("n0", C.c_double),
+                ("ck_path", C.c_char_p), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class _Sizes(C.Structure):
+    _fields_ = [("ntheta", C.c_int), ("nphi", C.c_int), ("npsi", C.c_int), ("no", C.c_int), ("np", C.c_int),
+                ("ncoef", C.c_int), ("nq", C.c_int), ("dv", C.c_double), ("rho0", C.c_double), ("kT", C.c_double),
+                ("dq", C.c_double)]
+
+
+class _MinOpts(C.Structure):
+    _fields_ = [("m", C.c_int), ("pgtol", C.c_double), ("ftol_abs", C.c_double), ("itermax", C.c_int),
+                ("precision", C.c_int)]
+
+
+class _MinRes(C.Structure):
+    _fields_ = [("f", C.c_double), ("pgnorm", C.c_double), ("iterations", C.c_int), ("evaluations", C.c_int),
+                ("status", C.c_int)]
+
+
+_DP = C.POINTER(C.c_double)
+
+# every entry point declared in include/mdft_b200.h: name -> (restype, argtypes)
+SIGNATURES = {
+    "mdft_create": (C.c_int, [C.POINTER(_Desc), C.POINTER(C.c_void_p)]),
+    "mdft_destroy": (C.c_int, [C.c_void_p]),
+    "mdft_last_error": (C.c_char_p, []),
+    "mdft_get_sizes": (C.c_int, [C.c_void_p, C.POINTER(_Sizes)]),
+    "mdft_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mdft_get_weights": (C.c_int, [C.c_void_p, _DP]),
+    "mdft_set_vext": (C.c_int, [C.c_void_p, _DP]),
+    "mdft_get_vext": (C.c_int, [C.c_void_p, _DP]),
+    "mdft_set_constant_correction": (C.c_int, [C.c_void_p, C.c_double]),
+    "mdft_energy_and_gradient": (C.c_int, [C.c_void_p, _DP, _DP, _DP, _DP]),
+    "mdft_energy_and_gradient_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _DP, _DP]),
+    "mdft_excess_energy": (C.c_int, [C.c_void_p, _DP, _DP, _DP]),
+    "mdft_compute_vext": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP,
+                                    C.c_double, _DP]),
+    "mdft_guess_density": (C.c_int, [C.c_void_p, _DP]),
+    "mdft_minimize": (C.c_int, [C.c_void_p, _DP, C.POINTER(_MinOpts), C.POINTER(_MinRes)]),
+    "mdft_guess_density_device": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mdft_minimize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_MinOpts), C.POINTER(_MinRes)]),
+    "mdft_get_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "mdft_pressure_correction": (C.c_int, [C.c_void_p, _DP, C.c_double, C.c_double, _DP]),
+    "mdft_pressure_correction_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, _DP]),
+    "mdft_solve": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP, C.c_double,
+                             C.c_double, C.POINTER(_MinOpts), _DP, _DP, C.POINTER(_MinRes)]),
+    "mdft_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "mdft_get_stage_times": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int)]),
+}
+
+
+def lib():
+    """Load libmdft_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise MdftError("libmdft_b200.so is not built; run __graft_entry__.build() or mdft_b200/build.py")
+        L = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_DP)
+
+
+def _check(rc):
+    if rc != 0:
+        raise MdftError("%s (code %d)" % (lib().mdft_last_error().decode(errors="replace"), rc))
+
+
+class Engine:
+    """One MDFT system on one GPU (grid, solvent, c(k), vext, device buffers)."""
+
+    def __init__(self, n, box, mmax, ck_path, temperature=298.0, n0=0.0333, mrso=2, precision=PREC_FP64, device=0):
+        nx, ny, nz = (n, n, n) if np.isscalar(n) else tuple(n)
+        lx, ly, lz = (box, box, box) if np.isscalar(box) else tuple(box)
+        self._ck = os.fsencode(ck_path)
+        d = _Desc(nx, ny, nz, lx, ly, lz, mmax, mrso, temperature, n0, self._ck, precision, device)
+        h = C.c_void_p()
+        _check(lib().mdft_create(C.byref(d), C.byref(h)))
+        self.h = h
+        s = _Sizes()
+        _check(lib().mdft_get_sizes(self.h, C.byref(s)))
+        self.sizes = s
+        self.no, self.np = s.no, s.np
+        self.dims = (nx, ny, nz)
+        self.box = (lx, ly, lz)
+        self.shape = (nz, ny, nx, s.no)
+        self.dv, self.rho0, self.kT = s.dv, s.rho0, s.kT
+        self.lj_tail = 0.0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mdft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state -------------------------------------------------------------
+    @property
+    def weights(self):
+        w = np.zeros(self.no)
+        _check(lib().mdft_get_weights(self.h, _p(w)))
+        return w
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().mdft_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def set_vext(self, vext):
+        v = np.ascontiguousarray(vext, dtype=np.float64).reshape(self.shape)
+        _check(lib().mdft_set_vext(self.h, _p(v)))
+
+    def get_vext(self):
+        v = np.empty(self.shape)
+        _check(lib().mdft_get_vext(self.h, _p(v)))
+        return v
+
+    def set_constant_correction(self, c: float):
+        _check(lib().mdft_set_constant_correction(self.h, float(c)))
+
+    # -- the hot path --------------------------------------------------------
+    def energy_and_gradient(self, xi, want_grad=True, df_out=None):
+        """Return (f, df, terms) with terms = [F_id, F_ext, F_exc, correction]; df = dF/dxi / dv."""
+        x = np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        f = np.zeros(1)
+        terms = np.zeros(4)
+        df = None
+        if want_grad:
+            df = df_out if df_out is not None else np.empty(self.shape)
+        _check(lib().mdft_energy_and_gradient(self.h, _p(x), _p(f), _p(df), _p(terms)))
+        return float(f[0]), df, terms
+
+    def energy_and_gradient_device(self, xi_ptr: int, df_ptr: int | None):
+        f = np.zeros(1)
+        terms = np.zeros(4)
+        _check(lib().mdft_energy_and_gradient_device(self.h, C.c_void_p(xi_ptr), C.c_void_p(df_ptr or 0), _p(f), _p(terms)))
+        return float(f[0]), terms
+
+    def excess_energy(self, xi, df=None):
+        """Excess term alone; df (if given) is accumulated into, as the reference does."""
+        x = np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        f = np.zeros(1)
+        if df is not None:
+            assert df.flags.c_contiguous and df.dtype == np.float64 and df.size == x.size
+        _check(lib().mdft_excess_energy(self.h, _p(x), _p(f), _p(df)))
+        return float(f[0])
+
+    # -- set-up and callers ---------------------------------------------------
+    def compute_vext(self, solute, solvent, rvdw=10.0):
+        q = np.ascontiguousarray(solute.q, dtype=np.float64)
+        sg = np.ascontiguousarray(solute.sig, dtype=np.float64)
+        ep = np.ascontiguousarray(solute.eps, dtype=np.float64)
+        xyz = np.ascontiguousarray(solute.xyz, dtype=np.float64)
+        vq = np.array(solvent.q, dtype=np.float64)
+        vs = np.array(solvent.sig, dtype=np.float64)
+        ve = np.array(solvent.eps, dtype=np.float64)
+        vx = np.array(solvent.xyz, dtype=np.float64)
+        lj = np.zeros(1)
+        _check(lib().mdft_compute_vext(self.h, len(q), _p(q), _p(sg), _p(ep), _p(xyz), len(vq), _p(vq), _p(vs),
+                                       _p(ve), _p(vx), float(rvdw), _p(lj)))
+        self.lj_tail = float(lj[0])
+        return self.lj_tail
+
+    def guess_density(self):
+        xi = np.empty(self.shape)
+        _check(lib().mdft_guess_density(self.h, _p(xi)))
+        return xi
+
+    def minimize(self, xi, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64):
+        x = np.array(xi, dtype=np.float64, copy=True).reshape(self.shape)
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
+        r = _MinRes()
+        _check(lib().mdft_minimize(self.h, _p(x), C.byref(o), C.byref(r)))
+        return x, dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status)
+
+    def guess_density_device(self, d_xi: int):
+        _check(lib().mdft_guess_density_device(self.h, C.c_void_p(d_xi)))
+
+    def minimize_device(self, d_xi: int, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64):
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
+        r = _MinRes()
+        _check(lib().mdft_minimize_device(self.h, C.c_void_p(d_xi), C.byref(o), C.byref(r)))
+        return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status)
+
+    @property
+    def launch_count(self) -> int:
+        c = C.c_longlong()
+        _check(lib().mdft_get_launch_count(self.h, C.byref(c)))
+        return c.value
+
+    def pressure_correction(self, xi, ftot, lj_tail=None):
+        x = np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        out = np.zeros(4)
+        _check(lib().mdft_pressure_correction(self.h, _p(x), float(ftot),
+                                              float(self.lj_tail if lj_tail is None else lj_tail), _p(out)))
+        return dict(dG=out[0], pmv=out[1], pbulk=out[2], deltaN=out[3])
+
+    def solve(self, solute, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
+              xi_out=None):
+        """vext -> guess_density -> L-BFGS -> pressure correction for one solute (main.f90's flow)."""
+        q = np.ascontiguousarray(solute.q, dtype=np.float64)
+        sg = np.ascontiguousarray(solute.sig, dtype=np.float64)
+        ep = np.ascontiguousarray(solute.eps, dtype=np.float64)
+        xyz = np.ascontiguousarray(solute.xyz, dtype=np.float64)
+        vq = np.array(solvent.q, dtype=np.float64)
+        vs = np.array(solvent.sig, dtype=np.float64)
+        ve = np.array(solvent.eps, dtype=np.float64)
+        vx = np.array(solvent.xyz, dtype=np.float64)
+        if xi_out is not None:
+            assert xi_out.dtype == np.float64 and xi_out.flags.c_contiguous and xi_out.size == int(np.prod(self.shape))
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
+        r = _MinRes()
+        out = np.zeros(6)
+        _check(lib().mdft_solve(self.h, len(q), _p(q), _p(sg), _p(ep), _p(xyz), len(vq), _p(vq), _p(vs), _p(ve), _p(vx),
+                                float(rvdw), float(solvent.eps_r), C.byref(o), _p(xi_out), _p(out), C.byref(r)))
+        self.lj_tail = float(out[3])
+        return dict(dG=out[0], f=out[1], pmv=out[2], lj_tail=out[3], pbulk=out[4], deltaN=out[5], pgnorm=r.pgnorm,
+                    iterations=r.iterations, evaluations=r.evaluations, status=r.status)
+
+    def set_timing(self, on=True):
+        _check(lib().mdft_set_timing(self.h, 1 if on else 0))
+
+    def stage_times(self):
+        ms = np.zeros(5)
+        cnt = C.c_int()
+        _check(lib().mdft_get_stage_times(self.h, _p(ms), C.byref(cnt)))
+        return dict(zip(("project", "fft_forward", "oz", "fft_inverse", "gather"), ms)), cnt.value

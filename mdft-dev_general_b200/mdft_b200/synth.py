@@ -189,7 +189,7 @@ def synthetic_ck(mmax: int, mrso: int = 2, n0: float = 0.0333, seed: int = 20260
     for khi in range(-mmax, mmax + 1):
         basis = [(m, mu) for m in range(abs(khi), mmax + 1) for mu in range(-(m // mrso) * mrso, m + 1, mrso)]
         blocks.append(np.array([[tindex[(m, n, mu, nu, khi)] for (n, nu) in basis] for (m, mu) in basis]))
-    kcheck = q[:: max(1, len(q) // 400)]
+    kcheck = np.arange(0.0, 50.0 + 1e-9, 0.125)  # fixed: the table values do not depend on kmax
     wvec = np.array([widths[orbit_key(t)] for t in tuples])
     vanish = np.array([t[2] != 0 or t[3] != 0 for t in tuples])
 

@@ -548,7 +548,7 @@ int orc_load_ck(orc *o, const char *path)
     const int mmax = o->mmax, mrso = o->mrso;
     int npl = npluc_of(mmax);
     if (npl < 0) { fclose(fp); set_err("no npluc for this mmax"); return -1; }
-    size_t cap = 1 << 16;
+    size_t cap = 1 << 23; /* mmax 5 rows are ~100 KB of text */
     char *line = malloc(cap);
     int lineno = 0;
     int *idx[5];

@@ -1,0 +1,116 @@
+"""CUDA engine vs the FP64 oracle, through the C-ABI (libmdft_b200.so).
+
+Tolerances (FP64 path): total energy <= 1e-10 relative, each term <= 1e-10
+of |F|, gradient max|df_gpu - df_oracle| <= 1e-8 * max|df_oracle|.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from mdft_b200 import Engine
+import cases
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+SV = cases.SOLVENT
+
+
+def pair(name, ckdir):
+    c = cases.CASES[name]
+    ck = cases.ck_path(ckdir, c["mmax"])
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    sol = cases.solute_of(c)
+    if sol is not None:
+        o.compute_vext(sol, SV, rvdw=c["rvdw"])
+    else:
+        o.set_vext(cases.random_vext(c, o.shape))
+    corr = cases.charge_correction(sol, c["L"])
+    o.set_const_corr(corr)
+    e.set_constant_correction(corr)
+    e.set_vext(o.get_vext())
+    return c, o, e, sol
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_energy_gradient_parity(tmp_path, name):
+    c, o, e, _ = pair(name, tmp_path)
+    xi = cases.xi_of(c, o.shape)
+    f0, df0, t0 = o.energy_grad(xi)
+    f1, df1, t1 = e.energy_and_gradient(xi)
+    assert abs(f1 - f0) <= 1e-10 * abs(f0), (f1, f0)
+    assert np.all(np.abs(t1 - t0) <= 1e-10 * abs(f0)), (t1, t0)
+    err = np.abs(df1 - df0).max() / np.abs(df0).max()
+    assert err <= 1e-8, err
+    g = np.load(os.path.join(GOLD, name + ".npz"))
+    assert abs(f1 - g["f"]) <= 1e-10 * abs(g["f"])
+    np.testing.assert_allclose(df1.reshape(-1)[g["idx"]], g["df_samples"], rtol=0, atol=1e-8 * np.abs(df0).max())
+    e.close()
+
+
+@pytest.mark.parametrize("name", ["mol16_m2", "rand12_m3"])
+def test_energy_only_and_excess_seam(tmp_path, name):
+    c, o, e, _ = pair(name, tmp_path)
+    xi = cases.xi_of(c, o.shape)
+    f0, df0, t0 = o.energy_grad(xi)
+    f1, _, t1 = e.energy_and_gradient(xi, want_grad=False)
+    assert abs(f1 - f0) <= 1e-10 * abs(f0)
+    # excess_energy accumulates into df like the reference's procedure pointer
+    base = np.random.default_rng(3).standard_normal(o.shape)
+    acc = base.copy()
+    fexc = e.excess_energy(xi, acc)
+    assert abs(fexc - t0[2]) <= 1e-10 * abs(f0)
+    w = e.weights
+    rho = xi ** 2 * e.rho0
+    dfid = np.where(rho > np.finfo(float).eps, w * 2 * e.rho0 * xi * (SV.kT * np.log(rho / e.rho0) + o.get_vext()), 0.0)
+    assert np.abs((acc - base) - (df0 - dfid)).max() <= 1e-8 * np.abs(df0).max()
+    e.close()
+
+
+@pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2", "mol24_m3", "mol8_m0"])
+def test_vext_parity(tmp_path, name):
+    c = cases.CASES[name]
+    ck = cases.ck_path(tmp_path, c["mmax"])
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    sol = cases.solute_of(c)
+    lj0 = o.compute_vext(sol, SV, rvdw=c["rvdw"])
+    lj1 = e.compute_vext(sol, SV, rvdw=c["rvdw"])
+    v0, v1 = o.get_vext(), e.get_vext()
+    assert abs(lj1 - lj0) <= 1e-12 * abs(lj0)
+    assert np.abs(v1 - v0).max() <= 1e-10 * np.abs(v0).max()
+    np.testing.assert_array_equal(e.guess_density(), o.guess_density())
+    e.close()
+
+
+def test_minimize_and_free_energy_parity(tmp_path):
+    # same solve on both sides; converged free energies agree to 1e-6 kJ/mol
+    c, o, e, sol = pair("ion16_m1", tmp_path)
+    lj = o.compute_vext(sol, SV, rvdw=c["rvdw"])
+    e.set_vext(o.get_vext())
+    x0 = o.guess_density()
+    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-9, tol=1e-12, itermax=400)
+    xg, r = e.minimize(x0, m=5, pgtol=1e-9, ftol_abs=1e-12, itermax=400)
+    assert sto in (0, 1) and r["status"] in (0, 1), (sto, r)
+    assert abs(r["f"] - fo) <= 1e-6, (r["f"], fo)
+    pg = e.pressure_correction(xg, r["f"], lj)
+    po = o.pressure_correction(xo, fo, lj)
+    assert abs(pg["dG"] - po["dG"]) <= 1e-6, (pg, po)
+    # the pressure correction itself on identical inputs
+    pg2 = e.pressure_correction(xo, fo, lj)
+    assert abs(pg2["dG"] - po["dG"]) <= 1e-9 * max(1.0, abs(po["dG"]))
+    e.close()
+
+
+def test_first_iterations_follow_the_oracle(tmp_path):
+    # a short solve: identical algorithm, so the iterates track each other closely
+    c, o, e, _ = pair("mol16_m2", tmp_path)
+    x0 = o.guess_density()
+    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-12, tol=-1.0, itermax=5)
+    xg, r = e.minimize(x0, m=5, pgtol=1e-12, ftol_abs=-1.0, itermax=5)
+    assert r["iterations"] == ito and r["evaluations"] == nfo
+    assert abs(r["f"] - fo) <= 1e-9 * abs(fo)
+    assert np.abs(xg - xo).max() <= 1e-7
+    e.close()
