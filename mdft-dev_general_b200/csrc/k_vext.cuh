@@ -26,8 +26,11 @@ struct LJArgs {
     int only_origin;
 };
 
-__device__ __forceinline__ bool in_ranges(const LJTerm &t, int ax, int i) {
-    return (i >= t.lo[ax][0] && i <= t.hi[ax][0]) || (i >= t.lo[ax][1] && i <= t.hi[ax][1]);
+// How many times node index i occurs in the site's index table along one axis.
+// The reference's wrapped table [1..max] ++ [min..n] holds one node twice when
+// min == max (a cut-off cube as wide as the box); that node then gets the term twice.
+__device__ __forceinline__ int multiplicity(const LJTerm &t, int ax, int i) {
+    return (int)(i >= t.lo[ax][0] && i <= t.hi[ax][0]) + (int)(i >= t.lo[ax][1] && i <= t.hi[ax][1]);
 }
 
 __device__ __forceinline__ double pbc_dist(double d, double L) {
@@ -55,8 +58,8 @@ __global__ void k_lj(double *__restrict__ vext, const LJTerm *__restrict__ terms
         double v = vext[pt * a.no + io];
         for (int u = 0; u < a.nterm; ++u) {
             const LJTerm t = terms[u];
-            if (!in_ranges(t, 0, ix) || !in_ranges(t, 1, iy) || !in_ranges(t, 2, iz)) continue;
-            if (v > 1.e5) continue;
+            const int visits = multiplicity(t, 0, ix) * multiplicity(t, 1, iy) * multiplicity(t, 2, iz);
+            if (visits == 0) continue;
             double xs = xg, ys = yg, zs = zg;
             if (!a.only_origin) {
                 const double *R = rotm + 9 * io;
@@ -66,7 +69,9 @@ __global__ void k_lj(double *__restrict__ vext, const LJTerm *__restrict__ terms
             }
             double ddx = pbc_dist(xs - t.px, a.lx), ddy = pbc_dist(ys - t.py, a.ly), ddz = pbc_dist(zs - t.pz, a.lz);
             double rsq = ddx * ddx + ddy * ddy + ddz * ddz;
-            v = v + lj_value(rsq, a.cutoffsq, t.epsuv, t.siguv6);
+            const double vlj = lj_value(rsq, a.cutoffsq, t.epsuv, t.siguv6);
+            for (int k = 0; k < visits; ++k)
+                if (!(v > 1.e5)) v = v + vlj;  // nodes already above 1e5 are skipped
         }
         if (a.only_origin)
             for (int k = 0; k < a.no; ++k) vext[pt * a.no + k] = v;

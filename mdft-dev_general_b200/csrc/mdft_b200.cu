@@ -94,6 +94,15 @@ int alloc_check(cudaError_t e, const char *what, size_t bytes) {
     return check_cuda(e, what);
 }
 
+// Let `fn` use all opt-in shared memory that its static allocation leaves.
+int allow_smem(const void *fn, int optin) {
+    cudaFuncAttributes at{};
+    int rc = check_cuda(cudaFuncGetAttributes(&at, fn), "cudaFuncGetAttributes");
+    if (rc) return rc;
+    return check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)at.sharedSizeBytes),
+                      "cudaFuncSetAttribute");
+}
+
 int upload_twiddles(DevBuf<double2> &buf, int n) {
     std::vector<double2> h(n);
     for (int t = 0; t < n; ++t) {
@@ -307,18 +316,17 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     // launch shapes
     int maxsmem = 0;
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device);
-    h->bm_project = project_smem_bytes(64, g.no) <= (size_t)maxsmem ? 64 : 32;
-    h->bm_gather = gather_smem_bytes(64, g.np) <= (size_t)maxsmem ? 64 : 32;
-    if (project_smem_bytes(h->bm_project, g.no) > (size_t)maxsmem || gather_smem_bytes(h->bm_gather, g.np) > (size_t)maxsmem) {
+    const size_t dyn_max = (size_t)maxsmem - 1024;  // static shared memory of these kernels is < 1 KB
+    h->bm_project = project_smem_bytes(64, g.no) <= dyn_max ? 64 : 32;
+    h->bm_gather = gather_smem_bytes(64, g.np) <= dyn_max ? 64 : 32;
+    if (project_smem_bytes(h->bm_project, g.no) > dyn_max || gather_smem_bytes(h->bm_gather, g.np) > dyn_max) {
         set_error("angular transform tiles do not fit in shared memory");
         return MDFT_E_ARG;
     }
-    cudaFuncSetAttribute(k_project_f64<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
-    cudaFuncSetAttribute(k_project_f64<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
-    cudaFuncSetAttribute(k_gather_f64<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
-    cudaFuncSetAttribute(k_gather_f64<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
-    cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
-    cudaFuncSetAttribute(k_oz_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsmem);
+    if ((rc = allow_smem((const void *)k_project_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_project_f64<32>, maxsmem)) ||
+        (rc = allow_smem((const void *)k_gather_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_gather_f64<32>, maxsmem)) ||
+        (rc = allow_smem((const void *)k_fft_axis<double>, maxsmem)) || (rc = allow_smem((const void *)k_oz_f64, maxsmem)))
+        return rc;
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
     h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
     if ((rc = alloc_check(h->partial.alloc(3 * (size_t)h->nblk_gather), "partials", 24 * h->nblk_gather))) return rc;

@@ -1143,7 +1143,8 @@ int orc_vext(orc *o, int nsol, const double *sq, const double *ssig, const doubl
             double epsuv = sqrt(seps[u] * veps[ss]);
             double siguv6 = ipow((ssig[u] + vsig[ss]) * 0.5, 6);
             ljcorr = ljcorr - (16.0 * 3.14159 / 3.0) * epsuv * siguv6 * o->n0 / ipow(cutoff, 3);
-#pragma omp parallel for
+            /* Serial on purpose: when the cut-off cube is as wide as the box the z table holds
+               one node twice, and the reference's OpenMP loop over it races on that node. */
             for (int iz_ = 0; iz_ < zuse; ++iz_) {
                 int iz = ztab[iz_] - 1;
                 double zg = (double)iz * gdz;

@@ -85,16 +85,18 @@ def test_vext_parity(tmp_path, name):
     e.close()
 
 
-def test_minimize_and_free_energy_parity(tmp_path):
-    # same solve on both sides; converged free energies agree to 1e-6 kJ/mol
-    c, o, e, sol = pair("ion16_m1", tmp_path)
+def test_minimize_trajectory_parity(tmp_path):
+    # same algorithm on both sides: after a fixed number of L-BFGS iterations the iterates,
+    # F and the solvation free energy agree (dG to 1e-6 kJ/mol)
+    c, o, e, sol = pair("mol16_m2", tmp_path)
     lj = o.compute_vext(sol, SV, rvdw=c["rvdw"])
     e.set_vext(o.get_vext())
     x0 = o.guess_density()
-    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-9, tol=1e-12, itermax=400)
-    xg, r = e.minimize(x0, m=5, pgtol=1e-9, ftol_abs=1e-12, itermax=400)
-    assert sto in (0, 1) and r["status"] in (0, 1), (sto, r)
-    assert abs(r["f"] - fo) <= 1e-6, (r["f"], fo)
+    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-12, tol=-1.0, itermax=25)
+    xg, r = e.minimize(x0, m=5, pgtol=1e-12, ftol_abs=-1.0, itermax=25)
+    assert (r["iterations"], r["evaluations"], r["status"]) == (ito, nfo, sto)
+    assert abs(r["f"] - fo) <= 1e-9 * abs(fo)
+    assert np.abs(xg - xo).max() <= 1e-6
     pg = e.pressure_correction(xg, r["f"], lj)
     po = o.pressure_correction(xo, fo, lj)
     assert abs(pg["dG"] - po["dG"]) <= 1e-6, (pg, po)
@@ -104,13 +106,41 @@ def test_minimize_and_free_energy_parity(tmp_path):
     e.close()
 
 
-def test_first_iterations_follow_the_oracle(tmp_path):
-    # a short solve: identical algorithm, so the iterates track each other closely
-    c, o, e, _ = pair("mol16_m2", tmp_path)
+@pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2"])
+def test_minimize_converged_parity(tmp_path, name):
+    # converged solves (max|df| <= 1e-6, F decrease <= 1e-9): the functional agrees to 1e-9
+    # relative; dG agrees to 1e-4 kJ/mol, the spread the oracle itself shows between
+    # stopping points of this flat minimum
+    c, o, e, sol = pair(name, tmp_path)
+    lj = o.compute_vext(sol, SV, rvdw=c["rvdw"])
+    e.set_vext(o.get_vext())
     x0 = o.guess_density()
-    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-12, tol=-1.0, itermax=5)
-    xg, r = e.minimize(x0, m=5, pgtol=1e-12, ftol_abs=-1.0, itermax=5)
-    assert r["iterations"] == ito and r["evaluations"] == nfo
-    assert abs(r["f"] - fo) <= 1e-9 * abs(fo)
-    assert np.abs(xg - xo).max() <= 1e-7
+    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-6, tol=1e-9, itermax=2000)
+    xg, r = e.minimize(x0, m=5, pgtol=1e-6, ftol_abs=1e-9, itermax=2000)
+    assert r["status"] in (0, 1, 2) and sto in (0, 1, 2)
+    assert abs(r["f"] - fo) <= 1e-9 * abs(fo), (r, fo)
+    pg = e.pressure_correction(xg, r["f"], lj)
+    po = o.pressure_correction(xo, fo, lj)
+    assert abs(pg["dG"] - po["dG"]) <= 1e-4, (pg, po)
     e.close()
+
+
+def test_solve_entry_point(tmp_path):
+    # mdft_solve (vext -> guess -> L-BFGS -> pressure correction) equals the step-by-step calls
+    c = cases.CASES["ion16_m1"]
+    ck = cases.ck_path(tmp_path, c["mmax"])
+    sol = cases.solute_of(c)
+    e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    xi = np.empty(e.shape)
+    res = e.solve(sol, SV, rvdw=c["rvdw"], m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=500, xi_out=xi)
+    e2 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    lj = e2.compute_vext(sol, SV, rvdw=c["rvdw"])
+    e2.set_constant_correction(cases.charge_correction(sol, c["L"]))
+    x2, r2 = e2.minimize(e2.guess_density(), m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=500)
+    p2 = e2.pressure_correction(x2, r2["f"], lj)
+    assert res["iterations"] == r2["iterations"] and res["evaluations"] == r2["evaluations"]
+    assert abs(res["f"] - r2["f"]) <= 1e-12 * abs(r2["f"])
+    assert abs(res["dG"] - p2["dG"]) <= 1e-9 * abs(p2["dG"])
+    np.testing.assert_array_equal(xi, x2)
+    e.close()
+    e2.close()
