@@ -33,6 +33,10 @@
 
 typedef double complex cplx;
 
+/* Reductions sum ORC_NCHUNK fixed chunks in order, so results do not depend on
+   the number of OpenMP threads. */
+#define ORC_NCHUNK 64
+
 #define ORC_PI 3.14159265358979323846264338327950288
 static const double EPSDP = 2.220446049250313080847263336181640625e-16; /* epsilon(1._dp) */
 static const double EPSSP = 1.1920928955078125e-07;                     /* epsilon(1.)    */
@@ -908,13 +912,15 @@ static int excess(orc *o, const double *xi, double *fexc, double *df)
     /* S7 gather + energy + gradient :728-762 */
     const double fourpisq = 4.0 * ORC_PI * ORC_PI;
     const double prefactor = -o->kT * 2.0 * fourpisq / o->mrso / o->n0;
-    double ff = 0.0;
-#pragma omp parallel reduction(+ : ff)
+    double pff[ORC_NCHUNK];
+#pragma omp parallel
     {
         double *vexc = malloc(sizeof(double) * no);
         cplx *ft = malloc(sizeof(cplx) * o->ntheta * o->nmu2 * (2 * o->mmax + 1));
 #pragma omp for
-        for (long r = 0; r < N; ++r) {
+        for (int ch = 0; ch < ORC_NCHUNK; ++ch) {
+          double ff = 0.0;
+          for (long r = N * ch / ORC_NCHUNK; r < N * (ch + 1) / ORC_NCHUNK; ++r) {
             proj2angl_pt(o, drho + r * np, vexc, ft);
             double s = 0;
             for (int io = 0; io < no; ++io) {
@@ -924,10 +930,14 @@ static int excess(orc *o, const double *xi, double *fexc, double *df)
                 if (df) df[r * no + io] = df[r * no + io] + 2.0 * rho0 * x * v;
             }
             ff += s;
+          }
+          pff[ch] = ff;
         }
         free(vexc);
         free(ft);
     }
+    double ff = 0.0;
+    for (int ch = 0; ch < ORC_NCHUNK; ++ch) ff += pff[ch];
     *fexc = ff * 0.5 * o->dv;
     return 0;
 }
@@ -937,9 +947,11 @@ static void ideal_and_external(const orc *o, const double *xi, double *fid, doub
 {
     const double kT = o->kT, dv = o->dv, rho0 = o->rho0;
     const int no = o->no;
-    double a = 0, b = 0;
-#pragma omp parallel for reduction(+ : a, b)
-    for (long r = 0; r < o->N; ++r)
+    double pa[ORC_NCHUNK], pb[ORC_NCHUNK];
+#pragma omp parallel for
+    for (int ch = 0; ch < ORC_NCHUNK; ++ch) {
+      double a = 0, b = 0;
+      for (long r = o->N * ch / ORC_NCHUNK; r < o->N * (ch + 1) / ORC_NCHUNK; ++r)
         for (int io = 0; io < no; ++io) {
             long i = r * no + io;
             double x = xi[i], rho = x * x * rho0;
@@ -951,6 +963,11 @@ static void ideal_and_external(const orc *o, const double *xi, double *fid, doub
                 a += kT * dv * o->w[io] * rho0;
             }
         }
+      pa[ch] = a;
+      pb[ch] = b;
+    }
+    double a = 0, b = 0;
+    for (int ch = 0; ch < ORC_NCHUNK; ++ch) { a += pa[ch]; b += pb[ch]; }
     *fid = a;
     *fext = b;
 }
@@ -1376,9 +1393,15 @@ static int dcsrch(double f, double g, double *stp, double ftol, double gtol, dou
 /* col=0 gives z = x - g/theta.                                               */
 static double ddot_(long n, const double *a, const double *b)
 {
+    double part[ORC_NCHUNK];
+#pragma omp parallel for
+    for (int ch = 0; ch < ORC_NCHUNK; ++ch) {
+        double s = 0;
+        for (long i = n * ch / ORC_NCHUNK; i < n * (ch + 1) / ORC_NCHUNK; ++i) s += a[i] * b[i];
+        part[ch] = s;
+    }
     double s = 0;
-#pragma omp parallel for reduction(+ : s)
-    for (long i = 0; i < n; ++i) s += a[i] * b[i];
+    for (int ch = 0; ch < ORC_NCHUNK; ++ch) s += part[ch];
     return s;
 }
 static double amax_(long n, const double *a)

@@ -108,20 +108,21 @@ def test_minimize_trajectory_parity(tmp_path):
 
 @pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2"])
 def test_minimize_converged_parity(tmp_path, name):
-    # converged solves (max|df| <= 1e-6, F decrease <= 1e-9): the functional agrees to 1e-9
-    # relative; dG agrees to 1e-4 kJ/mol, the spread the oracle itself shows between
-    # stopping points of this flat minimum
+    # Solves run as far as FP64 allows (max|df| <= 1e-10 asked, F test off; the line search
+    # stops at F's rounding floor, status 2).  The functional agrees to 1e-10 relative; dG,
+    # which depends on the density to first order, agrees to 2e-4 kJ/mol: the spread the
+    # oracle itself shows between such stopping points of this flat minimum.
     c, o, e, sol = pair(name, tmp_path)
     lj = o.compute_vext(sol, SV, rvdw=c["rvdw"])
     e.set_vext(o.get_vext())
     x0 = o.guess_density()
-    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-6, tol=1e-9, itermax=2000)
-    xg, r = e.minimize(x0, m=5, pgtol=1e-6, ftol_abs=1e-9, itermax=2000)
-    assert r["status"] in (0, 1, 2) and sto in (0, 1, 2)
-    assert abs(r["f"] - fo) <= 1e-9 * abs(fo), (r, fo)
+    xo, fo, nfo, ito, sto = o.minimize(x0, m=5, pgtol=1e-10, tol=-1.0, itermax=1000)
+    xg, r = e.minimize(x0, m=5, pgtol=1e-10, ftol_abs=-1.0, itermax=1000)
+    assert r["status"] in (0, 2) and sto in (0, 2)
+    assert abs(r["f"] - fo) <= 1e-10 * abs(fo), (r, fo)
     pg = e.pressure_correction(xg, r["f"], lj)
     po = o.pressure_correction(xo, fo, lj)
-    assert abs(pg["dG"] - po["dG"]) <= 1e-4, (pg, po)
+    assert abs(pg["dG"] - po["dG"]) <= 2e-4, (pg, po)
     e.close()
 
 
