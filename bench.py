@@ -5,8 +5,8 @@ Workload (one "step" = one solute solved end to end): a seeded 24-site neutral
 solute (random walk, 1.4-1.6 A bonds inside 6 A, sigma U[2.5,3.8], eps
 U[0.2,1.0], q ~ N(0,0.3) shifted to 0) in SPC/E-like 3-site water, 64^3 grid,
 32 A box, mmax 3, synthetic c(k); vext (LJ + Poisson) -> guess_density ->
-L-BFGS (m=5, stop at max|df| <= 1e-6 or an F decrease <= 1e-3) -> pressure
-correction -> dG.  Synthetic inputs stand in for the reference's data.
+L-BFGS (m=5, stop at max|df| <= 1e-6; the reference's F-decrease test is
+off, it stops ~1 kJ/mol short of the converged dG) -> pressure correction -> dG.  Synthetic inputs stand in for the reference's data.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -207,7 +207,7 @@ def main():
     eng = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local)
     stream = torch.cuda.ExternalStream(eng.stream)
     sols = [solute(10_000 * rank + i, box) for i in range(args.warmup + args.steps)]
-    opts = dict(m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=2000)
+    opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000)
 
     def barrier():
         if world > 1:
@@ -290,7 +290,7 @@ def main():
                 "config": {"workload": "%d^3 grid, %g A box, mmax %d, %d-site random-walk solute per step, synthetic c(k)"
                                        % (n, box, MMAX, NSITE),
                            "form": "plain FP64 (vext + guess + L-BFGS m=5 + pressure correction)",
-                           "stop": "max|df|<=1e-6 or F decrease<=1e-3", "l2": "inputs larger than L2 (176 MB per field)",
+                           "stop": "max|df|<=1e-6 (line-search stall accepted)", "l2": "inputs larger than L2 (176 MB per field)",
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "evaluations_per_solve": evals, "dG": [r["dG"] for r in timed],
                            "dG_error_vs_fp64": 0.0},

@@ -150,7 +150,7 @@ def _symmetrise(tuples, vals, sign_tab):
 
 def synthetic_ck(mmax: int, mrso: int = 2, n0: float = 0.0333, seed: int = 20260000,
                  kmax: float = 50.0, dk: float = 0.01, eta: float = 0.45, sigma: float = 2.8,
-                 amp: float = 0.2, margin: float = 0.1):
+                 amp: float = 0.2, margin: float = 0.5):
     """Return (q, tuples, values[nq, ntuple]) of a synthetic c^{mn}_{mu nu khi}(k).
 
     c000 = n0 * c_PY(k).  Every other projection is a_t g_t(k) with
