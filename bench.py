@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="small grid smoke run (not a bench number)")
+    ap.add_argument("--evals", type=int, default=0,
+                    help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
     return ap.parse_args()
 
 
@@ -207,6 +209,15 @@ def main():
     eng = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local)
     stream = torch.cuda.ExternalStream(eng.stream)
     sols = [solute(10_000 * rank + i, box) for i in range(args.warmup + args.steps)]
+    if args.evals:
+        # profiling mode: the same workload's evaluations at the guess density of the first solute
+        eng.compute_vext(sols[0], sv, rvdw=rvdw)
+        xi0 = eng.guess_density()
+        for _ in range(args.evals):
+            f, _, terms = eng.energy_and_gradient(xi0)
+        print(json.dumps({"evals": args.evals, "f": f, "terms": list(map(float, terms))}))
+        eng.close()
+        return
     opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000)
 
     def barrier():

@@ -174,6 +174,23 @@ int mdft_pressure_correction_device(mdft_handle *h, const double *d_xi, double f
 int mdft_set_timing(mdft_handle *h, int on);
 int mdft_get_stage_times(const mdft_handle *h, double *ms5, int *count);
 
+/* Ideal + external term without any device allocation (no counterpart in the
+ * reference).  For callers that may not allocate GPU memory: a Fortran or C host that
+ * embeds the engine inside a program whose own pool owns every device allocation, or a
+ * time-critical loop that must not change the device's memory footprint.  Inputs and
+ * outputs stay the caller's device buffers: xi and vext (npoints*no doubles, io
+ * fastest), w (no doubles), df (may be NULL; receives the id+ext gradient, divided by dv
+ * like the reference's df), out (2 doubles: F_id, F_ext).  Work is queued on `stream`
+ * (a cudaStream_t, NULL for the default stream); nothing is synchronised.  The
+ * per-block partial sums go to a fixed 256 KB array inside the library, one per GPU that
+ * loads it, held until the process exits, so npoints is limited to 1,048,576 (larger
+ * sizes return MDFT_E_ARG with a message).  The first call on a device looks up that
+ * array's device address; make that first call before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Same arithmetic as src/module_energy_ideal_and_external.f90:46-73. */
+int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const double *d_w, int no, long long npoints,
+                                double kT, double rho0, double dv, double *d_df, double *d_out, void *stream);
+
 /* Number of kernels this handle has launched since creation. */
 int mdft_get_launch_count(const mdft_handle *h, long long *count);
 

@@ -1,0 +1,138 @@
+// Ideal + external term with no device allocation: the per-block partial sums
+// live in a fixed array inside the library instead of a buffer from cudaMalloc.
+#include "../../include/mdft_b200.h"
+
+#include <mutex>
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int kPointsPerBlock = 64;
+constexpr int kThreads = 256;
+constexpr int kMaxBlocks = 16384;  // => at most 1,048,576 grid points per call
+constexpr int kMaxDevices = 64;
+constexpr double kEpsDp = 2.220446049250313080847263336181640625e-16;
+
+// Partial sums {F_id, F_ext} of every block of the last call (256 KB on every GPU that
+// loads the library, kept until the process exits).  Each call overwrites the entries it
+// reads back, so nothing carries over between calls; calls that overlap on the GPU race.
+static __device__ __align__(256) double g_partials[2 * kMaxBlocks];
+
+// Device address of g_partials per device, looked up on the first call on that device.
+double *g_partials_addr[kMaxDevices] = {nullptr};
+std::mutex g_lock;
+
+// energy_ideal_and_external (src/module_energy_ideal_and_external.f90:46-73) over the
+// points [blockIdx.x*64, +64) of one block: partial F_id, F_ext and df = id+ext gradient.
+__global__ void __launch_bounds__(kThreads) k_ideal_external_partials(const double *__restrict__ xi, const double *__restrict__ vext,
+                                                                    const double *__restrict__ w, int no, long long npoints,
+                                                                    double kT, double rho0, double dv, double *__restrict__ df,
+                                                                    double *__restrict__ partials) {
+    const long long first = (long long)blockIdx.x * kPointsPerBlock * no;
+    const long long last = min(first + (long long)kPointsPerBlock * no, npoints * no);
+    double fid = 0.0, fext = 0.0;
+    for (long long i = first + threadIdx.x; i < last; i += blockDim.x) {
+        const int io = (int)(i % no);
+        const double x = xi[i], wio = w[io];
+        const double rho = x * x * rho0;
+        double g = 0.0;
+        if (rho > kEpsDp) {
+            const double lg = log(rho / rho0), v = vext[i];
+            fid += kT * dv * wio * (rho * lg - rho + rho0);
+            fext += dv * wio * rho * v;
+            g = wio * 2.0 * rho0 * x * (kT * lg + v);
+        } else {
+            fid += kT * dv * wio * rho0;
+        }
+        if (df) df[i] = g;
+    }
+    __shared__ double s_id[kThreads / 32], s_ext[kThreads / 32];
+    for (int off = 16; off > 0; off >>= 1) {
+        fid += __shfl_down_sync(0xffffffffu, fid, off);
+        fext += __shfl_down_sync(0xffffffffu, fext, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_id[threadIdx.x >> 5] = fid;
+        s_ext[threadIdx.x >> 5] = fext;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k) {
+            a += s_id[k];
+            b += s_ext[k];
+        }
+        partials[2 * blockIdx.x] = a;
+        partials[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// Sum the nblk partial pairs in a fixed order into out[0..1].
+__global__ void k_sum_partials(const double *__restrict__ partials, int nblk, double *__restrict__ out) {
+    __shared__ double sa[kThreads], sb[kThreads];
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+        a += partials[2 * k];
+        b += partials[2 * k + 1];
+    }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) {
+            sa[threadIdx.x] += sa[threadIdx.x + off];
+            sb[threadIdx.x] += sb[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sa[0];
+        out[1] = sb[0];
+    }
+}
+
+int fail(int code, const char *msg) {
+    mdft::set_error("%s", msg);
+    return code;
+}
+
+}  // namespace
+
+extern "C" int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const double *d_w, int no,
+                                           long long npoints, double kT, double rho0, double dv, double *d_df,
+                                           double *d_out, void *stream) {
+    if (!d_xi || !d_vext || !d_w || !d_out || no <= 0 || npoints <= 0)
+        return fail(MDFT_E_ARG, "mdft_ideal_external_noalloc: null pointer or non-positive size");
+    const long long nblk = (npoints + kPointsPerBlock - 1) / kPointsPerBlock;
+    if (nblk > kMaxBlocks) {
+        mdft::set_error("mdft_ideal_external_noalloc: %lld grid points exceed the fixed scratch limit of %d points",
+                        npoints, kMaxBlocks * kPointsPerBlock);
+        return MDFT_E_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(MDFT_E_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return fail(MDFT_E_ARG, "mdft_ideal_external_noalloc: device ordinal out of range");
+    double *scratch;
+    {
+        // First call on this device: look up the device address of the fixed array
+        // (host code may not use &g_partials, which is only a host-side stand-in).
+        std::lock_guard<std::mutex> lk(g_lock);
+        if (!g_partials_addr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_partials);
+            if (e != cudaSuccess) return fail(MDFT_E_CUDA, cudaGetErrorString(e));
+            g_partials_addr[dev] = static_cast<double *>(p);
+        }
+        scratch = g_partials_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_ideal_external_partials<<<(unsigned)nblk, kThreads, 0, st>>>(d_xi, d_vext, d_w, no, npoints, kT, rho0, dv, d_df, scratch);
+    k_sum_partials<<<1, kThreads, 0, st>>>(scratch, (int)nblk, d_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(MDFT_E_CUDA, cudaGetErrorString(e));
+    return MDFT_OK;
+}

@@ -81,6 +81,8 @@ SIGNATURES = {
     "mdft_guess_density_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mdft_minimize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_MinOpts), C.POINTER(_MinRes)]),
     "mdft_get_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "mdft_ideal_external_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double,
+                                              C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mdft_pressure_correction": (C.c_int, [C.c_void_p, _DP, C.c_double, C.c_double, _DP]),
     "mdft_pressure_correction_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, _DP]),
     "mdft_solve": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP, C.c_double,
