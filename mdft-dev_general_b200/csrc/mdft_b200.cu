@@ -11,6 +11,7 @@
 #include "k_angular.cuh"
 #include "k_fft.cuh"
 #include "k_oz.cuh"
+#include "k_oz2.cuh"
 #include "k_vec.cuh"
 #include "k_vext.cuh"
 
@@ -59,8 +60,10 @@ struct mdft_handle {
     int bm_project = 64, bm_gather = 64;
     long long nblk_project = 0, nblk_gather = 0;
     FftAxis fft[3];
-    OzArgs oz{};
-    int oz_grid = 0;
+    Oz2Args oz{};
+    DevBuf<int> oz_ints;
+    DevBuf<double> oz_dbls;
+    int oz_grid = 0, oz_warps = 8;
     size_t oz_smem = 0;
     // timing
     bool timing = false;
@@ -180,7 +183,8 @@ int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal,
     stage_mark(h, 1);
     if ((rc = launch_fft(h, +1))) return rc;
     stage_mark(h, 2);
-    k_oz_f64<<<h->oz_grid, 256, h->oz_smem, h->stream>>>(h->planes.p, h->ctab.p, h->oz);
+    k_oz2<double><<<h->oz_grid, 32 * h->oz_warps, h->oz_smem, h->stream>>>(h->planes.p, h->ctab.p, h->oz_ints.p,
+                                                                            h->oz_dbls.p, h->oz);
     if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
     stage_mark(h, 3);
     if ((rc = launch_fft(h, -1))) return rc;
@@ -297,21 +301,6 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     cudaMemcpy(h->w.p, g.w.data(), g.no * 8, cudaMemcpyHostToDevice);
     if ((rc = alloc_check(h->ctab.alloc((size_t)h->ct.nq * h->ct.ncoef), "c table", h->ct.c.size() * 8))) return rc;
     cudaMemcpy(h->ctab.p, h->ct.c.data(), h->ct.c.size() * 8, cudaMemcpyHostToDevice);
-    // constant tables
-    RotCoef rcf;
-    build_rot_coef(rcf);
-    std::vector<int> pm(kMaxNpConst, 0), pmup(kMaxNpConst, 0), pmu2(kMaxNpConst, 0), ias(kMaxNpConst, 0);
-    for (int i = 0; i < g.np; ++i) {
-        pm[i] = g.pm[i];
-        pmup[i] = g.pmup[i];
-        pmu2[i] = g.pmu[i] / g.mrso;
-        ias[i] = h->ct.ia_start[i];
-    }
-    cudaMemcpyToSymbol(c_rot, &rcf, sizeof rcf);
-    cudaMemcpyToSymbol(c_pm, pm.data(), kMaxNpConst * sizeof(int));
-    cudaMemcpyToSymbol(c_pmup, pmup.data(), kMaxNpConst * sizeof(int));
-    cudaMemcpyToSymbol(c_pmu2, pmu2.data(), kMaxNpConst * sizeof(int));
-    cudaMemcpyToSymbol(c_ia_start, ias.data(), kMaxNpConst * sizeof(int));
     if ((rc = check_cuda(cudaGetLastError(), "table upload"))) return rc;
     // launch shapes
     int maxsmem = 0;
@@ -325,7 +314,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     }
     if ((rc = allow_smem((const void *)k_project_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_project_f64<32>, maxsmem)) ||
         (rc = allow_smem((const void *)k_gather_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_gather_f64<32>, maxsmem)) ||
-        (rc = allow_smem((const void *)k_fft_axis<double>, maxsmem)) || (rc = allow_smem((const void *)k_oz_f64, maxsmem)))
+        (rc = allow_smem((const void *)k_fft_axis<double>, maxsmem)) || (rc = allow_smem((const void *)k_oz2<double>, maxsmem)))
         return rc;
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
     h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
@@ -338,18 +327,29 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     if ((rc = setup_fft(h.get()))) return rc;
     for (int ax = 0; ax < 3; ++ax)
         if (h->fft[ax].smem > (size_t)maxsmem) { set_error("FFT tile does not fit in shared memory"); return MDFT_E_ARG; }
-    OzArgs &oz = h->oz;
-    oz.nx = g.nx; oz.ny = g.ny; oz.nz = g.nz; oz.N = g.N;
-    oz.mmax = g.mmax; oz.mrso = g.mrso; oz.np = g.np;
-    oz.ncoef = h->ct.ncoef; oz.nq = h->ct.nq; oz.dq = h->ct.dq;
-    oz.twopi_lx = 2.0 * kPi / g.lx;
-    oz.twopi_ly = 2.0 * kPi / g.ly;
-    oz.twopi_lz = 2.0 * kPi / g.lz;
-    oz.quirks = 1;
-    oz.nk = (long long)g.nx * g.ny * (g.nz / 2 + 1);
-    h->oz_grid = (int)((oz.nk + 7) / 8);
-    h->oz_smem = oz_smem_bytes(g.mmax, g.np, 8);
-    if (h->oz_smem > (size_t)maxsmem) { set_error("OZ tile does not fit in shared memory"); return MDFT_E_ARG; }
+    {
+        OzTables tb;
+        build_oz_tables(g, h->ct, tb);
+        if ((rc = alloc_check(h->oz_ints.alloc(tb.ints.size()), "OZ tables", tb.ints.size() * 4))) return rc;
+        if ((rc = alloc_check(h->oz_dbls.alloc(std::max<size_t>(1, tb.dbls.size())), "OZ tables", tb.dbls.size() * 8))) return rc;
+        cudaMemcpy(h->oz_ints.p, tb.ints.data(), tb.ints.size() * 4, cudaMemcpyHostToDevice);
+        if (!tb.dbls.empty()) cudaMemcpy(h->oz_dbls.p, tb.dbls.data(), tb.dbls.size() * 8, cudaMemcpyHostToDevice);
+        Oz2Args &oz = h->oz;
+        oz.nx = g.nx; oz.ny = g.ny; oz.nz = g.nz; oz.N = g.N;
+        oz.nk = (long long)g.nx * g.ny * (g.nz / 2 + 1);
+        oz.mmax = g.mmax; oz.np = g.np; oz.ncoef = h->ct.ncoef; oz.nq = h->ct.nq; oz.dq = h->ct.dq;
+        oz.twopi_lx = 2.0 * kPi / g.lx; oz.twopi_ly = 2.0 * kPi / g.ly; oz.twopi_lz = 2.0 * kPi / g.lz;
+        oz.quirks = 1;
+        oz.n_ints = (int)tb.ints.size(); oz.n_dbls = (int)tb.dbls.size(); oz.nrot = tb.nrot;
+        oz.fwd_off = tb.fwd_off; oz.fwd_terms = tb.fwd_terms; oz.oz_off = tb.oz_off; oz.oz_terms = tb.oz_terms;
+        oz.bwd_off = tb.bwd_off; oz.bwd_terms = tb.bwd_terms; oz.sign = tb.sign; oz.lvl_off = tb.lvl_off;
+        oz.rec_int = tb.rec_int;
+        h->oz_warps = 8;
+        while (h->oz_warps > 1 && oz2_smem_bytes<double>(oz, h->oz_warps) > dyn_max) h->oz_warps /= 2;
+        h->oz_smem = oz2_smem_bytes<double>(oz, h->oz_warps);
+        if (h->oz_smem > dyn_max) { set_error("OZ tile does not fit in shared memory"); return MDFT_E_ARG; }
+        h->oz_grid = (int)((oz.nk + h->oz_warps - 1) / h->oz_warps);
+    }
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "create"))) return rc;
     *out = h.release();
     return MDFT_OK;
@@ -359,7 +359,7 @@ int mdft_destroy(mdft_handle *h) {
     if (!h) return MDFT_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->xi.free(); h->vext.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
-    h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free();
+    h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free(); h->oz_ints.free(); h->oz_dbls.free();
     for (int i = 0; i < 3; ++i) h->tw64[i].free();
     lbfgs_free(h->lb);
     h->vpart.free();

@@ -21,10 +21,13 @@ CASES = {
     "rand12_m3": dict(n=12, L=6.0, mmax=3, solute="none", seed=3, rvdw=2.9, xseed=13),
     "mol24_m3": dict(n=24, L=12.0, mmax=3, solute="walk6", seed=4, rvdw=5.9, xseed=14),
     "mol8_m0": dict(n=8, L=4.0, mmax=0, solute="walk3", seed=5, rvdw=1.9, xseed=15),
+    "rand8_m5": dict(n=8, L=4.0, mmax=5, solute="none", seed=6, rvdw=1.9, xseed=16, dk=0.1),
 }
 
 
-def ck_path(directory, mmax, kmax=14.0, dk=0.02, seed=20260000):
+def ck_path(directory, mmax, kmax=14.0, dk=None, seed=20260000):
+    if dk is None:
+        dk = 0.1 if mmax >= 5 else 0.02
     path = os.path.join(str(directory), "ck_m%d_k%g_d%g_s%d.txt" % (mmax, kmax, dk, seed))
     if not os.path.exists(path):
         synth.make_ck_file(path, mmax, kmax=kmax, dk=dk, seed=seed)
