@@ -1,0 +1,179 @@
+// Batched 3-D FFTs over the projection planes, templated on precision and length.
+//
+//  k_fft_xy<T, N>  : one CTA per (projection, z) plane of N x N points: the plane is
+//                    staged in shared memory, transformed along x then y, written back.
+//  k_fft_z<T, N>   : one CTA per (projection, y) and TL consecutive x: columns along z.
+//
+// Every radix pass is in place: each thread loads the inputs of its butterflies into
+// registers (twiddled), a barrier, then writes the outputs at their Stockham positions.
+// The radix sequence (4s, then 2, then 3s) is fixed at compile time, so butterflies are
+// fully unrolled.  sign=+1: X[k] = sum_j x[j] e^{+2 pi i jk/N} (plan3dp of
+// src/module_energy_cproj_mrso.f90:260); sign=-1: plan3dm; no scaling.
+#pragma once
+
+#include "common.cuh"
+#include "k_fft.cuh"
+
+namespace mdft {
+
+__host__ __device__ constexpr int count_factor(int n, int f) { return (n % f == 0 && n > 1) ? 1 + count_factor(n / f, f) : 0; }
+__host__ __device__ constexpr int npass_of(int n) {
+    return count_factor(n, 4) + count_factor(n / (1 << (2 * count_factor(n, 4))), 2) +
+           count_factor(n / (1 << (2 * count_factor(n, 4))) / (1 << count_factor(n / (1 << (2 * count_factor(n, 4))), 2)), 3);
+}
+// radix of pass p for length n: all 4s, then 2s, then 3s
+__host__ __device__ constexpr int radix_of(int n, int p) {
+    return p < count_factor(n, 4) ? 4
+           : p < count_factor(n, 4) + count_factor(n / (1 << (2 * count_factor(n, 4))), 2) ? 2
+                                                                                               : 3;
+}
+// product of the radices before pass p (the Stockham span Ns)
+__host__ __device__ constexpr int span_of(int n, int p) { return p == 0 ? 1 : span_of(n, p - 1) * radix_of(n, p - 1); }
+
+template <typename T, int R>
+__device__ __forceinline__ void dft_small(typename Cplx<T>::t (&v)[R], int sign) {
+    using C = typename Cplx<T>::t;
+    if constexpr (R == 2) {
+        C a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        C s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+        C wd;
+        wd.x = -(T)sign * d13.y;
+        wd.y = (T)sign * d13.x;
+        v[0] = cadd(s02, s13);
+        v[1] = cadd(d02, wd);
+        v[2] = csub(s02, s13);
+        v[3] = csub(d02, wd);
+    } else {  // R == 3
+        const T c3 = (T)-0.5;
+        const T s3 = (T)sign * (T)0.86602540378443864676372317075294;
+        C s12 = cadd(v[1], v[2]), d12 = csub(v[1], v[2]);
+        C m;
+        m.x = v[0].x + c3 * s12.x;
+        m.y = v[0].y + c3 * s12.y;
+        C rot;
+        rot.x = -s3 * d12.y;
+        rot.y = s3 * d12.x;
+        v[0] = cadd(v[0], s12);
+        v[1] = cadd(m, rot);
+        v[2] = csub(m, rot);
+    }
+}
+
+// One in-place Stockham pass of radix R over `lines` transforms of length N stored at
+// buf[line * lstride + i * istride]; tw[t] = e^{+2 pi i t/N}.  LF: consecutive threads take
+// consecutive lines (for strided lines, so that shared-memory accesses stay contiguous).
+template <typename T, int N, int R, int NS, int LINES, int THREADS, bool LF>
+__device__ __forceinline__ void stockham_pass(typename Cplx<T>::t *buf, int istride, int lstride,
+                                              const typename Cplx<T>::t *tw, int sign) {
+    using C = typename Cplx<T>::t;
+    constexpr int NB = N / R;
+    constexpr int ITEMS = NB * LINES;
+    constexpr int PER = (ITEMS + THREADS - 1) / THREADS;
+    constexpr int TSTEP = N / (NS * R);
+    C v[PER][R];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int it = threadIdx.x + k * THREADS;
+        if (ITEMS % THREADS == 0 || it < ITEMS) {
+            const int line = LF ? it % LINES : it / NB, j = LF ? it / LINES : it % NB, jm = j % NS;
+            C *b = buf + line * lstride;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                C x = b[(j + r * NB) * istride];
+                if (r > 0 && NS > 1) {
+                    C w = tw[(jm * TSTEP * r) % N];
+                    if (sign < 0) w.y = -w.y;
+                    x = cmul(x, w);
+                }
+                v[k][r] = x;
+            }
+            dft_small<T, R>(v[k], sign);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int it = threadIdx.x + k * THREADS;
+        if (ITEMS % THREADS == 0 || it < ITEMS) {
+            const int line = LF ? it % LINES : it / NB, j = LF ? it / LINES : it % NB, jm = j % NS;
+            C *b = buf + line * lstride;
+            const int idxD = (j / NS) * NS * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) b[(idxD + r * NS) * istride] = v[k][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int N, int P, int LINES, int THREADS, bool LF>
+__device__ __forceinline__ void fft_lines(typename Cplx<T>::t *buf, int istride, int lstride,
+                                          const typename Cplx<T>::t *tw, int sign) {
+    if constexpr (P < npass_of(N)) {
+        stockham_pass<T, N, radix_of(N, P), span_of(N, P), LINES, THREADS, LF>(buf, istride, lstride, tw, sign);
+        fft_lines<T, N, P + 1, LINES, THREADS, LF>(buf, istride, lstride, tw, sign);
+    }
+}
+
+template <typename T, int N> __host__ __device__ constexpr int xy_threads() { return (N >= 96) ? 1024 : (N >= 48 ? 512 : 256); }
+
+// data: [planes][N][N] (y then x); one CTA per plane
+template <typename T, int N>
+__global__ void __launch_bounds__(xy_threads<T, N>(), (xy_threads<T, N>() <= 512 ? 2 : 1)) k_fft_xy(typename Cplx<T>::t *__restrict__ data,
+                                                               const typename Cplx<T>::t *__restrict__ tw, int sign) {
+    using C = typename Cplx<T>::t;
+    constexpr int THREADS = xy_threads<T, N>();
+    constexpr int LD = N + 1;  // padded row
+    extern __shared__ __align__(16) unsigned char xy_smem[];
+    C *twl = reinterpret_cast<C *>(xy_smem);
+    C *buf = twl + N;
+    C *g = data + (size_t)blockIdx.x * N * N;
+    for (int i = threadIdx.x; i < N; i += THREADS) twl[i] = tw[i];
+    for (int i = threadIdx.x; i < N * N; i += THREADS) buf[(i / N) * LD + (i % N)] = g[i];
+    __syncthreads();
+    fft_lines<T, N, 0, N, THREADS, false>(buf, 1, LD, twl, sign);  // along x: line = y
+    fft_lines<T, N, 0, N, THREADS, true>(buf, LD, 1, twl, sign);   // along y: line = x
+    for (int i = threadIdx.x; i < N * N; i += THREADS) g[i] = buf[(i / N) * LD + (i % N)];
+}
+
+template <typename T, int N> __host__ __device__ constexpr size_t xy_smem_bytes() { return sizeof(typename Cplx<T>::t) * (N + (size_t)N * (N + 1)); }
+
+template <typename T> __host__ __device__ constexpr int z_tl() { return sizeof(T) == 8 ? 16 : 32; }
+
+// data: [planes][nz = N][ny][nx]; CTA = (plane, y, x-tile of TL)
+template <typename T, int N>
+__global__ void __launch_bounds__(256) k_fft_z(typename Cplx<T>::t *__restrict__ data, const typename Cplx<T>::t *__restrict__ tw,
+                                              int nx, int ny, int sign) {
+    using C = typename Cplx<T>::t;
+    constexpr int TL = z_tl<T>();
+    constexpr int LD = TL + 1;
+    extern __shared__ __align__(16) unsigned char z_smem[];
+    C *twl = reinterpret_cast<C *>(z_smem);
+    C *buf = twl + N;
+    const int xt = nx / TL;
+    const long long t = blockIdx.x;
+    const int ix0 = (int)(t % xt) * TL;
+    const long long rest = t / xt;  // plane * ny + iy
+    const long long p = rest / ny, iy = rest % ny;
+    const long long plane = (long long)nx * ny * N;
+    C *g = data + p * plane + iy * nx + ix0;
+    const long long zs = (long long)nx * ny;
+    for (int i = threadIdx.x; i < N; i += 256) twl[i] = tw[i];
+    for (int f = threadIdx.x; f < N * TL; f += 256) {
+        const int i = f / TL, l = f % TL;
+        buf[i * LD + l] = g[i * zs + l];
+    }
+    __syncthreads();
+    fft_lines<T, N, 0, TL, 256, true>(buf, LD, 1, twl, sign);
+    for (int f = threadIdx.x; f < N * TL; f += 256) {
+        const int i = f / TL, l = f % TL;
+        g[i * zs + l] = buf[i * LD + l];
+    }
+}
+
+template <typename T, int N> __host__ __device__ constexpr size_t z_smem_bytes() { return sizeof(typename Cplx<T>::t) * (N + (size_t)N * (z_tl<T>() + 1)); }
+
+}  // namespace mdft

@@ -10,6 +10,7 @@
 #include "setup_host.cuh"
 #include "k_angular.cuh"
 #include "k_fft.cuh"
+#include "k_fft2.cuh"
 #include "k_oz.cuh"
 #include "k_oz2.cuh"
 #include "k_vec.cuh"
@@ -155,11 +156,87 @@ int setup_fft(mdft_handle *h) {
     return 0;
 }
 
+bool xy_smem_ok(int n) { return sizeof(double2) * (size_t)n * (n + 2) <= 200 * 1024; }
+
+// Specialised plane (x,y) and column (z) transforms for the supported lengths; the
+// generic per-axis kernel otherwise.
+template <typename T, int N>
+cudaError_t fft_xy_n(typename Cplx<T>::t *data, long long nplanes, const typename Cplx<T>::t *tw, int sign, cudaStream_t st,
+                     bool prepare) {
+    if (prepare)
+        return cudaFuncSetAttribute(k_fft_xy<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem_bytes<T, N>());
+    k_fft_xy<T, N><<<(unsigned)nplanes, xy_threads<T, N>(), xy_smem_bytes<T, N>(), st>>>(data, tw, sign);
+    return cudaGetLastError();
+}
+template <typename T, int N>
+cudaError_t fft_z_n(typename Cplx<T>::t *data, long long nplanes, int nx, int ny, const typename Cplx<T>::t *tw, int sign,
+                    cudaStream_t st, bool prepare) {
+    if (prepare)
+        return cudaFuncSetAttribute(k_fft_z<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)z_smem_bytes<T, N>());
+    const long long grid = nplanes * ny * (nx / z_tl<T>());
+    k_fft_z<T, N><<<(unsigned)grid, 256, z_smem_bytes<T, N>(), st>>>(data, tw, nx, ny, sign);
+    return cudaGetLastError();
+}
+
+// returns cudaErrorNotSupported when no specialised kernel exists for n
+template <typename T>
+cudaError_t fft_xy(int n, typename Cplx<T>::t *data, long long nplanes, const typename Cplx<T>::t *tw, int sign, cudaStream_t st,
+                   bool prepare) {
+    switch (n) {
+    case 8: return fft_xy_n<T, 8>(data, nplanes, tw, sign, st, prepare);
+    case 12: return fft_xy_n<T, 12>(data, nplanes, tw, sign, st, prepare);
+    case 16: return fft_xy_n<T, 16>(data, nplanes, tw, sign, st, prepare);
+    case 24: return fft_xy_n<T, 24>(data, nplanes, tw, sign, st, prepare);
+    case 32: return fft_xy_n<T, 32>(data, nplanes, tw, sign, st, prepare);
+    case 48: return fft_xy_n<T, 48>(data, nplanes, tw, sign, st, prepare);
+    case 64: return fft_xy_n<T, 64>(data, nplanes, tw, sign, st, prepare);
+    case 96: return fft_xy_n<T, 96>(data, nplanes, tw, sign, st, prepare);
+    default: return cudaErrorNotSupported;
+    }
+}
+template <typename T>
+cudaError_t fft_z(int n, typename Cplx<T>::t *data, long long nplanes, int nx, int ny, const typename Cplx<T>::t *tw, int sign,
+                  cudaStream_t st, bool prepare) {
+    if (nx % z_tl<T>()) return cudaErrorNotSupported;
+    switch (n) {
+    case 8: return fft_z_n<T, 8>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 12: return fft_z_n<T, 12>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 16: return fft_z_n<T, 16>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 24: return fft_z_n<T, 24>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 32: return fft_z_n<T, 32>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 48: return fft_z_n<T, 48>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 64: return fft_z_n<T, 64>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 96: return fft_z_n<T, 96>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    case 128: return fft_z_n<T, 128>(data, nplanes, nx, ny, tw, sign, st, prepare);
+    default: return cudaErrorNotSupported;
+    }
+}
+
 int launch_fft(mdft_handle *h, int sign) {
-    for (int ax = 0; ax < 3; ++ax) {
+    const Grid &g = h->g;
+    bool xy_done = false;
+    if (g.nx == g.ny && xy_smem_ok(g.nx)) {
+        cudaError_t e = fft_xy<double>(g.nx, h->planes.p, (long long)g.np * g.nz, (const double2 *)h->fft[0].tw, sign, h->stream, false);
+        if (e == cudaSuccess) { xy_done = true; h->launches += 1; }
+        else if (e != cudaErrorNotSupported) return check_cuda(e, "fft xy launch");
+        else cudaGetLastError();
+    }
+    for (int ax = 0; ax < 2 && !xy_done; ++ax) {
         FftAxis &F = h->fft[ax];
         F.args.sign = sign;
         k_fft_axis<double><<<F.grid, kFftThreads, F.smem, h->stream>>>(h->planes.p, (const double2 *)F.tw, F.args);
+        h->launches += 1;
+    }
+    cudaError_t e = fft_z<double>(g.nz, h->planes.p, g.np, g.nx, g.ny, (const double2 *)h->fft[2].tw, sign, h->stream, false);
+    if (e == cudaSuccess) { h->launches += 1; }
+    else if (e == cudaErrorNotSupported) {
+        cudaGetLastError();
+        FftAxis &F = h->fft[2];
+        F.args.sign = sign;
+        k_fft_axis<double><<<F.grid, kFftThreads, F.smem, h->stream>>>(h->planes.p, (const double2 *)F.tw, F.args);
+        h->launches += 1;
+    } else {
+        return check_cuda(e, "fft z launch");
     }
     return check_cuda(cudaGetLastError(), "fft launch");
 }
@@ -209,7 +286,7 @@ int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal,
             h->planes.p, h->B.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
     if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
     k_reduce3<<<1, 256, 0, h->stream>>>(h->partial.p, h->nblk_gather, h->sums.p);
-    h->launches += 10;
+    h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft)
     stage_mark(h, 5);
     return check_cuda(cudaGetLastError(), "reduce launch");
 }
@@ -316,6 +393,13 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         (rc = allow_smem((const void *)k_gather_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_gather_f64<32>, maxsmem)) ||
         (rc = allow_smem((const void *)k_fft_axis<double>, maxsmem)) || (rc = allow_smem((const void *)k_oz2<double>, maxsmem)))
         return rc;
+    for (int n : {g.nx, g.nz}) {
+        cudaError_t e1 = fft_xy<double>(n, nullptr, 0, nullptr, 1, nullptr, true);
+        cudaError_t e2 = fft_z<double>(n, nullptr, 0, g.nx, g.ny, nullptr, 1, nullptr, true);
+        if (e1 != cudaSuccess && e1 != cudaErrorNotSupported) return check_cuda(e1, "fft xy attribute");
+        if (e2 != cudaSuccess && e2 != cudaErrorNotSupported) return check_cuda(e2, "fft z attribute");
+        cudaGetLastError();
+    }
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
     h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
     if ((rc = alloc_check(h->partial.alloc(3 * (size_t)h->nblk_gather), "partials", 24 * h->nblk_gather))) return rc;
