@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="small grid smoke run (not a bench number)")
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
+                    help="mixed: FP32 excess pipeline then an FP64 polish; fp64: plain FP64 solve")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
     return ap.parse_args()
@@ -133,9 +135,8 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def stage_bytes(N, no, np_):
-    """Algorithmic bytes per evaluation of each stage (FP64)."""
-    c = 16
+def stage_bytes(N, no, np_, c=16):
+    """Algorithmic bytes per evaluation of each stage (c = bytes per complex projection value)."""
     return {"project": N * (no * 8 + np_ * c), "fft_forward": 2 * np_ * N * c, "oz": 2 * np_ * N * c,
             "fft_inverse": 2 * np_ * N * c, "gather": N * (np_ * c + 3 * no * 8)}
 
@@ -197,7 +198,7 @@ def main():
         return reference_arm(args, rank, world)
     import torch
     import torch.distributed as dist
-    from mdft_b200 import Engine, synth
+    from mdft_b200 import Engine, PREC_FP64, PREC_MIXED, synth
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -206,7 +207,8 @@ def main():
     rvdw = RVDW if not args.quick else 7.9
     ck = ck_file(MMAX)
     sv = synth.Solvent()
-    eng = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local)
+    prec = PREC_FP64 if args.form == "fp64" else PREC_MIXED
+    eng = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec)
     stream = torch.cuda.ExternalStream(eng.stream)
     sols = [solute(10_000 * rank + i, box) for i in range(args.warmup + args.steps)]
     if args.evals:
@@ -218,7 +220,7 @@ def main():
         print(json.dumps({"evals": args.evals, "f": f, "terms": list(map(float, terms))}))
         eng.close()
         return
-    opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000)
+    opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, precision=prec)
 
     def barrier():
         if world > 1:
@@ -268,15 +270,25 @@ def main():
     h2d = 8 * (4 * s0.nsite + 4 * 3 * 2)  # solute q, sig, eps, xyz + solvent sites
     d2h = xi_host.nbytes + 8 * 6
 
+    # ---- FP64 reference dG of the timed solutes (outside the timed regions) ----
+    if prec == PREC_FP64:
+        dg_ref = [r["dG"] for r in timed]
+    else:
+        ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
+        dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts, precision=PREC_FP64))["dG"]
+                  for i in range(args.warmup, args.warmup + args.steps)]
+        ref.close()
+    dg_err = [abs(r["dG"] - d) for r, d in zip(timed, dg_ref)]
+
     # ---- roofline of the dominant stage: per-stage CUDA events over evaluations at a converged density ----
     xi_ref = xi_host.reshape(eng.shape).copy()
     eng.set_timing(True)
     for _ in range(5):
-        eng.energy_and_gradient(xi_ref)
+        eng.energy_and_gradient(xi_ref)  # in the engine's evaluation precision
     st, cnt = eng.stage_times()
     eng.set_timing(False)
     per = {k: v / cnt for k, v in st.items()}
-    sb = stage_bytes(n ** 3, eng.no, eng.np)
+    sb = stage_bytes(n ** 3, eng.no, eng.np, 16 if prec == PREC_FP64 else 8)
     dom = max(per, key=per.get)
     peak, peak_kind = measured_peak_hbm()
     achieved = sb[dom] / (per[dom] * 1e-3) / 1e9
@@ -297,14 +309,19 @@ def main():
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == PREC_FP64 else "f32+f64",
+                "data": "synthetic",
                 "config": {"workload": "%d^3 grid, %g A box, mmax %d, %d-site random-walk solute per step, synthetic c(k)"
                                        % (n, box, MMAX, NSITE),
-                           "form": "plain FP64 (vext + guess + L-BFGS m=5 + pressure correction)",
+                           "form": ("plain FP64" if prec == PREC_FP64 else
+                                    "mixed: FP32 projections/FFT/OZ with FP64 ideal term, reductions and L-BFGS, "
+                                    "then an FP64 polish") + " (vext + guess + L-BFGS m=5 + pressure correction)",
                            "stop": "max|df|<=1e-6 (line-search stall accepted)", "l2": "inputs larger than L2 (176 MB per field)",
                            "parallelism": "replicas" if world > 1 else "single GPU",
-                           "evaluations_per_solve": evals, "dG": [r["dG"] for r in timed],
-                           "dG_error_vs_fp64": 0.0},
+                           "evaluations_per_solve": evals,
+                           "fp32_evaluations_per_solve": [r.get("evaluations_mixed", 0) for r in timed],
+                           "dG": [r["dG"] for r in timed], "dG_fp64": dg_ref,
+                           "dG_error_vs_fp64_max": max(dg_err), "all_within_0.1": bool(max(dg_err) <= 0.1)},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line))

@@ -139,11 +139,15 @@ typedef struct mdft_minimize_result {
     int iterations;  /* L-BFGS iterations                                        */
     int evaluations; /* energy_and_gradient calls                                 */
     int status;      /* 0 pgtol, 1 f-reduction, 2 line-search failure, 3 itermax   */
+    int evaluations_mixed; /* of which FP32-pipeline evaluations (MDFT_PREC_MIXED)   */
 } mdft_minimize_result;
 
 /* minimization_using_lbfgs (src/energy_minimization.f90:232-290) with the
  * unconstrained L-BFGS-B of src/module_lbfgs_nocedal_mdft.f90:136-534, run on
- * the device: xi is read from and written to the host buffer. */
+ * the device: xi is read from and written to the host buffer.  With
+ * MDFT_PREC_MIXED the iterations use FP32 projections/FFTs/OZ until the
+ * stopping test holds, then continue with FP64 evaluations (fresh history)
+ * until it holds in FP64; f and pgnorm are always FP64 values. */
 int mdft_minimize(mdft_handle *h, double *xi, const mdft_minimize_opts *opts, mdft_minimize_result *res);
 
 /* Device-pointer variants (on the handle's stream): d_xi is a device array of

@@ -1,4 +1,5 @@
-// Angular transforms as per-point dense contractions (FP64 path).
+// Angular transforms as per-point dense contractions, templated on the compute
+// precision T (double: parity path; float: mixed path).
 //
 //  project (S1, src/module_energy_cproj_mrso.f90:276-290 with angl2proj):
 //     drho_p[ip][r] = sum_io rho0 (xi[r][io]^2 - 1) A[io][ip]
@@ -10,9 +11,12 @@
 // stages BM points x K inputs in shared memory (coalesced: a point's no
 // doubles are contiguous, a projection plane's points are contiguous), the
 // matrix in 32-row slabs, and each thread keeps a (BM/16) x 4 register tile.
+// xi, vext, df, the epilogue arithmetic (log, ideal and external terms) and all
+// partial sums are FP64 in both precisions.
 #pragma once
 
 #include "common.cuh"
+#include "k_fft.cuh"
 
 namespace mdft {
 
@@ -34,78 +38,85 @@ struct GatherArgs {
     int df_mode;                          // 0 none, 1 store (id + exc), 2 accumulate exc
 };
 
+template <typename T> struct Vec4;
+template <> struct Vec4<double> { struct t { double2 a, b; }; };
+template <> struct Vec4<float> { using t = float4; };
+__device__ __forceinline__ void unpack4(const Vec4<double>::t &v, double (&o)[4]) { o[0] = v.a.x; o[1] = v.a.y; o[2] = v.b.x; o[3] = v.b.y; }
+__device__ __forceinline__ void unpack4(const float4 &v, float (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+
 // one 32-row slab of the inner product
-template <int TM>
-__device__ __forceinline__ void ang_slab(const double *__restrict__ As, int lda, const double *__restrict__ Bs, int k0,
-                                         int tx, int ty, double (&acc)[TM][4]) {
+template <typename T, int TM>
+__device__ __forceinline__ void ang_slab(const T *__restrict__ As, int lda, const T *__restrict__ Bs, int k0, int tx, int ty,
+                                         T (&acc)[TM][4]) {
 #pragma unroll 8
     for (int kk = 0; kk < kAngBK; ++kk) {
-        const double *ar = As + (size_t)(k0 + kk) * lda + ty * TM;
-        double a[TM];
+        const T *ar = As + (size_t)(k0 + kk) * lda + ty * TM;
+        T a[TM];
 #pragma unroll
         for (int i = 0; i < TM; ++i) a[i] = ar[i];
-        const double2 *br = reinterpret_cast<const double2 *>(Bs + kk * kAngBN + tx * 4);
-        double2 b01 = br[0], b23 = br[1];
+        T b[4];
+        unpack4(*reinterpret_cast<const typename Vec4<T>::t *>(Bs + kk * kAngBN + tx * 4), b);
 #pragma unroll
-        for (int i = 0; i < TM; ++i) {
-            acc[i][0] = fma(a[i], b01.x, acc[i][0]);
-            acc[i][1] = fma(a[i], b01.y, acc[i][1]);
-            acc[i][2] = fma(a[i], b23.x, acc[i][2]);
-            acc[i][3] = fma(a[i], b23.y, acc[i][3]);
-        }
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
 }
 
 // Load a 32 x 64 slab of the row-major K x J matrix M (zero outside).
-__device__ __forceinline__ void ang_load_slab(double *Bs, const double *__restrict__ M, int K, int J, int k0, int j0) {
+template <typename T>
+__device__ __forceinline__ void ang_load_slab(T *Bs, const T *__restrict__ M, int K, int J, int k0, int j0) {
     for (int f = threadIdx.x; f < kAngBK * kAngBN; f += blockDim.x) {
         int kk = f / kAngBN, jj = f % kAngBN;
         int k = k0 + kk, j = j0 + jj;
-        Bs[f] = (k < K && j < J) ? M[(size_t)k * J + j] : 0.0;
+        Bs[f] = (k < K && j < J) ? M[(size_t)k * J + j] : (T)0;
     }
 }
 
-// S1: xi [N][no] -> planes [np][N] (complex).
-template <int BM>
-__global__ void __launch_bounds__(kAngThreads) k_project_f64(const double *__restrict__ xi, const double *__restrict__ A,
-                                                             double2 *__restrict__ planes, AngularArgs a) {
+// S1: xi [N][no] (FP64) -> planes [np][N] (complex T).
+template <typename T, int BM>
+__global__ void __launch_bounds__(kAngThreads) k_project(const double *__restrict__ xi, const T *__restrict__ A,
+                                                         typename Cplx<T>::t *__restrict__ planes, AngularArgs a) {
+    using C = typename Cplx<T>::t;
     constexpr int TM = BM / 16;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char ang_smem[];
+    T *smem = reinterpret_cast<T *>(ang_smem);
     const int K = a.no, J = 2 * a.np;
     const int Kpad = (K + kAngBK - 1) / kAngBK * kAngBK;
     const int lda = BM + 1;
-    double *As = smem;                          // [Kpad][BM+1]
-    double *Bs = As + (size_t)Kpad * lda;       // [BK][BN]
-    double2 *Cs = reinterpret_cast<double2 *>(Bs + kAngBK * kAngBN);  // [BN/2][BM]
+    T *As = smem;                                                   // [Kpad][BM+1]
+    T *Bs = As + ((size_t)Kpad * lda + 3) / 4 * 4;                  // [BK][BN], 16-byte aligned
+    C *Cs = reinterpret_cast<C *>(Bs + kAngBK * kAngBN);            // [BN/2][BM]
     const long long pt0 = (long long)blockIdx.x * BM;
     const int npts = (int)min((long long)BM, a.N - pt0);
-    // inputs: rho0 (xi^2 - 1), coalesced along io
     for (int f = threadIdx.x; f < BM * Kpad; f += blockDim.x) {
         int p = f / Kpad, k = f % Kpad;
-        double v = 0.0;
+        T v = 0;
         if (p < npts && k < K) {
             double x = xi[(pt0 + p) * K + k];
-            v = a.rho0 * (x * x - 1.0);
+            v = (T)(a.rho0 * (x * x - 1.0));
         }
         As[(size_t)k * lda + p] = v;
     }
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     for (int j0 = 0; j0 < J; j0 += kAngBN) {
-        double acc[TM][4];
+        T acc[TM][4];
 #pragma unroll
-        for (int i = 0; i < TM; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
+        for (int i = 0; i < TM; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = (T)0;
         for (int k0 = 0; k0 < Kpad; k0 += kAngBK) {
             __syncthreads();
-            ang_load_slab(Bs, A, K, J, k0, j0);
+            ang_load_slab<T>(Bs, A, K, J, k0, j0);
             __syncthreads();
-            ang_slab<TM>(As, lda, Bs, k0, tx, ty, acc);
+            ang_slab<T, TM>(As, lda, Bs, k0, tx, ty, acc);
         }
-        // stage the chunk as complex [ip_local][point]
 #pragma unroll
         for (int i = 0; i < TM; ++i) {
             int p = ty * TM + i;
-            Cs[(tx * 2 + 0) * BM + p] = make_double2(acc[i][0], acc[i][1]);
-            Cs[(tx * 2 + 1) * BM + p] = make_double2(acc[i][2], acc[i][3]);
+            C u, v;
+            u.x = acc[i][0]; u.y = acc[i][1];
+            v.x = acc[i][2]; v.y = acc[i][3];
+            Cs[(tx * 2 + 0) * BM + p] = u;
+            Cs[(tx * 2 + 1) * BM + p] = v;
         }
         __syncthreads();
         const int ip0 = j0 / 2;
@@ -118,29 +129,34 @@ __global__ void __launch_bounds__(kAngThreads) k_project_f64(const double *__res
 }
 
 // S7 fused with the ideal + external term.  partial[block] = {F_id, F_ext, sum for F_exc}.
-template <int BM>
-__global__ void __launch_bounds__(kAngThreads) k_gather_f64(const double2 *__restrict__ planes, const double *__restrict__ B,
-                                                            const double *__restrict__ xi, const double *__restrict__ vext,
-                                                            const double *__restrict__ w, double *__restrict__ df,
-                                                            double *__restrict__ partial, GatherArgs a) {
+template <typename T, int BM>
+__global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::t *__restrict__ planes, const T *__restrict__ B,
+                                                        const double *__restrict__ xi, const double *__restrict__ vext,
+                                                        const double *__restrict__ w, double *__restrict__ df,
+                                                        double *__restrict__ partial, GatherArgs a) {
+    using C = typename Cplx<T>::t;
     constexpr int TM = BM / 16;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char ang_smem[];
+    T *smem = reinterpret_cast<T *>(ang_smem);
     const int K = 2 * a.np, J = a.no;
     const int Kpad = (K + kAngBK - 1) / kAngBK * kAngBK;
     const int lda = BM + 1;
-    double *As = smem;                     // [Kpad][BM+1]
-    double *Bs = As + (size_t)Kpad * lda;  // [BK][BN]
-    double *Cs = Bs + kAngBK * kAngBN;     // [BM][BN+1]
+    T *As = smem;                                    // [Kpad][BM+1]
+    T *Bs = As + ((size_t)Kpad * lda + 3) / 4 * 4;   // [BK][BN]
+    T *Cs = Bs + kAngBK * kAngBN;                    // [BM][BN+1]
     __shared__ double red[3][kAngThreads / 32];
     const long long pt0 = (long long)blockIdx.x * BM;
     const int npts = (int)min((long long)BM, a.N - pt0);
+    const T cst = (T)a.cst;
     for (int f = threadIdx.x; f < (Kpad / 2) * BM; f += blockDim.x) {
         int ip = f / BM, p = f % BM;
-        double2 v = make_double2(0.0, 0.0);
+        C v;
+        v.x = 0;
+        v.y = 0;
         if (p < npts && ip < a.np) {
             v = planes[(size_t)ip * a.N + pt0 + p];
-            v.x *= a.cst;
-            v.y *= a.cst;
+            v.x *= cst;
+            v.y *= cst;
         }
         As[(size_t)(2 * ip) * lda + p] = v.x;
         As[(size_t)(2 * ip + 1) * lda + p] = v.y;
@@ -148,14 +164,14 @@ __global__ void __launch_bounds__(kAngThreads) k_gather_f64(const double2 *__res
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     double fid = 0.0, fext = 0.0, fexc = 0.0;
     for (int j0 = 0; j0 < J; j0 += kAngBN) {
-        double acc[TM][4];
+        T acc[TM][4];
 #pragma unroll
-        for (int i = 0; i < TM; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
+        for (int i = 0; i < TM; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = (T)0;
         for (int k0 = 0; k0 < Kpad; k0 += kAngBK) {
             __syncthreads();
-            ang_load_slab(Bs, B, K, J, k0, j0);
+            ang_load_slab<T>(Bs, B, K, J, k0, j0);
             __syncthreads();
-            ang_slab<TM>(As, lda, Bs, k0, tx, ty, acc);
+            ang_slab<T, TM>(As, lda, Bs, k0, tx, ty, acc);
         }
 #pragma unroll
         for (int i = 0; i < TM; ++i)
@@ -167,7 +183,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather_f64(const double2 *__res
             if (p >= npts || io >= J) continue;
             size_t g = (size_t)(pt0 + p) * J + io;
             double wio = w[io];
-            double vexc = a.prefactor * wio * Cs[p * (kAngBN + 1) + jj];
+            double vexc = a.prefactor * wio * (double)Cs[p * (kAngBN + 1) + jj];
             double x = xi[g];
             fexc += (x * x * a.rho0 - a.rho0) * vexc;
             double dexc = 2.0 * a.rho0 * x * vexc;
@@ -214,13 +230,15 @@ __global__ void __launch_bounds__(kAngThreads) k_gather_f64(const double2 *__res
     }
 }
 
+template <typename T>
 inline size_t project_smem_bytes(int BM, int no) {
     int Kpad = (no + kAngBK - 1) / kAngBK * kAngBK;
-    return sizeof(double) * ((size_t)Kpad * (BM + 1) + kAngBK * kAngBN) + sizeof(double2) * (kAngBN / 2) * BM;
+    return sizeof(T) * (((size_t)Kpad * (BM + 1) + 3) / 4 * 4 + kAngBK * kAngBN) + sizeof(typename Cplx<T>::t) * (kAngBN / 2) * BM;
 }
+template <typename T>
 inline size_t gather_smem_bytes(int BM, int np) {
     int Kpad = (2 * np + kAngBK - 1) / kAngBK * kAngBK;
-    return sizeof(double) * ((size_t)Kpad * (BM + 1) + kAngBK * kAngBN + (size_t)BM * (kAngBN + 1));
+    return sizeof(T) * (((size_t)Kpad * (BM + 1) + 3) / 4 * 4 + kAngBK * kAngBN + (size_t)BM * (kAngBN + 1));
 }
 
 // Sum n rows of 3 partials into out[3] (one block, fixed order).

@@ -57,6 +57,10 @@ struct mdft_handle {
     DevBuf<double> xi, vext, df, w, A, B, partial, sums;
     DevBuf<double2> planes, ctab;
     DevBuf<double2> tw64[3];
+    // mixed path: FP32 projections, c table, twiddles and angular matrices
+    DevBuf<float> A32, B32;
+    DevBuf<float2> planes32, ctab32, tw32[3];
+    int eval_prec = MDFT_PREC_FP64;  // precision of the evaluations run_pipeline performs
     double *h_sums = nullptr;  // pinned {F_id, F_ext, sum_exc}
     int bm_project = 64, bm_gather = 64;
     long long nblk_project = 0, nblk_gather = 0;
@@ -64,8 +68,8 @@ struct mdft_handle {
     Oz2Args oz{};
     DevBuf<int> oz_ints;
     DevBuf<double> oz_dbls;
-    int oz_grid = 0, oz_warps = 8;
-    size_t oz_smem = 0;
+    int oz_grid = 0, oz_warps = 8, oz_grid32 = 0, oz_warps32 = 8;
+    size_t oz_smem = 0, oz_smem32 = 0;
     // timing
     bool timing = false;
     cudaEvent_t ev[ST_COUNT + 1] = {};
@@ -152,11 +156,15 @@ int setup_fft(mdft_handle *h) {
         int rc = upload_twiddles(h->tw64[ax], dims[ax]);
         if (rc) return rc;
         F.tw = h->tw64[ax].p;
+        std::vector<double2> t64(dims[ax]);
+        cudaMemcpy(t64.data(), h->tw64[ax].p, dims[ax] * sizeof(double2), cudaMemcpyDeviceToHost);
+        std::vector<float2> t32(dims[ax]);
+        for (int t = 0; t < dims[ax]; ++t) t32[t] = make_float2((float)t64[t].x, (float)t64[t].y);
+        if ((rc = alloc_check(h->tw32[ax].alloc(dims[ax]), "fft twiddles", dims[ax] * sizeof(float2)))) return rc;
+        cudaMemcpy(h->tw32[ax].p, t32.data(), dims[ax] * sizeof(float2), cudaMemcpyHostToDevice);
     }
     return 0;
 }
-
-bool xy_smem_ok(int n) { return sizeof(double2) * (size_t)n * (n + 2) <= 200 * 1024; }
 
 // Specialised plane (x,y) and column (z) transforms for the supported lengths; the
 // generic per-axis kernel otherwise.
@@ -212,28 +220,33 @@ cudaError_t fft_z(int n, typename Cplx<T>::t *data, long long nplanes, int nx, i
     }
 }
 
-int launch_fft(mdft_handle *h, int sign) {
+template <typename T>
+int launch_fft_t(mdft_handle *h, typename Cplx<T>::t *planes, const void *const *tw, int sign) {
+    using C = typename Cplx<T>::t;
     const Grid &g = h->g;
     bool xy_done = false;
-    if (g.nx == g.ny && xy_smem_ok(g.nx)) {
-        cudaError_t e = fft_xy<double>(g.nx, h->planes.p, (long long)g.np * g.nz, (const double2 *)h->fft[0].tw, sign, h->stream, false);
+    if (g.nx == g.ny && sizeof(C) * (size_t)g.nx * (g.nx + 2) <= 200 * 1024) {
+        cudaError_t e = fft_xy<T>(g.nx, planes, (long long)g.np * g.nz, (const C *)tw[0], sign, h->stream, false);
         if (e == cudaSuccess) { xy_done = true; h->launches += 1; }
         else if (e != cudaErrorNotSupported) return check_cuda(e, "fft xy launch");
         else cudaGetLastError();
     }
     for (int ax = 0; ax < 2 && !xy_done; ++ax) {
         FftAxis &F = h->fft[ax];
-        F.args.sign = sign;
-        k_fft_axis<double><<<F.grid, kFftThreads, F.smem, h->stream>>>(h->planes.p, (const double2 *)F.tw, F.args);
+        FftAxisArgs a = F.args;
+        a.sign = sign;
+        k_fft_axis<T><<<F.grid, kFftThreads, fft_smem_bytes<T>(a.plan.n, a.TL), h->stream>>>(planes, (const C *)tw[ax], a);
         h->launches += 1;
     }
-    cudaError_t e = fft_z<double>(g.nz, h->planes.p, g.np, g.nx, g.ny, (const double2 *)h->fft[2].tw, sign, h->stream, false);
-    if (e == cudaSuccess) { h->launches += 1; }
-    else if (e == cudaErrorNotSupported) {
+    cudaError_t e = fft_z<T>(g.nz, planes, g.np, g.nx, g.ny, (const C *)tw[2], sign, h->stream, false);
+    if (e == cudaSuccess) {
+        h->launches += 1;
+    } else if (e == cudaErrorNotSupported) {
         cudaGetLastError();
         FftAxis &F = h->fft[2];
-        F.args.sign = sign;
-        k_fft_axis<double><<<F.grid, kFftThreads, F.smem, h->stream>>>(h->planes.p, (const double2 *)F.tw, F.args);
+        FftAxisArgs a = F.args;
+        a.sign = sign;
+        k_fft_axis<T><<<F.grid, kFftThreads, fft_smem_bytes<T>(a.plan.n, a.TL), h->stream>>>(planes, (const C *)tw[2], a);
         h->launches += 1;
     } else {
         return check_cuda(e, "fft z launch");
@@ -241,30 +254,47 @@ int launch_fft(mdft_handle *h, int sign) {
     return check_cuda(cudaGetLastError(), "fft launch");
 }
 
+int launch_fft(mdft_handle *h, int sign) {
+    const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
+    return launch_fft_t<double>(h, h->planes.p, tw, sign);
+}
+
 void stage_mark(mdft_handle *h, int i) {
     if (h->timing) cudaEventRecord(h->ev[i], h->stream);
 }
 
 // The excess-term pipeline plus (optionally) the ideal/external term on device
-// arrays; leaves {F_id, F_ext, sum_exc} in h->sums.
-int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode) {
+// arrays, in precision T; leaves {F_id, F_ext, sum_exc} in h->sums.
+template <typename T>
+int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode) {
+    using C = typename Cplx<T>::t;
     const Grid &g = h->g;
+    const bool dbl = sizeof(T) == 8;
+    C *planes = dbl ? (C *)h->planes.p : (C *)h->planes32.p;
+    const T *A = dbl ? (const T *)h->A.p : (const T *)h->A32.p;
+    const T *B = dbl ? (const T *)h->B.p : (const T *)h->B32.p;
+    const C *ctab = dbl ? (const C *)h->ctab.p : (const C *)h->ctab32.p;
+    const void *tw[3];
+    for (int ax = 0; ax < 3; ++ax) tw[ax] = dbl ? (const void *)h->tw64[ax].p : (const void *)h->tw32[ax].p;
     stage_mark(h, 0);
     AngularArgs aa{g.N, g.no, g.np, g.rho0};
     if (h->bm_project == 64)
-        k_project_f64<64><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes(64, g.no), h->stream>>>(d_xi, h->A.p, h->planes.p, aa);
+        k_project<T, 64><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(64, g.no), h->stream>>>(d_xi, A, planes, aa);
     else
-        k_project_f64<32><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes(32, g.no), h->stream>>>(d_xi, h->A.p, h->planes.p, aa);
+        k_project<T, 32><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(32, g.no), h->stream>>>(d_xi, A, planes, aa);
     int rc = check_cuda(cudaGetLastError(), "project launch");
     if (rc) return rc;
     stage_mark(h, 1);
-    if ((rc = launch_fft(h, +1))) return rc;
+    if ((rc = launch_fft_t<T>(h, planes, tw, +1))) return rc;
     stage_mark(h, 2);
-    k_oz2<double><<<h->oz_grid, 32 * h->oz_warps, h->oz_smem, h->stream>>>(h->planes.p, h->ctab.p, h->oz_ints.p,
-                                                                            h->oz_dbls.p, h->oz);
+    Oz2Args oz = h->oz;
+    oz.quirks = dbl ? 1 : 0;
+    const int ozw = dbl ? h->oz_warps : h->oz_warps32;
+    k_oz2<T><<<dbl ? h->oz_grid : h->oz_grid32, 32 * ozw, dbl ? h->oz_smem : h->oz_smem32, h->stream>>>(planes, ctab, h->oz_ints.p,
+                                                                                                       h->oz_dbls.p, oz);
     if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
     stage_mark(h, 3);
-    if ((rc = launch_fft(h, -1))) return rc;
+    if ((rc = launch_fft_t<T>(h, planes, tw, -1))) return rc;
     stage_mark(h, 4);
     GatherArgs ga;
     ga.N = g.N;
@@ -279,16 +309,21 @@ int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal,
     ga.do_ideal = do_ideal;
     ga.df_mode = d_df ? df_mode : 0;
     if (h->bm_gather == 64)
-        k_gather_f64<64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes(64, g.np), h->stream>>>(
-            h->planes.p, h->B.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+        k_gather<T, 64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(64, g.np), h->stream>>>(
+            planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
     else
-        k_gather_f64<32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes(32, g.np), h->stream>>>(
-            h->planes.p, h->B.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+        k_gather<T, 32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(32, g.np), h->stream>>>(
+            planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
     if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
     k_reduce3<<<1, 256, 0, h->stream>>>(h->partial.p, h->nblk_gather, h->sums.p);
-    h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft)
+    h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft_t)
     stage_mark(h, 5);
     return check_cuda(cudaGetLastError(), "reduce launch");
+}
+
+int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode) {
+    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode);
+    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode);
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
@@ -375,29 +410,50 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     if ((rc = alloc_check(h->w.alloc(g.no), "w", g.no * 8))) return rc;
     cudaMemcpy(h->A.p, A.data(), A.size() * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(h->B.p, B.data(), B.size() * 8, cudaMemcpyHostToDevice);
+    {
+        std::vector<float> A32(A.begin(), A.end()), B32(B.begin(), B.end());
+        if ((rc = alloc_check(h->A32.alloc(A32.size()), "A32", A32.size() * 4))) return rc;
+        if ((rc = alloc_check(h->B32.alloc(B32.size()), "B32", B32.size() * 4))) return rc;
+        cudaMemcpy(h->A32.p, A32.data(), A32.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->B32.p, B32.data(), B32.size() * 4, cudaMemcpyHostToDevice);
+        if ((rc = alloc_check(h->planes32.alloc((size_t)g.np * g.N), "FP32 projection planes", (size_t)g.np * g.N * 8))) return rc;
+    }
     cudaMemcpy(h->w.p, g.w.data(), g.no * 8, cudaMemcpyHostToDevice);
     if ((rc = alloc_check(h->ctab.alloc((size_t)h->ct.nq * h->ct.ncoef), "c table", h->ct.c.size() * 8))) return rc;
     cudaMemcpy(h->ctab.p, h->ct.c.data(), h->ct.c.size() * 8, cudaMemcpyHostToDevice);
+    {
+        std::vector<float> c32(h->ct.c.begin(), h->ct.c.end());
+        if ((rc = alloc_check(h->ctab32.alloc((size_t)h->ct.nq * h->ct.ncoef), "FP32 c table", c32.size() * 4))) return rc;
+        cudaMemcpy(h->ctab32.p, c32.data(), c32.size() * 4, cudaMemcpyHostToDevice);
+    }
     if ((rc = check_cuda(cudaGetLastError(), "table upload"))) return rc;
     // launch shapes
     int maxsmem = 0;
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device);
     const size_t dyn_max = (size_t)maxsmem - 1024;  // static shared memory of these kernels is < 1 KB
-    h->bm_project = project_smem_bytes(64, g.no) <= dyn_max ? 64 : 32;
-    h->bm_gather = gather_smem_bytes(64, g.np) <= dyn_max ? 64 : 32;
-    if (project_smem_bytes(h->bm_project, g.no) > dyn_max || gather_smem_bytes(h->bm_gather, g.np) > dyn_max) {
+    h->bm_project = project_smem_bytes<double>(64, g.no) <= dyn_max ? 64 : 32;
+    h->bm_gather = gather_smem_bytes<double>(64, g.np) <= dyn_max ? 64 : 32;
+    if (project_smem_bytes<double>(h->bm_project, g.no) > dyn_max || gather_smem_bytes<double>(h->bm_gather, g.np) > dyn_max) {
         set_error("angular transform tiles do not fit in shared memory");
         return MDFT_E_ARG;
     }
-    if ((rc = allow_smem((const void *)k_project_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_project_f64<32>, maxsmem)) ||
-        (rc = allow_smem((const void *)k_gather_f64<64>, maxsmem)) || (rc = allow_smem((const void *)k_gather_f64<32>, maxsmem)) ||
-        (rc = allow_smem((const void *)k_fft_axis<double>, maxsmem)) || (rc = allow_smem((const void *)k_oz2<double>, maxsmem)))
-        return rc;
+    {
+        const void *fns[] = {(const void *)k_project<double, 64>, (const void *)k_project<double, 32>,
+                             (const void *)k_gather<double, 64>,  (const void *)k_gather<double, 32>,
+                             (const void *)k_project<float, 64>,  (const void *)k_project<float, 32>,
+                             (const void *)k_gather<float, 64>,   (const void *)k_gather<float, 32>,
+                             (const void *)k_fft_axis<double>,    (const void *)k_fft_axis<float>,
+                             (const void *)k_oz2<double>,         (const void *)k_oz2<float>};
+        for (const void *fn : fns)
+            if ((rc = allow_smem(fn, maxsmem))) return rc;
+    }
     for (int n : {g.nx, g.nz}) {
-        cudaError_t e1 = fft_xy<double>(n, nullptr, 0, nullptr, 1, nullptr, true);
-        cudaError_t e2 = fft_z<double>(n, nullptr, 0, g.nx, g.ny, nullptr, 1, nullptr, true);
-        if (e1 != cudaSuccess && e1 != cudaErrorNotSupported) return check_cuda(e1, "fft xy attribute");
-        if (e2 != cudaSuccess && e2 != cudaErrorNotSupported) return check_cuda(e2, "fft z attribute");
+        cudaError_t e[4] = {fft_xy<double>(n, nullptr, 0, nullptr, 1, nullptr, true),
+                            fft_z<double>(n, nullptr, 0, g.nx, g.ny, nullptr, 1, nullptr, true),
+                            fft_xy<float>(n, nullptr, 0, nullptr, 1, nullptr, true),
+                            fft_z<float>(n, nullptr, 0, g.nx, g.ny, nullptr, 1, nullptr, true)};
+        for (cudaError_t x : e)
+            if (x != cudaSuccess && x != cudaErrorNotSupported) return check_cuda(x, "fft attribute");
         cudaGetLastError();
     }
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
@@ -433,7 +489,12 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         h->oz_smem = oz2_smem_bytes<double>(oz, h->oz_warps);
         if (h->oz_smem > dyn_max) { set_error("OZ tile does not fit in shared memory"); return MDFT_E_ARG; }
         h->oz_grid = (int)((oz.nk + h->oz_warps - 1) / h->oz_warps);
+        h->oz_warps32 = 8;
+        while (h->oz_warps32 > 1 && oz2_smem_bytes<float>(oz, h->oz_warps32) > dyn_max) h->oz_warps32 /= 2;
+        h->oz_smem32 = oz2_smem_bytes<float>(oz, h->oz_warps32);
+        h->oz_grid32 = (int)((oz.nk + h->oz_warps32 - 1) / h->oz_warps32);
     }
+    h->eval_prec = h->precision;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "create"))) return rc;
     *out = h.release();
     return MDFT_OK;
@@ -444,7 +505,11 @@ int mdft_destroy(mdft_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->xi.free(); h->vext.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
     h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free(); h->oz_ints.free(); h->oz_dbls.free();
-    for (int i = 0; i < 3; ++i) h->tw64[i].free();
+    for (int i = 0; i < 3; ++i) {
+        h->tw64[i].free();
+        h->tw32[i].free();
+    }
+    h->A32.free(); h->B32.free(); h->planes32.free(); h->ctab32.free();
     lbfgs_free(h->lb);
     h->vpart.free();
     h->vsc.free();

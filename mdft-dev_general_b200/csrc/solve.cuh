@@ -527,8 +527,31 @@ done:
 
 int check_min_opts(const mdft_minimize_opts *o) {
     if (o->m < 1 || o->m > 64 || o->itermax < 1) { set_error("invalid minimiser options"); return MDFT_E_ARG; }
-    if (o->precision != MDFT_PREC_FP64) { set_error("only the FP64 minimiser is available in this build"); return MDFT_E_ARG; }
+    if (o->precision != MDFT_PREC_FP64 && o->precision != MDFT_PREC_MIXED) { set_error("unknown precision %d", o->precision); return MDFT_E_ARG; }
     return 0;
+}
+
+// FP64 solve, or the mixed solve: L-BFGS with FP32-pipeline evaluations, then an FP64
+// polish from that point with a fresh history.  F, max|df| and the status are FP64's.
+int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_result *res) {
+    const int saved = h->eval_prec;
+    int rc;
+    res->evaluations_mixed = 0;
+    if (o->precision == MDFT_PREC_MIXED) {
+        h->eval_prec = MDFT_PREC_MIXED;
+        mdft_minimize_result r1{};
+        rc = minimize_impl(h, o, &r1);
+        if (rc) { h->eval_prec = saved; return rc; }
+        h->eval_prec = MDFT_PREC_FP64;
+        rc = minimize_impl(h, o, res);
+        res->iterations += r1.iterations;
+        res->evaluations_mixed = r1.evaluations;
+    } else {
+        h->eval_prec = MDFT_PREC_FP64;
+        rc = minimize_impl(h, o, res);
+    }
+    h->eval_prec = saved;
+    return rc;
 }
 
 }  // namespace
@@ -542,7 +565,7 @@ int mdft_minimize(mdft_handle *h, double *xi, const mdft_minimize_opts *o, mdft_
     if ((rc = lbfgs_alloc(h, o->m))) return rc;
     LbfgsState &L = h->lb;
     if ((rc = check_cuda(cudaMemcpyAsync(L.x.p, xi, L.n * 8, cudaMemcpyHostToDevice, h->stream), "xi upload"))) return rc;
-    if ((rc = minimize_impl(h, o, res))) return rc;
+    if ((rc = solve_phases(h, o, res))) return rc;
     if ((rc = check_cuda(cudaMemcpyAsync(xi, L.x.p, L.n * 8, cudaMemcpyDeviceToHost, h->stream), "xi download"))) return rc;
     return check_cuda(cudaStreamSynchronize(h->stream), "xi download");
 }
@@ -554,7 +577,7 @@ int mdft_minimize_device(mdft_handle *h, double *d_xi, const mdft_minimize_opts 
     if ((rc = lbfgs_alloc(h, o->m))) return rc;
     LbfgsState &L = h->lb;
     if ((rc = check_cuda(cudaMemcpyAsync(L.x.p, d_xi, L.n * 8, cudaMemcpyDeviceToDevice, h->stream), "xi copy"))) return rc;
-    if ((rc = minimize_impl(h, o, res))) return rc;
+    if ((rc = solve_phases(h, o, res))) return rc;
     if ((rc = check_cuda(cudaMemcpyAsync(d_xi, L.x.p, L.n * 8, cudaMemcpyDeviceToDevice, h->stream), "xi copy"))) return rc;
     return check_cuda(cudaStreamSynchronize(h->stream), "xi copy");
 }
@@ -587,8 +610,11 @@ int pressure_impl(mdft_handle *h, const double *d_xi, double ftot, double lj_tai
     const double deltaN = nwithout - nwith;
     // empty box: xi = 0, no charged-solute corrections (src/module_pressure_correction.f90:117-126)
     if ((rc = check_cuda(cudaMemsetAsync(h->xi.p, 0, nf * 8, st), "xi clear"))) return rc;
-    h->launches += 0;
-    if ((rc = run_pipeline(h, h->xi.p, nullptr, 1, 0))) return rc;
+    const int saved = h->eval_prec;
+    h->eval_prec = MDFT_PREC_FP64;  // the reported free energy is always an FP64 evaluation
+    rc = run_pipeline(h, h->xi.p, nullptr, 1, 0);
+    h->eval_prec = saved;
+    if (rc) return rc;
     double fid, fext, fexc;
     if ((rc = finish_sums(h, &fid, &fext, &fexc))) return rc;
     double f0 = 0.0;
@@ -647,7 +673,7 @@ int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, co
     const double vmax = (-std::log(kEpsDp) - (double)0.05f) * h->g.kT;
     k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, L.x.p, vmax, L.n);
     h->launches += 1;
-    if ((rc = minimize_impl(h, o, res))) return rc;
+    if ((rc = solve_phases(h, o, res))) return rc;
     double pc[4];
     if ((rc = pressure_impl(h, L.x.p, res->f, lj, pc))) return rc;
     out[0] = pc[0];

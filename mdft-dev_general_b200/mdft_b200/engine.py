@@ -55,7 +55,7 @@ class _MinOpts(C.Structure):
 
 class _MinRes(C.Structure):
     _fields_ = [("f", C.c_double), ("pgnorm", C.c_double), ("iterations", C.c_int), ("evaluations", C.c_int),
-                ("status", C.c_int)]
+                ("status", C.c_int), ("evaluations_mixed", C.c_int)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -233,7 +233,8 @@ class Engine:
         o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
         r = _MinRes()
         _check(lib().mdft_minimize(self.h, _p(x), C.byref(o), C.byref(r)))
-        return x, dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status)
+        return x, dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
+                       evaluations_mixed=r.evaluations_mixed)
 
     def guess_density_device(self, d_xi: int):
         _check(lib().mdft_guess_density_device(self.h, C.c_void_p(d_xi)))
@@ -242,7 +243,8 @@ class Engine:
         o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
         r = _MinRes()
         _check(lib().mdft_minimize_device(self.h, C.c_void_p(d_xi), C.byref(o), C.byref(r)))
-        return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status)
+        return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
+                    evaluations_mixed=r.evaluations_mixed)
 
     @property
     def launch_count(self) -> int:
@@ -277,7 +279,8 @@ class Engine:
                                 float(rvdw), float(solvent.eps_r), C.byref(o), _p(xi_out), _p(out), C.byref(r)))
         self.lj_tail = float(out[3])
         return dict(dG=out[0], f=out[1], pmv=out[2], lj_tail=out[3], pbulk=out[4], deltaN=out[5], pgnorm=r.pgnorm,
-                    iterations=r.iterations, evaluations=r.evaluations, status=r.status)
+                    iterations=r.iterations, evaluations=r.evaluations, status=r.status,
+                    evaluations_mixed=r.evaluations_mixed)
 
     def set_timing(self, on=True):
         _check(lib().mdft_set_timing(self.h, 1 if on else 0))
