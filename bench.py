@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--quick", action="store_true", help="small grid smoke run (not a bench number)")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 excess pipeline then an FP64 polish; fp64: plain FP64 solve")
+    ap.add_argument("--pgtol-mixed", type=float, default=0.0, help="FP32-phase stop (<=0: the final pgtol)")
+    ap.add_argument("--polish", type=int, default=0, help="mixed: 1 = FP64 polish phase, 0 = one FP64 evaluation")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
     return ap.parse_args()
@@ -220,7 +222,8 @@ def main():
         print(json.dumps({"evals": args.evals, "f": f, "terms": list(map(float, terms))}))
         eng.close()
         return
-    opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, precision=prec)
+    opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, precision=prec, pgtol_mixed=args.pgtol_mixed,
+                polish=args.polish)
 
     def barrier():
         if world > 1:
@@ -275,7 +278,7 @@ def main():
         dg_ref = [r["dG"] for r in timed]
     else:
         ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
-        dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts, precision=PREC_FP64))["dG"]
+        dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts, precision=PREC_FP64, polish=1))["dG"]
                   for i in range(args.warmup, args.warmup + args.steps)]
         ref.close()
     dg_err = [abs(r["dG"] - d) for r, d in zip(timed, dg_ref)]

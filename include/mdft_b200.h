@@ -131,6 +131,9 @@ typedef struct mdft_minimize_opts {
     double ftol_abs; /* stop when f_old - f <= ftol_abs (factr*epsmch)             */
     int itermax;     /* maximum iterations (maximum_iteration_nbr)                 */
     int precision;   /* MDFT_PREC_* of the evaluations used by this solve          */
+    double pgtol_mixed; /* MIXED: stop the FP32 phase at max|df| <= this (<= 0: pgtol) */
+    int polish;      /* MIXED: 1 = continue with FP64 evaluations until pgtol holds;
+                        0 = one FP64 evaluation at the FP32 phase's result          */
 } mdft_minimize_opts;
 
 typedef struct mdft_minimize_result {
@@ -146,8 +149,9 @@ typedef struct mdft_minimize_result {
  * unconstrained L-BFGS-B of src/module_lbfgs_nocedal_mdft.f90:136-534, run on
  * the device: xi is read from and written to the host buffer.  With
  * MDFT_PREC_MIXED the iterations use FP32 projections/FFTs/OZ until the
- * stopping test holds, then continue with FP64 evaluations (fresh history)
- * until it holds in FP64; f and pgnorm are always FP64 values. */
+ * stopping test (pgtol_mixed) holds, then either continue with FP64
+ * evaluations (fresh history) until pgtol holds in FP64 (polish = 1) or end
+ * with one FP64 evaluation (polish = 0); f and pgnorm are always FP64 values. */
 int mdft_minimize(mdft_handle *h, double *xi, const mdft_minimize_opts *opts, mdft_minimize_result *res);
 
 /* Device-pointer variants (on the handle's stream): d_xi is a device array of

@@ -539,12 +539,23 @@ int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_resu
     res->evaluations_mixed = 0;
     if (o->precision == MDFT_PREC_MIXED) {
         h->eval_prec = MDFT_PREC_MIXED;
+        mdft_minimize_opts o1 = *o;
+        if (o->pgtol_mixed > 0) o1.pgtol = o->pgtol_mixed;
         mdft_minimize_result r1{};
-        rc = minimize_impl(h, o, &r1);
-        if (rc) { h->eval_prec = saved; return rc; }
+        rc = minimize_impl(h, &o1, &r1);
         h->eval_prec = MDFT_PREC_FP64;
-        rc = minimize_impl(h, o, res);
-        res->iterations += r1.iterations;
+        if (!rc && o->polish) {
+            rc = minimize_impl(h, o, res);
+            res->iterations += r1.iterations;
+        } else if (!rc) {
+            // one FP64 evaluation at the FP32 phase's point: f, gradient and max|df| in FP64
+            double f, gmax;
+            rc = eval_fg(h, h->lb.x.p, h->df.p, nullptr, &f, nullptr, &gmax);
+            *res = r1;
+            res->f = f;
+            res->pgnorm = gmax;
+            res->evaluations = 1;
+        }
         res->evaluations_mixed = r1.evaluations;
     } else {
         h->eval_prec = MDFT_PREC_FP64;

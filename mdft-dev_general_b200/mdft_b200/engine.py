@@ -50,7 +50,7 @@ class _Sizes(C.Structure):
 
 class _MinOpts(C.Structure):
     _fields_ = [("m", C.c_int), ("pgtol", C.c_double), ("ftol_abs", C.c_double), ("itermax", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("pgtol_mixed", C.c_double), ("polish", C.c_int)]
 
 
 class _MinRes(C.Structure):
@@ -228,9 +228,10 @@ class Engine:
         _check(lib().mdft_guess_density(self.h, _p(xi)))
         return xi
 
-    def minimize(self, xi, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64):
+    def minimize(self, xi, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64, pgtol_mixed=0.0,
+                 polish=1):
         x = np.array(xi, dtype=np.float64, copy=True).reshape(self.shape)
-        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
         r = _MinRes()
         _check(lib().mdft_minimize(self.h, _p(x), C.byref(o), C.byref(r)))
         return x, dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
@@ -239,8 +240,9 @@ class Engine:
     def guess_density_device(self, d_xi: int):
         _check(lib().mdft_guess_density_device(self.h, C.c_void_p(d_xi)))
 
-    def minimize_device(self, d_xi: int, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64):
-        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
+    def minimize_device(self, d_xi: int, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
+                        pgtol_mixed=0.0, polish=1):
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
         r = _MinRes()
         _check(lib().mdft_minimize_device(self.h, C.c_void_p(d_xi), C.byref(o), C.byref(r)))
         return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
@@ -260,7 +262,7 @@ class Engine:
         return dict(dG=out[0], pmv=out[1], pbulk=out[2], deltaN=out[3])
 
     def solve(self, solute, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
-              xi_out=None):
+              xi_out=None, pgtol_mixed=0.0, polish=1):
         """vext -> guess_density -> L-BFGS -> pressure correction for one solute (main.f90's flow)."""
         q = np.ascontiguousarray(solute.q, dtype=np.float64)
         sg = np.ascontiguousarray(solute.sig, dtype=np.float64)
@@ -272,7 +274,7 @@ class Engine:
         vx = np.array(solvent.xyz, dtype=np.float64)
         if xi_out is not None:
             assert xi_out.dtype == np.float64 and xi_out.flags.c_contiguous and xi_out.size == int(np.prod(self.shape))
-        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision)
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
         r = _MinRes()
         out = np.zeros(6)
         _check(lib().mdft_solve(self.h, len(q), _p(q), _p(sg), _p(ep), _p(xyz), len(vq), _p(vq), _p(vs), _p(ve), _p(vx),
