@@ -5,8 +5,10 @@ Workload (one "step" = one solute solved end to end): a seeded 24-site neutral
 solute (random walk, 1.4-1.6 A bonds inside 6 A, sigma U[2.5,3.8], eps
 U[0.2,1.0], q ~ N(0,0.3) shifted to 0) in SPC/E-like 3-site water, 64^3 grid,
 32 A box, mmax 3, synthetic c(k); vext (LJ + Poisson) -> guess_density ->
-L-BFGS (m=5, stop at max|df| <= 1e-6; the reference's F-decrease test is
-off, it stops ~1 kJ/mol short of the converged dG) -> pressure correction -> dG.  Synthetic inputs stand in for the reference's data.
+L-BFGS (m=5, stop at max|df| <= 1e-4 in FP64; the reference's F-decrease test
+is off, it stops ~1 kJ/mol short of the converged dG) -> pressure correction -> dG.
+Every run re-solves its solutes in FP64 to max|df| <= 1e-6 and reports the largest
+|dG - dG_FP64| (the metric's 0.1 kJ/mol bar).  Synthetic inputs stand in for the reference's data.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -35,6 +37,11 @@ UNIT = "solutes/s"
 N_GRID, BOX, MMAX, NSITE = 64, 32.0, 3, 24
 RVDW = 10.0
 CK_SEED = 20260001
+# Stop rule of the timed solves: max|df| <= 1e-4 in FP64.  On this workload the FP64 dG path
+# is within 0.01-0.03 kJ/mol of its max|df| <= 1e-6 value there; every run checks its dG
+# against an FP64 solve to 1e-6 (PGTOL_REF) and reports the largest deviation.
+PGTOL = 1e-4
+PGTOL_REF = 1e-6
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel (FP64 path),
 # from the ncu captures summarised in profiles/ (None until captured for this kernel)
@@ -51,8 +58,9 @@ def parse():
     ap.add_argument("--quick", action="store_true", help="small grid smoke run (not a bench number)")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 excess pipeline then an FP64 polish; fp64: plain FP64 solve")
+    ap.add_argument("--pgtol", type=float, default=PGTOL, help="stop at max|df| <= pgtol (FP64 gradient)")
     ap.add_argument("--pgtol-mixed", type=float, default=0.0, help="FP32-phase stop (<=0: the final pgtol)")
-    ap.add_argument("--polish", type=int, default=0, help="mixed: 1 = FP64 polish phase, 0 = one FP64 evaluation")
+    ap.add_argument("--polish", type=int, default=1, help="mixed: 1 = FP64 iterations until pgtol, 0 = one FP64 evaluation")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
     return ap.parse_args()
@@ -222,7 +230,7 @@ def main():
         print(json.dumps({"evals": args.evals, "f": f, "terms": list(map(float, terms))}))
         eng.close()
         return
-    opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, precision=prec, pgtol_mixed=args.pgtol_mixed,
+    opts = dict(m=5, pgtol=args.pgtol, ftol_abs=-1.0, itermax=3000, precision=prec, pgtol_mixed=args.pgtol_mixed,
                 polish=args.polish)
 
     def barrier():
@@ -273,14 +281,11 @@ def main():
     h2d = 8 * (4 * s0.nsite + 4 * 3 * 2)  # solute q, sig, eps, xyz + solvent sites
     d2h = xi_host.nbytes + 8 * 6
 
-    # ---- FP64 reference dG of the timed solutes (outside the timed regions) ----
-    if prec == PREC_FP64:
-        dg_ref = [r["dG"] for r in timed]
-    else:
-        ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
-        dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts, precision=PREC_FP64, polish=1))["dG"]
-                  for i in range(args.warmup, args.warmup + args.steps)]
-        ref.close()
+    # ---- FP64 reference dG of the timed solutes, converged to PGTOL_REF (outside the timed regions) ----
+    ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
+    dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts, precision=PREC_FP64, pgtol=PGTOL_REF, polish=1))["dG"]
+              for i in range(args.warmup, args.warmup + args.steps)]
+    ref.close()
     dg_err = [abs(r["dG"] - d) for r, d in zip(timed, dg_ref)]
 
     # ---- roofline of the dominant stage: per-stage CUDA events over evaluations at a converged density ----
@@ -319,7 +324,9 @@ def main():
                            "form": ("plain FP64" if prec == PREC_FP64 else
                                     "mixed: FP32 projections/FFT/OZ with FP64 ideal term, reductions and L-BFGS, "
                                     "then an FP64 polish") + " (vext + guess + L-BFGS m=5 + pressure correction)",
-                           "stop": "max|df|<=1e-6 (line-search stall accepted)", "l2": "inputs larger than L2 (176 MB per field)",
+                           "stop": "max|df|<=%g in FP64 (line-search stall accepted); dG checked against FP64 "
+                                   "solves to max|df|<=%g" % (args.pgtol, PGTOL_REF),
+                           "l2": "inputs larger than L2 (176 MB per field)",
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "evaluations_per_solve": evals,
                            "fp32_evaluations_per_solve": [r.get("evaluations_mixed", 0) for r in timed],

@@ -149,9 +149,10 @@ typedef struct mdft_minimize_result {
  * unconstrained L-BFGS-B of src/module_lbfgs_nocedal_mdft.f90:136-534, run on
  * the device: xi is read from and written to the host buffer.  With
  * MDFT_PREC_MIXED the iterations use FP32 projections/FFTs/OZ until the
- * stopping test (pgtol_mixed) holds, then either continue with FP64
- * evaluations (fresh history) until pgtol holds in FP64 (polish = 1) or end
- * with one FP64 evaluation (polish = 0); f and pgnorm are always FP64 values. */
+ * stopping test (pgtol_mixed) holds or a line search fails, then either
+ * continue with FP64 evaluations, keeping the L-BFGS history, until pgtol
+ * holds in FP64 (polish = 1) or end with one FP64 evaluation (polish = 0);
+ * f and pgnorm are always FP64 values. */
 int mdft_minimize(mdft_handle *h, double *xi, const mdft_minimize_opts *opts, mdft_minimize_result *res);
 
 /* Device-pointer variants (on the handle's stream): d_xi is a device array of

@@ -30,12 +30,15 @@ struct AngularArgs {
     double rho0;
 };
 
+constexpr int kGatherSums = 5;  // per-block partials of k_gather
+
 struct GatherArgs {
     long long N;
     int no, np;
     double rho0, kT, dv, prefactor, cst;  // prefactor = -kT 2 (4 pi^2)/mrso/n0, cst = 1/N
     int do_ideal;                         // add F_id, F_ext and their gradient
     int df_mode;                          // 0 none, 1 store (id + exc), 2 accumulate exc
+    const double *dvec;                   // df_mode 1: also df.dvec (null: df.df is not wanted -> 0)
 };
 
 template <typename T> struct Vec4;
@@ -128,7 +131,9 @@ __global__ void __launch_bounds__(kAngThreads) k_project(const double *__restric
     }
 }
 
-// S7 fused with the ideal + external term.  partial[block] = {F_id, F_ext, sum for F_exc}.
+// S7 fused with the ideal + external term.  partial[block] = {F_id, F_ext, sum for F_exc,
+// df.dvec, max|df|} (the last two only with df_mode 1: the line-search slope and the
+// projected-gradient norm of the minimiser come out of the same pass).
 template <typename T, int BM>
 __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::t *__restrict__ planes, const T *__restrict__ B,
                                                         const double *__restrict__ xi, const double *__restrict__ vext,
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
     T *As = smem;                                    // [Kpad][BM+1]
     T *Bs = As + ((size_t)Kpad * lda + 3) / 4 * 4;   // [BK][BN]
     T *Cs = Bs + kAngBK * kAngBN;                    // [BM][BN+1]
-    __shared__ double red[3][kAngThreads / 32];
+    __shared__ double red[5][kAngThreads / 32];
     const long long pt0 = (long long)blockIdx.x * BM;
     const int npts = (int)min((long long)BM, a.N - pt0);
     const T cst = (T)a.cst;
@@ -162,7 +167,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
         As[(size_t)(2 * ip + 1) * lda + p] = v.y;
     }
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double fid = 0.0, fext = 0.0, fexc = 0.0;
+    double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0;
     for (int j0 = 0; j0 < J; j0 += kAngBN) {
         T acc[TM][4];
 #pragma unroll
@@ -200,8 +205,14 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
                     fid += a.kT * a.dv * wio * a.rho0;
                 }
             }
-            if (a.df_mode == 1) df[g] = did + dexc;
-            else if (a.df_mode == 2) df[g] = df[g] + dexc;
+            if (a.df_mode == 1) {
+                const double gv = did + dexc;
+                df[g] = gv;
+                if (a.dvec) gdv = fma(gv, a.dvec[g], gdv);
+                gmx = fmax(gmx, fabs(gv));
+            } else if (a.df_mode == 2) {
+                df[g] = df[g] + dexc;
+            }
         }
     }
     // block reduction (fixed order -> deterministic)
@@ -209,24 +220,33 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
         fid += __shfl_down_sync(0xffffffffu, fid, off);
         fext += __shfl_down_sync(0xffffffffu, fext, off);
         fexc += __shfl_down_sync(0xffffffffu, fexc, off);
+        gdv += __shfl_down_sync(0xffffffffu, gdv, off);
+        gmx = fmax(gmx, __shfl_down_sync(0xffffffffu, gmx, off));
     }
     int wid = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (lane == 0) {
         red[0][wid] = fid;
         red[1][wid] = fext;
         red[2][wid] = fexc;
+        red[3][wid] = gdv;
+        red[4][wid] = gmx;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s0 = 0, s1 = 0, s2 = 0;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
         for (int i = 0; i < kAngThreads / 32; ++i) {
             s0 += red[0][i];
             s1 += red[1][i];
             s2 += red[2][i];
+            s3 += red[3][i];
+            s4 = fmax(s4, red[4][i]);
         }
-        partial[3 * (size_t)blockIdx.x + 0] = s0;
-        partial[3 * (size_t)blockIdx.x + 1] = s1;
-        partial[3 * (size_t)blockIdx.x + 2] = s2;
+        double *pp = partial + kGatherSums * (size_t)blockIdx.x;
+        pp[0] = s0;
+        pp[1] = s1;
+        pp[2] = s2;
+        pp[3] = s3;
+        pp[4] = s4;
     }
 }
 
@@ -241,32 +261,27 @@ inline size_t gather_smem_bytes(int BM, int np) {
     return sizeof(T) * (((size_t)Kpad * (BM + 1) + 3) / 4 * 4 + kAngBK * kAngBN + (size_t)BM * (kAngBN + 1));
 }
 
-// Sum n rows of 3 partials into out[3] (one block, fixed order).
-__global__ void k_reduce3(const double *__restrict__ partial, long long n, double *__restrict__ out) {
-    __shared__ double s[3][256];
-    double a0 = 0, a1 = 0, a2 = 0;
+// Sum n rows of kGatherSums partials into out[0..4] (one block, fixed order): entries 0-3
+// are sums, entry 4 a maximum.
+__global__ void k_reduce_sums(const double *__restrict__ partial, long long n, double *__restrict__ out) {
+    __shared__ double s[kGatherSums][256];
+    double a[kGatherSums] = {0, 0, 0, 0, 0};
     for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-        a0 += partial[3 * i + 0];
-        a1 += partial[3 * i + 1];
-        a2 += partial[3 * i + 2];
+        const double *pp = partial + kGatherSums * i;
+        for (int j = 0; j < 4; ++j) a[j] += pp[j];
+        a[4] = fmax(a[4], pp[4]);
     }
-    s[0][threadIdx.x] = a0;
-    s[1][threadIdx.x] = a1;
-    s[2][threadIdx.x] = a2;
+    for (int j = 0; j < kGatherSums; ++j) s[j][threadIdx.x] = a[j];
     __syncthreads();
     for (int off = blockDim.x / 2; off > 0; off >>= 1) {
         if ((int)threadIdx.x < off) {
-            s[0][threadIdx.x] += s[0][threadIdx.x + off];
-            s[1][threadIdx.x] += s[1][threadIdx.x + off];
-            s[2][threadIdx.x] += s[2][threadIdx.x + off];
+            for (int j = 0; j < 4; ++j) s[j][threadIdx.x] += s[j][threadIdx.x + off];
+            s[4][threadIdx.x] = fmax(s[4][threadIdx.x], s[4][threadIdx.x + off]);
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[0] = s[0][0];
-        out[1] = s[1][0];
-        out[2] = s[2][0];
-    }
+    if (threadIdx.x == 0)
+        for (int j = 0; j < kGatherSums; ++j) out[j] = s[j][0];
 }
 
 }  // namespace mdft

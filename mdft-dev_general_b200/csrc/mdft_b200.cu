@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 
@@ -14,6 +16,7 @@
 #include "k_oz.cuh"
 #include "k_oz2.cuh"
 #include "k_vec.cuh"
+#include "k_lbfgs.cuh"
 #include "k_vext.cuh"
 
 namespace mdft {
@@ -72,6 +75,7 @@ struct mdft_handle {
     size_t oz_smem = 0, oz_smem32 = 0;
     // timing
     bool timing = false;
+    bool trace = false;  // MDFT_TRACE=1 in the environment at create: per-iteration log on stderr
     cudaEvent_t ev[ST_COUNT + 1] = {};
     double stage_ms[ST_COUNT] = {0};
     int stage_count = 0;
@@ -254,19 +258,14 @@ int launch_fft_t(mdft_handle *h, typename Cplx<T>::t *planes, const void *const 
     return check_cuda(cudaGetLastError(), "fft launch");
 }
 
-int launch_fft(mdft_handle *h, int sign) {
-    const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
-    return launch_fft_t<double>(h, h->planes.p, tw, sign);
-}
-
 void stage_mark(mdft_handle *h, int i) {
     if (h->timing) cudaEventRecord(h->ev[i], h->stream);
 }
 
 // The excess-term pipeline plus (optionally) the ideal/external term on device
-// arrays, in precision T; leaves {F_id, F_ext, sum_exc} in h->sums.
+// arrays, in precision T; leaves {F_id, F_ext, sum_exc, df.dvec, max|df|} in h->sums.
 template <typename T>
-int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode) {
+int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const double *dvec) {
     using C = typename Cplx<T>::t;
     const Grid &g = h->g;
     const bool dbl = sizeof(T) == 8;
@@ -308,6 +307,7 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     ga.cst = 1.0 / (double)(g.nx * g.ny * g.nz);
     ga.do_ideal = do_ideal;
     ga.df_mode = d_df ? df_mode : 0;
+    ga.dvec = dvec;
     if (h->bm_gather == 64)
         k_gather<T, 64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(64, g.np), h->stream>>>(
             planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
@@ -315,19 +315,20 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
         k_gather<T, 32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(32, g.np), h->stream>>>(
             planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
     if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
-    k_reduce3<<<1, 256, 0, h->stream>>>(h->partial.p, h->nblk_gather, h->sums.p);
+    k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, h->nblk_gather, h->sums.p);
     h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft_t)
     stage_mark(h, 5);
     return check_cuda(cudaGetLastError(), "reduce launch");
 }
 
-int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode) {
-    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode);
-    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode);
+// dvec (df_mode 1 only): h_sums[3] = df.dvec, h_sums[4] = max|df| after finish_sums
+int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const double *dvec = nullptr) {
+    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec);
+    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec);
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
-    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
+    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, kGatherSums * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
     if (rc) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "evaluation"))) return rc;
     if (h->timing) {
@@ -378,6 +379,10 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     if (!(d->temperature > 0) || !(d->n0 > 0)) { set_error("temperature and n0 must be positive"); return MDFT_E_ARG; }
     if (d->precision != MDFT_PREC_FP64 && d->precision != MDFT_PREC_MIXED) { set_error("unknown precision %d", d->precision); return MDFT_E_ARG; }
     std::unique_ptr<mdft_handle> h(new mdft_handle());
+    {
+        const char *tr = std::getenv("MDFT_TRACE");
+        h->trace = tr && tr[0] && tr[0] != '0';
+    }
     h->precision = d->precision;
     h->device = d->device;
     // host-side set-up first: argument and c(k) errors do not depend on the device
@@ -458,10 +463,10 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     }
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
     h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
-    if ((rc = alloc_check(h->partial.alloc(3 * (size_t)h->nblk_gather), "partials", 24 * h->nblk_gather))) return rc;
+    if ((rc = alloc_check(h->partial.alloc(kGatherSums * (size_t)h->nblk_gather), "partials", 8 * kGatherSums * h->nblk_gather))) return rc;
     if ((rc = alloc_check(h->sums.alloc(8), "sums", 64))) return rc;
     if ((rc = check_cuda(cudaMallocHost(&h->h_sums, 8 * sizeof(double)), "pinned sums"))) return rc;
-    if ((rc = alloc_check(h->vpart.alloc(2 * kRedBlocks), "reduction partials", 16 * kRedBlocks))) return rc;
+    if ((rc = alloc_check(h->vpart.alloc((size_t)kMaxRows * kRedBlocks), "reduction partials", 8 * kMaxRows * kRedBlocks))) return rc;
     if ((rc = alloc_check(h->vsc.alloc(kScalarSlots), "reduction scalars", 8 * kScalarSlots))) return rc;
     if ((rc = check_cuda(cudaMallocHost(&h->h_vsc, sizeof(double) * kScalarSlots), "pinned scalars"))) return rc;
     if ((rc = setup_fft(h.get()))) return rc;

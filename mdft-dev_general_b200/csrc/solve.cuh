@@ -10,38 +10,21 @@ constexpr double kQfact = 1.602176565e-19 * 1.602176565e-19 * 1.0e-3 * 6.0221412
 
 inline unsigned vec_grid() { return kRedBlocks; }
 
-// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.
+// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g| (both taken in
+// the gather pass that writes g).
 int eval_fg(mdft_handle *h, const double *x, double *g, const double *dvec, double *f, double *gd, double *gmax) {
-    LbfgsState &L = h->lb;
-    int rc = run_pipeline(h, x, g, 1, 1);
+    int rc = run_pipeline(h, x, g, 1, 1, dvec);
     if (rc) return rc;
-    k_dot_max<<<vec_grid(), kRedThreads, 0, h->stream>>>(g, dvec, L.n, h->vpart.p);
-    k_finish_dot_max<<<1, 256, 0, h->stream>>>(h->vpart.p, vec_grid(), h->vsc.p, 0);
-    h->launches += 2;
-    if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc, h->vsc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "scalars"))) return rc;
     double fid, fext, fexc;
     if ((rc = finish_sums(h, &fid, &fext, &fexc))) return rc;
     *f = combine(h, fid, fext, fexc);
-    if (gd) *gd = h->h_vsc[0];
-    if (gmax) *gmax = h->h_vsc[1];
-    if (!std::isfinite(h->h_vsc[0]) || !std::isfinite(h->h_vsc[1])) {
+    const double gdv = h->h_sums[3], gmx = h->h_sums[4];
+    if (gd) *gd = gdv;
+    if (gmax) *gmax = gmx;
+    if (!std::isfinite(gdv) || !std::isfinite(gmx)) {
         set_error("non-finite gradient");
         return MDFT_E_NUMERIC;
     }
-    return 0;
-}
-
-// host value of a.b (a, b device)
-int dev_dot(mdft_handle *h, const double *a, const double *b, double *out) {
-    LbfgsState &L = h->lb;
-    k_dot_max<<<vec_grid(), kRedThreads, 0, h->stream>>>(a, b, L.n, h->vpart.p);
-    k_finish_dot_max<<<1, 256, 0, h->stream>>>(h->vpart.p, vec_grid(), h->vsc.p, 2);
-    h->launches += 2;
-    int rc = check_cuda(cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "dot");
-    (void)L;
-    if (rc) return rc;
-    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "dot"))) return rc;
-    *out = h->h_vsc[2];
     return 0;
 }
 
@@ -53,7 +36,7 @@ int lbfgs_alloc(mdft_handle *h, int m) {
     L.n = n;
     L.m = m;
     int rc;
-    DevBuf<double> *v[] = {&L.x, &L.z, &L.d, &L.t, &L.r, &L.q};
+    DevBuf<double> *v[] = {&L.x, &L.d, &L.t, &L.r};
     for (auto *b : v)
         if ((rc = alloc_check(b->alloc(n), "L-BFGS vector", n * 8))) return rc;
     if ((rc = alloc_check(L.S.alloc((size_t)m * n), "L-BFGS s history", (size_t)m * n * 8))) return rc;
@@ -396,74 +379,274 @@ int mdft_guess_density(const mdft_handle *h, double *xi) {
 namespace {
 
 // The L-BFGS loop on L.x (already holding the start point).
-int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_result *res) {
+// History of the compact limited-memory matrix.  Slots head, head+1, ... (mod m) hold the
+// pairs oldest first; Gram entries are kept by slot: sy[i*m+j] = s_i.y_j (i not newer than
+// j), yy[i*m+j] = y_i.y_j, and sg/yg = s_i.g, y_i.g at the current gradient.
+// Relative rounding noise of F assumed for the FP32 phase of a mixed solve (FP32 planes,
+// FP64 sums): the tolerance of its approximate Wolfe test.
+constexpr double kMixedNoiseRel = 1e-6;
+
+struct LbfgsHist {
+    int m = 0, col = 0, head = 0;
+    double theta = 1.0, gg = 0.0;
+    std::vector<double> sy, yy, sg, yg;
+    void reset(int mm) {
+        m = mm;
+        col = 0;
+        head = 0;
+        theta = 1.0;
+        sy.assign((size_t)m * m, 0.0);
+        yy.assign((size_t)m * m, 0.0);
+        sg.assign(m, 0.0);
+        yg.assign(m, 0.0);
+    }
+    int slot(int c) const { return (head + c) % m; }
+};
+
+constexpr int kRowsBase = 64;  // first device scalar slot of the history inner products
+
+template <int K>
+void launch_pair_dots(int mode, const PairDotsArgs &a, cudaStream_t st) {
+    const unsigned G = vec_grid();
+    if (mode == 0) k_pair_dots<K, 0><<<G, kRedThreads, 0, st>>>(a);
+    else if (mode == 1) k_pair_dots<K, 1><<<G, kRedThreads, 0, st>>>(a);
+    else k_pair_dots<K, 2><<<G, kRedThreads, 0, st>>>(a);
+}
+
+int pair_rows_of(int K, int mode) { return mode == 0 ? 2 * K + 1 : (mode == 1 ? 4 * K + 4 : 4 * K + 1); }
+
+// Inner products of the history with the gradient g; with t >= 0 the new pair
+// s_t = stp d, y_t = g - gold is formed in slot t first and its products with the older
+// slots enter the Gram matrices (the caller sets sy[t][t] and theta).  Blocks on the result.
+int pair_dots(mdft_handle *h, LbfgsHist &H, const double *g, const double *gold, const double *d, double stp, int t) {
+    LbfgsState &L = h->lb;
+    const long long n = L.n;
+    const int m = H.m;
+    cudaStream_t st = h->stream;
+    std::vector<int> olds;
+    for (int c = 0; c < H.col; ++c)
+        if (H.slot(c) != t) olds.push_back(H.slot(c));
+    const int nold = (int)olds.size();
+    const int ngroups = std::max(1, (nold + kPairGroup - 1) / kPairGroup);
+    std::vector<int> base(ngroups), kk(ngroups), mode(ngroups);
+    int off = kRowsBase;
+    for (int gi = 0; gi < ngroups; ++gi) {
+        kk[gi] = std::min(kPairGroup, nold - kPairGroup * gi);
+        mode[gi] = t < 0 ? 0 : (gi == 0 ? 1 : 2);
+        PairDotsArgs a{};
+        a.g = g;
+        a.gold = gold;
+        a.d = d;
+        for (int k = 0; k < kk[gi]; ++k) {
+            a.s[k] = L.S.p + (size_t)olds[kPairGroup * gi + k] * n;
+            a.y[k] = L.Y.p + (size_t)olds[kPairGroup * gi + k] * n;
+        }
+        a.snew = t >= 0 ? L.S.p + (size_t)t * n : nullptr;
+        a.ynew = t >= 0 ? L.Y.p + (size_t)t * n : nullptr;
+        a.stp = stp;
+        a.n = n;
+        a.part = h->vpart.p;
+        switch (kk[gi]) {
+            case 0: launch_pair_dots<0>(mode[gi], a, st); break;
+            case 1: launch_pair_dots<1>(mode[gi], a, st); break;
+            case 2: launch_pair_dots<2>(mode[gi], a, st); break;
+            case 3: launch_pair_dots<3>(mode[gi], a, st); break;
+            case 4: launch_pair_dots<4>(mode[gi], a, st); break;
+            case 5: launch_pair_dots<5>(mode[gi], a, st); break;
+            case 6: launch_pair_dots<6>(mode[gi], a, st); break;
+            case 7: launch_pair_dots<7>(mode[gi], a, st); break;
+            default: launch_pair_dots<8>(mode[gi], a, st); break;
+        }
+        const int rows = pair_rows_of(kk[gi], mode[gi]);
+        k_finish_rows<<<rows, 256, 0, st>>>(h->vpart.p, (int)vec_grid(), h->vsc.p + off);
+        h->launches += 2;
+        base[gi] = off;
+        off += rows;
+    }
+    int rc = check_cuda(cudaGetLastError(), "history inner products");
+    if (rc) return rc;
+    if (off > kScalarSlots) {
+        set_error("history too long for the scalar slots");
+        return MDFT_E_ARG;
+    }
+    if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc + kRowsBase, h->vsc.p + kRowsBase, (off - kRowsBase) * sizeof(double),
+                                         cudaMemcpyDeviceToHost, st), "history inner products"))) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(st), "history inner products"))) return rc;
+    const double *r = h->h_vsc;
+    for (int gi = 0; gi < ngroups; ++gi) {
+        const int K = kk[gi], b = base[gi];
+        for (int k = 0; k < K; ++k) {
+            const int j = olds[kPairGroup * gi + k];
+            H.sg[j] = r[b + k];
+            H.yg[j] = r[b + K + k];
+            if (mode[gi] != 0) {
+                H.sy[(size_t)j * m + t] = r[b + 2 * K + 1 + k];
+                H.yy[(size_t)j * m + t] = H.yy[(size_t)t * m + j] = r[b + 3 * K + 1 + k];
+            }
+        }
+        if (gi == 0) H.gg = r[b + 2 * K];
+        if (mode[gi] == 1) {
+            H.yy[(size_t)t * m + t] = r[b + 4 * K + 1];
+            H.yg[t] = r[b + 4 * K + 2];
+            H.sg[t] = r[b + 4 * K + 3];
+        }
+    }
+    for (int c = 0; c < H.col; ++c) {
+        const int j = H.slot(c);
+        if (!std::isfinite(H.sg[j]) || !std::isfinite(H.yg[j])) {
+            set_error("non-finite history inner product");
+            return MDFT_E_NUMERIC;
+        }
+    }
+    return 0;
+}
+
+template <int K>
+void launch_direction(const DirArgs &a, cudaStream_t st) {
+    k_direction<K><<<vec_grid(), kRedThreads, 0, st>>>(a);
+}
+
+// d = -H g with H the inverse of the compact L-BFGS matrix, H0 = I/theta:
+//   H g = g/theta + S top - Y u/theta,  u = R^-1 S'g,  top = R^-T ((D + Y'Y/theta) u - Y'g/theta)
+// (R = upper triangle of S'Y, D its diagonal; no history: d = -g/theta).  Returns g.d and
+// d.d (blocking).
+int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, double *gd, double *dd) {
+    LbfgsState &L = h->lb;
+    const long long n = L.n;
+    const int k = H.col, m = H.m;
+    cudaStream_t st = h->stream;
+    const double gam = 1.0 / H.theta;
+    std::vector<const double *> vec;
+    std::vector<double> coef;
+    if (k > 0) {
+        std::vector<int> idx(k);
+        for (int c = 0; c < k; ++c) idx[c] = H.slot(c);
+        auto R = [&](int a, int b) { return H.sy[(size_t)idx[a] * m + idx[b]]; };
+        auto YY = [&](int a, int b) { return H.yy[(size_t)idx[a] * m + idx[b]]; };
+        std::vector<double> u(k), w(k), top(k);
+        for (int a = k - 1; a >= 0; --a) {
+            double s = H.sg[idx[a]];
+            for (int b = a + 1; b < k; ++b) s -= R(a, b) * u[b];
+            u[a] = s / R(a, a);
+        }
+        for (int a = 0; a < k; ++a) {
+            double yu = 0.0;
+            for (int b = 0; b < k; ++b) yu += YY(a, b) * u[b];
+            w[a] = R(a, a) * u[a] + gam * yu - gam * H.yg[idx[a]];
+        }
+        for (int a = 0; a < k; ++a) {
+            double s = w[a];
+            for (int b = 0; b < a; ++b) s -= R(b, a) * top[b];
+            top[a] = s / R(a, a);
+        }
+        for (int a = 0; a < k; ++a) {
+            vec.push_back(L.S.p + (size_t)idx[a] * n);
+            coef.push_back(-top[a]);
+            vec.push_back(L.Y.p + (size_t)idx[a] * n);
+            coef.push_back(gam * u[a]);
+        }
+        for (double c : coef)
+            if (!std::isfinite(c)) {
+                set_error("non-finite search-direction coefficient");
+                return MDFT_E_NUMERIC;
+            }
+    }
+    const int nv = (int)vec.size();
+    constexpr int kV = 2 * kPairGroup;
+    const int nl = std::max(1, (nv + kV - 1) / kV);
+    for (int li = 0; li < nl; ++li) {
+        DirArgs a{};
+        a.g = g;
+        a.cg = -gam;
+        const int K = std::min(kV, nv - kV * li);
+        for (int j = 0; j < K; ++j) {
+            a.v[j] = vec[kV * li + j];
+            a.cv[j] = coef[kV * li + j];
+        }
+        a.d = d;
+        a.accumulate = li > 0;
+        a.n = n;
+        a.part = (li == nl - 1) ? h->vpart.p : nullptr;
+        switch (K) {
+            case 0: launch_direction<0>(a, st); break;
+            case 2: launch_direction<2>(a, st); break;
+            case 4: launch_direction<4>(a, st); break;
+            case 6: launch_direction<6>(a, st); break;
+            case 8: launch_direction<8>(a, st); break;
+            case 10: launch_direction<10>(a, st); break;
+            case 12: launch_direction<12>(a, st); break;
+            case 14: launch_direction<14>(a, st); break;
+            default: launch_direction<16>(a, st); break;
+        }
+        h->launches += 1;
+    }
+    k_finish_rows<<<2, 256, 0, st>>>(h->vpart.p, (int)vec_grid(), h->vsc.p + 2);
+    h->launches += 1;
+    int rc = check_cuda(cudaGetLastError(), "direction");
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "direction"))) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(st), "direction"))) return rc;
+    *gd = h->h_vsc[2];
+    *dd = h->h_vsc[3];
+    if (!std::isfinite(*gd) || !std::isfinite(*dd)) {
+        set_error("non-finite search direction");
+        return MDFT_E_NUMERIC;
+    }
+    return 0;
+}
+
+// MDFT_TRACE: one stderr line per accepted iteration with F, max|df| and the particle
+// deficit dN of the current point (dG along the path = F - dN/n0 Pbulk + LJ tail).
+void trace_iter(mdft_handle *h, const double *x, int iter, int nfgv, double f, double gmax, double stp) {
+    if (!h->trace) return;
+    const Grid &g = h->g;
+    k_density_sum<<<vec_grid(), 256, 0, h->stream>>>(x, h->w.p, g.no, (long long)h->lb.n, g.rho0, h->vpart.p);
+    k_finish_dot_max<<<1, 256, 0, h->stream>>>(h->vpart.p, vec_grid(), h->vsc.p, 4);
+    cudaMemcpyAsync(h->h_vsc + 4, h->vsc.p + 4, 8, cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    const double dN = g.n0 * (g.lx * g.ly * g.lz) - h->h_vsc[4] * g.dv;
+    std::fprintf(stderr, "mdft-trace it %d nfg %d prec %s f %.15e gmax %.6e stp %.6e dN %.15e\n", iter, nfgv,
+                 h->eval_prec == MDFT_PREC_MIXED ? "mixed" : "fp64", f, gmax, stp, dN);
+}
+
+// The L-BFGS iteration of src/module_lbfgs_nocedal_mdft.f90 mainlb (no bounds): search
+// direction, Moré-Thuente line search (lnsrlb/dcsrch), stopping tests, matupd.  The
+// current and trial points (x, g) live in two buffer pairs that swap on acceptance, so a
+// rejected trial costs no copies.  H carries the history in and out (an empty H starts
+// from steepest descent with stp = 1/|d|); with stop_on_ls_fail a failed line search
+// ends the run instead of restarting from an empty history; noise_rel > 0 adds the
+// approximate Wolfe acceptance for an F with that relative rounding noise (the FP32
+// phase).  The result is left in L.x.
+int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_result *res, LbfgsHist &H,
+                  bool stop_on_ls_fail, double noise_rel = 0.0) {
     int rc;
     LbfgsState &L = h->lb;
     const long long n = L.n;
     const int m = o->m;
-    const unsigned G = vec_grid();
     cudaStream_t st = h->stream;
-    const long long l0 = h->launches;
-    long long vec_launches = 0;
-    double *g = h->df.p;  // gradient lives in the handle's df buffer
+    if (H.m != m) H.reset(m);
+    double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
-    std::vector<double> rho(m, 0.0);
-    double f = 0, fold = 0, theta = 1.0, stp = 0, gd = 0, gdold = 0, gmax = 0;
-    int col = 0, head = 0, itail = 0, iupdat = 0, iter = 0, nfgv = 0, status = 3;
-    if ((rc = eval_fg(h, L.x.p, g, nullptr, &f, nullptr, &gmax))) return rc;
+    double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0;
+    int iter = 0, nfgv = 0, status = 3;
+    const bool fresh = H.col == 0;
+    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax))) return rc;
     nfgv = 1;
+    trace_iter(h, xc, 0, nfgv, f, gmax, 0.0);
     double sbgnrm = gmax;
     if (sbgnrm <= o->pgtol) { status = 0; goto done; }
+    if (H.col > 0 && (rc = pair_dots(h, H, gc, nullptr, nullptr, 0.0, -1))) return rc;
     while (iter < o->itermax) {
         // ---- search direction ----
-        if (col == 0) {
-            k_sd_step<<<G, 256, 0, st>>>(L.x.p, g, L.z.p, L.d.p, n); ++vec_launches;
-        } else {
-            // two-loop recursion for q = -H g, H0 = I/theta (equal to the compact L-BFGS-B step
-            // of formk/cmprlb/subsm for an unconstrained problem)
-            double *q = L.q.p, *sc = h->vsc.p;
-            auto aslot = [](int j) { return 8 + 2 * j; };
-            auto bslot = [m](int j) { return 8 + 2 * m + 2 * j; };
-            k_neg<<<G, 256, 0, st>>>(g, q, n); ++vec_launches;
-            int jn = (head + col - 1) % m;
-            k_dot_max<<<G, kRedThreads, 0, st>>>(L.S.p + (size_t)jn * n, q, n, h->vpart.p); ++vec_launches;
-            k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, aslot(jn)); ++vec_launches;
-            for (int k = col - 1; k >= 0; --k) {
-                int j = (head + k) % m;
-                int jnext = (k > 0) ? (head + k - 1) % m : -1;
-                k_axpy_dot<<<G, kRedThreads, 0, st>>>(q, L.Y.p + (size_t)j * n, jnext >= 0 ? L.S.p + (size_t)jnext * n : nullptr,
-                                                       n, sc, aslot(j), -rho[j], -1, 0.0, 1.0, jnext >= 0 ? h->vpart.p : nullptr); ++vec_launches;
-                if (jnext >= 0) k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, aslot(jnext)); ++vec_launches;
-            }
-            int j0 = head % m;
-            k_axpy_dot<<<G, kRedThreads, 0, st>>>(q, nullptr, L.Y.p + (size_t)j0 * n, n, sc, -1, 0.0, -1, 0.0, 1.0 / theta, h->vpart.p); ++vec_launches;
-            k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, bslot(j0)); ++vec_launches;
-            for (int k = 0; k < col; ++k) {
-                int j = (head + k) % m;
-                int jnext = (k + 1 < col) ? (head + k + 1) % m : -1;
-                k_axpy_dot<<<G, kRedThreads, 0, st>>>(q, L.S.p + (size_t)j * n, jnext >= 0 ? L.Y.p + (size_t)jnext * n : nullptr, n,
-                                                       sc, aslot(j), rho[j], bslot(j), rho[j], 1.0, jnext >= 0 ? h->vpart.p : nullptr); ++vec_launches;
-                if (jnext >= 0) k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, sc, bslot(jnext)); ++vec_launches;
-            }
-            k_qn_step<<<G, 256, 0, st>>>(L.x.p, q, L.z.p, L.d.p, n); ++vec_launches;
-        }
-        if ((rc = check_cuda(cudaGetLastError(), "direction"))) return rc;
+        if ((rc = direction(h, H, gc, L.d.p, &gd, &dd))) return rc;
         // ---- line search (lnsrlb) ----
         const double stpmx = big;
-        if (iter == 0) {
-            double dtd;
-            if ((rc = dev_dot(h, L.d.p, L.d.p, &dtd))) return rc;
-            stp = std::min(1.0 / std::sqrt(dtd), stpmx);
-        } else {
-            stp = 1.0;
-        }
-        cudaMemcpyAsync(L.t.p, L.x.p, n * 8, cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(L.r.p, g, n * 8, cudaMemcpyDeviceToDevice, st);
+        stp = (iter == 0 && fresh) ? std::min(1.0 / std::sqrt(dd), stpmx) : 1.0;
         fold = f;
-        int ifun = 0, iback = 0, info = 0;
-        if ((rc = dev_dot(h, g, L.d.p, &gd))) return rc;
         gdold = gd;
+        int ifun = 0, iback = 0, info = 0;
+        double gmax_t = gmax;
         LineSearch LS;
         if (gd >= 0.0) {
             info = -4;
@@ -474,49 +657,68 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 ++nfgv;
                 iback = ifun - 1;
                 if (iback >= 20) break;
-                k_trial_point<<<G, 256, 0, st>>>(L.x.p, L.z.p, L.d.p, L.t.p, stp, n); ++vec_launches;
-                if ((rc = eval_fg(h, L.x.p, g, L.d.p, &f, &gd, &gmax))) return rc;
+                k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                h->launches += 1;
+                if ((rc = eval_fg(h, xt, gt, L.d.p, &f, &gd, &gmax_t))) return rc;
+                const double stp_eval = stp;
                 task = dcsrch(f, gd, stp, ftol, gtol, xtol, 0.0, stpmx, false, LS);
+                // Approximate Wolfe test (Hager and Zhang, SIAM J. Optim. 16 (2005) 170, eq. 4.1):
+                // when F carries rounding noise of relative size noise_rel, a trial whose F is
+                // within that noise of F(0) and whose slope satisfies
+                // sigma g'(0) <= g'(stp) <= (2 delta - 1) g'(0) is accepted.
+                if (task == LS_FG && noise_rel > 0.0 && f <= fold + noise_rel * std::fabs(fold) &&
+                    gd >= 0.9 * gdold && gd <= -0.8 * gdold) {
+                    stp = stp_eval;
+                    task = LS_CONV;
+                }
             }
             if (task == LS_ERROR) info = -1;
         }
         if (info != 0 || iback >= 20) {
-            cudaMemcpyAsync(L.x.p, L.t.p, n * 8, cudaMemcpyDeviceToDevice, st);
-            cudaMemcpyAsync(g, L.r.p, n * 8, cudaMemcpyDeviceToDevice, st);
-            f = fold;
-            if (col == 0) {
+            f = fold;  // x and g stay at the last accepted point
+            if (h->trace) std::fprintf(stderr, "mdft-trace line search failed (info %d, iback %d, col %d)\n", info, iback, H.col);
+            if (H.col == 0 || stop_on_ls_fail) {
                 status = 2;
                 ++iter;
                 goto done;
             }
-            col = 0; head = 0; itail = 0; theta = 1.0; iupdat = 0;
+            H.col = 0;
+            H.head = 0;
+            H.theta = 1.0;
             continue;
         }
         ++iter;
+        std::swap(xc, xt);
+        std::swap(gc, gt);
+        gmax = gmax_t;
         sbgnrm = gmax;
+        trace_iter(h, xc, iter, nfgv, f, gmax, stp);
         if (sbgnrm <= o->pgtol) { status = 0; goto done; }
         if ((fold - f) <= o->ftol_abs) { status = 1; goto done; }
         // ---- BFGS update (matupd) ----
-        k_diff_norm<<<G, kRedThreads, 0, st>>>(g, L.r.p, n, h->vpart.p); ++vec_launches;
-        k_finish_dot_max<<<1, 256, 0, st>>>(h->vpart.p, G, h->vsc.p, 2); ++vec_launches;
-        if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, 8, cudaMemcpyDeviceToHost, st), "rr"))) return rc;
-        if ((rc = check_cuda(cudaStreamSynchronize(st), "rr"))) return rc;
-        double rr = h->h_vsc[2], dr, ddum;
+        double dr, ddum;
         if (stp == 1.0) { dr = gd - gdold; ddum = -gdold; }
         else { dr = (gd - gdold) * stp; ddum = -gdold * stp; }
-        if (dr <= epsmch * ddum) continue;  // update skipped
-        ++iupdat;
-        if (iupdat <= m) { col = iupdat; itail = (head + iupdat - 1) % m; }
-        else { itail = (itail + 1) % m; head = (head + 1) % m; }
-        k_scale_copy<<<G, 256, 0, st>>>(L.S.p + (size_t)itail * n, L.d.p, stp, n); ++vec_launches;
-        cudaMemcpyAsync(L.Y.p + (size_t)itail * n, L.r.p, n * 8, cudaMemcpyDeviceToDevice, st);
-        rho[itail] = 1.0 / dr;
-        theta = rr / dr;
+        if (dr <= epsmch * ddum) {  // update skipped: refresh the products with the new g
+            if (H.col > 0 && (rc = pair_dots(h, H, gc, nullptr, nullptr, 0.0, -1))) return rc;
+            continue;
+        }
+        int t;
+        if (H.col < m) {
+            t = H.slot(H.col);
+            ++H.col;
+        } else {
+            t = H.head;
+            H.head = (H.head + 1) % m;
+        }
+        if ((rc = pair_dots(h, H, gc, gt, L.d.p, stp, t))) return rc;
+        H.sy[(size_t)t * m + t] = dr;
+        H.theta = H.yy[(size_t)t * m + t] / dr;
     }
 done:
+    if (xc != L.x.p) cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
+    if (gc != h->df.p) cudaMemcpyAsync(h->df.p, gc, n * 8, cudaMemcpyDeviceToDevice, st);
     if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;
-    h->launches += vec_launches;
-    (void)l0;
     res->f = f;
     res->pgnorm = sbgnrm;
     res->iterations = iter;
@@ -531,25 +733,27 @@ int check_min_opts(const mdft_minimize_opts *o) {
     return 0;
 }
 
-// FP64 solve, or the mixed solve: L-BFGS with FP32-pipeline evaluations, then an FP64
-// polish from that point with a fresh history.  F, max|df| and the status are FP64's.
+// FP64 solve, or the mixed solve: L-BFGS with FP32-pipeline evaluations until its
+// stopping test holds or its line search fails, then (polish) FP64 iterations from that
+// point that keep the history, or one FP64 evaluation.  F, max|df| and the status are FP64's.
 int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_result *res) {
     const int saved = h->eval_prec;
     int rc;
+    LbfgsHist H;
+    H.reset(o->m);
     res->evaluations_mixed = 0;
     if (o->precision == MDFT_PREC_MIXED) {
         h->eval_prec = MDFT_PREC_MIXED;
         mdft_minimize_opts o1 = *o;
         if (o->pgtol_mixed > 0) o1.pgtol = o->pgtol_mixed;
         mdft_minimize_result r1{};
-        rc = minimize_impl(h, &o1, &r1);
+        rc = minimize_impl(h, &o1, &r1, H, true, kMixedNoiseRel);
         h->eval_prec = MDFT_PREC_FP64;
         if (!rc && o->polish) {
-            rc = minimize_impl(h, o, res);
+            rc = minimize_impl(h, o, res, H, false);
             res->iterations += r1.iterations;
         } else if (!rc) {
-            // one FP64 evaluation at the FP32 phase's point: f, gradient and max|df| in FP64
-            double f, gmax;
+            double f = 0.0, gmax = 0.0;
             rc = eval_fg(h, h->lb.x.p, h->df.p, nullptr, &f, nullptr, &gmax);
             *res = r1;
             res->f = f;
@@ -559,7 +763,7 @@ int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_resu
         res->evaluations_mixed = r1.evaluations;
     } else {
         h->eval_prec = MDFT_PREC_FP64;
-        rc = minimize_impl(h, o, res);
+        rc = minimize_impl(h, o, res, H, false);
     }
     h->eval_prec = saved;
     return rc;
@@ -665,7 +869,16 @@ int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, co
     int rc = check_min_opts(o);
     if (rc) return rc;
     double lj = 0.0;
+    auto t0 = std::chrono::steady_clock::now();
+    auto lap = [&](const char *what) {
+        if (!h->trace) return;
+        cudaStreamSynchronize(h->stream);
+        auto t1 = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "mdft-trace time %s %.3f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+        t0 = t1;
+    };
     if ((rc = mdft_compute_vext(h, nsite, q, sig, eps, xyz, nsv, sq, ssig, seps, sxyz, rvdw, &lj))) return rc;
+    lap("vext");
     // charged-solute corrections (src/module_energy_and_gradient.f90:191-204,281-344)
     double qnet = 0.0, quad = 0.0;
     for (int s = 0; s < nsite; ++s) qnet += q[s];
@@ -684,9 +897,12 @@ int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, co
     const double vmax = (-std::log(kEpsDp) - (double)0.05f) * h->g.kT;
     k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, L.x.p, vmax, L.n);
     h->launches += 1;
+    lap("guess");
     if ((rc = solve_phases(h, o, res))) return rc;
+    lap("minimise");
     double pc[4];
     if ((rc = pressure_impl(h, L.x.p, res->f, lj, pc))) return rc;
+    lap("pressure");
     out[0] = pc[0];
     out[1] = res->f;
     out[2] = pc[1];
