@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--pgtol", type=float, default=PGTOL, help="stop at max|df| <= pgtol (FP64 gradient)")
     ap.add_argument("--pgtol-mixed", type=float, default=0.0, help="FP32-phase stop (<=0: the final pgtol)")
     ap.add_argument("--polish", type=int, default=1, help="mixed: 1 = FP64 iterations until pgtol, 0 = one FP64 evaluation")
+    ap.add_argument("--solves", type=int, default=0,
+                    help="profiling mode: only N solves of the workload (no timing, no reference solves)")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
     return ap.parse_args()
@@ -232,6 +234,14 @@ def main():
         return
     opts = dict(m=5, pgtol=args.pgtol, ftol_abs=-1.0, itermax=3000, precision=prec, pgtol_mixed=args.pgtol_mixed,
                 polish=args.polish)
+    if args.solves:
+        # profiling mode: N solves of the timed solutes, nothing else
+        for i in range(args.solves):
+            r = eng.solve(sols[args.warmup + i % args.steps], sv, rvdw=rvdw, **opts)
+        print(json.dumps({"solves": args.solves, "dG": r["dG"], "evaluations": r["evaluations"],
+                          "evaluations_mixed": r["evaluations_mixed"]}))
+        eng.close()
+        return
 
     def barrier():
         if world > 1:

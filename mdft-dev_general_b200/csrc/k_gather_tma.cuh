@@ -1,0 +1,238 @@
+// S7 gather fused with the ideal + external term (same arithmetic as k_gather), as a
+// persistent pipeline: one CTA per SM walks the 32-point tiles blockIdx.x, +gridDim.x, ...
+// For each tile, warp 0 issues bulk copies of the tile's projection chunks (np runs of 32
+// complex values), xi, vext and the search direction (three contiguous 32 x no runs of
+// FP64) into one of two shared-memory stages; the copies of the next tile are in flight
+// while the current one is computed.  The gamma -> orientation matrix B (2np x no) stays
+// in shared memory for the whole launch.
+//
+// Warp w owns points 4w..4w+3 of a tile and lane l the orientations l, l+32, l+64 (NCOL
+// columns of 32), so the matrix products read the projections as broadcasts and B
+// without bank conflicts, and each epilogue store of df is a coalesced 256-byte run.
+// Partial sums (F_id, F_ext, F_exc sum, df.d, max|df|) are kept per thread across tiles
+// and reduced once per CTA in a fixed order.
+//
+// Used when N is a multiple of 32, no <= 96, the pointers are 16-byte aligned and the
+// stages fit in shared memory (mmax <= 3); k_gather covers the rest.
+#pragma once
+
+#include "common.cuh"
+#include "k_angular.cuh"
+#include "k_fft.cuh"
+#include "k_tma.cuh"
+
+namespace mdft {
+
+constexpr int kGtBM = 32;     // points per tile
+constexpr int kGtStages = 2;  // pipeline depth
+constexpr int kGtThreads = 256;
+
+template <typename T>
+__host__ __device__ inline size_t gt_stage_bytes(int np, int no) {
+    return (size_t)np * kGtBM * sizeof(typename Cplx<T>::t) + 3 * (size_t)kGtBM * no * sizeof(double);
+}
+template <typename T>
+__host__ __device__ inline size_t gt_b_bytes(int np, int ncol) {
+    return (size_t)2 * np * 32 * ncol * sizeof(T);
+}
+template <typename T>
+inline size_t gather_tma_smem_bytes(int np, int no, int ncol) {
+    return gt_b_bytes<T>(np, ncol) + kGtStages * gt_stage_bytes<T>(np, no);
+}
+
+// four consecutive complex values from shared memory (32- or 64-byte aligned)
+__device__ __forceinline__ void load4(const float2 *p, float2 (&v)[4]) {
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    v[0] = make_float2(a.x, a.y);
+    v[1] = make_float2(a.z, a.w);
+    v[2] = make_float2(b.x, b.y);
+    v[3] = make_float2(b.z, b.w);
+}
+__device__ __forceinline__ void load4(const double2 *p, double2 (&v)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = p[k];
+}
+
+template <typename T, int NCOL>
+__global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cplx<T>::t *__restrict__ planes,
+                                                              const T *__restrict__ B, const double *__restrict__ xi,
+                                                              const double *__restrict__ vext, const double *__restrict__ w,
+                                                              double *__restrict__ df, double *__restrict__ partial,
+                                                              int *__restrict__ err, GatherArgs a, int ntiles) {
+    using C = typename Cplx<T>::t;
+    constexpr int NC = 32 * NCOL;
+    const int no = a.no, np = a.np, K = 2 * np;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    extern __shared__ __align__(128) unsigned char gt_smem[];
+    T *Bs = reinterpret_cast<T *>(gt_smem);
+    unsigned char *stage0 = gt_smem + gt_b_bytes<T>(np, NCOL);
+    const size_t sbytes = gt_stage_bytes<T>(np, no);
+    const size_t plbytes = (size_t)np * kGtBM * sizeof(C);
+    const size_t fbytes = (size_t)kGtBM * no * sizeof(double);
+    __shared__ uint64_t full[kGtStages];
+    __shared__ int abort_flag;
+    __shared__ double red[kGatherSums][kGtThreads / 32];
+
+    const bool want_v = a.do_ideal != 0, want_d = a.df_mode == 1 && a.dvec != nullptr;
+    const uint32_t tx = (uint32_t)(plbytes + fbytes * (1 + (want_v ? 1 : 0) + (want_d ? 1 : 0)));
+    const int nmine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    auto issue = [&](int i) {  // warp 0: copies of this CTA's i-th tile into stage i % S
+        const int s = i % kGtStages;
+        const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * kGtBM;
+        unsigned char *st = stage0 + s * sbytes;
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], tx);
+        __syncwarp();
+        const int ncopy = np + 3;
+        for (int c = lane; c < ncopy; c += 32) {
+            if (c < np) {
+                bulk_load(st + (size_t)c * kGtBM * sizeof(C), planes + (size_t)c * a.N + pt0, (uint32_t)(kGtBM * sizeof(C)), &full[s]);
+            } else if (c == np) {
+                bulk_load(st + plbytes, xi + pt0 * no, (uint32_t)fbytes, &full[s]);
+            } else if (c == np + 1) {
+                if (want_v) bulk_load(st + plbytes + fbytes, vext + pt0 * no, (uint32_t)fbytes, &full[s]);
+            } else {
+                if (want_d) bulk_load(st + plbytes + 2 * fbytes, a.dvec + pt0 * no, (uint32_t)fbytes, &full[s]);
+            }
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < kGtStages; ++s) mbar_init(&full[s], 1);
+        mbar_fence_init();
+        abort_flag = 0;
+    }
+    __syncthreads();
+    if (warp == 0)
+        for (int i = 0; i < kGtStages && i < nmine; ++i) issue(i);
+    // resident matrix, zero-padded to NC columns
+    for (int f = tid; f < K * NC; f += kGtThreads) {
+        const int k = f / NC, j = f % NC;
+        Bs[f] = j < no ? B[(size_t)k * no + j] : (T)0;
+    }
+    double wv[NCOL];
+#pragma unroll
+    for (int c = 0; c < NCOL; ++c) wv[c] = (lane + 32 * c < no) ? w[lane + 32 * c] : 0.0;
+    __syncthreads();
+
+    const double pre = a.prefactor * a.cst;
+    double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0;
+    for (int i = 0; i < nmine; ++i) {
+        const int s = i % kGtStages;
+        const bool ok = mbar_wait(&full[s], (uint32_t)((i / kGtStages) & 1));
+        if (!ok) abort_flag = 1;
+        if (ok) {
+            const unsigned char *st = stage0 + s * sbytes;
+            const C *pl = reinterpret_cast<const C *>(st);
+            const double *xs = reinterpret_cast<const double *>(st + plbytes);
+            const double *vs = xs + (size_t)kGtBM * no;
+            const double *ds = vs + (size_t)kGtBM * no;
+            T acc[4][NCOL];
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int c = 0; c < NCOL; ++c) acc[p][c] = (T)0;
+#pragma unroll 4
+            for (int ip = 0; ip < np; ++ip) {
+                C av[4];
+                load4(pl + ip * kGtBM + 4 * warp, av);
+                const T *br = Bs + (size_t)(2 * ip) * NC + lane;
+#pragma unroll
+                for (int c = 0; c < NCOL; ++c) {
+                    const T bre = br[32 * c], bim = br[NC + 32 * c];
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) {
+                        acc[p][c] = fma(av[p].x, bre, acc[p][c]);
+                        acc[p][c] = fma(av[p].y, bim, acc[p][c]);
+                    }
+                }
+            }
+            // Epilogue without branches on the data, so that the twelve FP64 logs of a
+            // thread are independent and interleave.  Columns past no have weight 0 and
+            // read a valid element (e = 0); their results are not stored.
+            const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * kGtBM;
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int c = 0; c < NCOL; ++c) {
+                    const int io = lane + 32 * c;
+                    const bool valid = io < no;
+                    const size_t e = valid ? (size_t)(4 * warp + p) * no + io : 0;
+                    const double wio = wv[c];
+                    const double vexc = pre * wio * (double)acc[p][c];
+                    const double x = xs[e];
+                    const double x2 = x * x;
+                    fexc += (x2 * a.rho0 - a.rho0) * vexc;
+                    const double dexc = 2.0 * a.rho0 * x * vexc;
+                    double did = 0.0;
+                    if (want_v) {
+                        const double v = vs[e];
+                        const double rho = x2 * a.rho0;
+                        const bool occ = rho > kEpsDp;
+                        const double lg = log(occ ? x2 : 1.0);  // log(rho / rho0)
+                        fid += a.kT * a.dv * wio * (occ ? rho * lg - rho + a.rho0 : a.rho0);
+                        fext += occ ? a.dv * wio * rho * v : 0.0;
+                        did = occ ? wio * 2.0 * a.rho0 * x * (a.kT * lg + v) : 0.0;
+                    }
+                    if (a.df_mode == 1) {
+                        const double gv = did + dexc;
+                        if (valid) df[pt0 * no + e] = gv;
+                        if (want_d) gdv = fma(gv, ds[e], gdv);
+                        gmx = fmax(gmx, fabs(gv));
+                    }
+                }
+        }
+        __syncthreads();  // stage s fully consumed (and abort_flag visible)
+        if (abort_flag) break;
+        if (warp == 0 && i + kGtStages < nmine) issue(i + kGtStages);
+    }
+    if (abort_flag) {
+        // A copy never completed: report it, then give the copies still in flight (the
+        // failed tile's and, if issued, the next one's) a bounded wait before the CTA exits.
+        if (tid == 0) {
+            atomicExch(err, 1);
+            for (int i = 0; i < nmine; ++i) {
+                const bool done = mbar_try_wait(&full[i % kGtStages], (uint32_t)((i / kGtStages) & 1));
+                if (!done) {
+                    (void)mbar_wait(&full[i % kGtStages], (uint32_t)((i / kGtStages) & 1));
+                    if (i + 1 < nmine) (void)mbar_wait(&full[(i + 1) % kGtStages], (uint32_t)(((i + 1) / kGtStages) & 1));
+                    break;
+                }
+            }
+        }
+        return;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        fid += __shfl_down_sync(0xffffffffu, fid, off);
+        fext += __shfl_down_sync(0xffffffffu, fext, off);
+        fexc += __shfl_down_sync(0xffffffffu, fexc, off);
+        gdv += __shfl_down_sync(0xffffffffu, gdv, off);
+        gmx = fmax(gmx, __shfl_down_sync(0xffffffffu, gmx, off));
+    }
+    if (lane == 0) {
+        red[0][warp] = fid;
+        red[1][warp] = fext;
+        red[2][warp] = fexc;
+        red[3][warp] = gdv;
+        red[4][warp] = gmx;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+        for (int k = 0; k < kGtThreads / 32; ++k) {
+            s0 += red[0][k];
+            s1 += red[1][k];
+            s2 += red[2][k];
+            s3 += red[3][k];
+            s4 = fmax(s4, red[4][k]);
+        }
+        double *pp = partial + kGatherSums * (size_t)blockIdx.x;
+        pp[0] = s0;
+        pp[1] = s1;
+        pp[2] = s2;
+        pp[3] = s3;
+        pp[4] = s4;
+    }
+}
+
+}  // namespace mdft

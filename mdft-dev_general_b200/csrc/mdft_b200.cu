@@ -17,6 +17,7 @@
 #include "k_oz2.cuh"
 #include "k_vec.cuh"
 #include "k_lbfgs.cuh"
+#include "k_gather_tma.cuh"
 #include "k_vext.cuh"
 
 namespace mdft {
@@ -67,6 +68,10 @@ struct mdft_handle {
     double *h_sums = nullptr;  // pinned {F_id, F_ext, sum_exc}
     int bm_project = 64, bm_gather = 64;
     long long nblk_project = 0, nblk_gather = 0;
+    int nsm = 148;
+    int gt_ncol64 = 0, gt_ncol32 = 0;  // k_gather_tma columns of 32 per precision (0: not usable)
+    DevBuf<int> kerr;                  // set by a pipeline kernel whose bounded wait ran out
+    int *h_kerr = nullptr;
     FftAxis fft[3];
     Oz2Args oz{};
     DevBuf<int> oz_ints;
@@ -308,14 +313,28 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     ga.do_ideal = do_ideal;
     ga.df_mode = d_df ? df_mode : 0;
     ga.dvec = dvec;
-    if (h->bm_gather == 64)
+    const int gt_ncol = dbl ? h->gt_ncol64 : h->gt_ncol32;
+    auto al16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+    long long red_blocks = h->nblk_gather;
+    if (gt_ncol > 0 && ga.df_mode != 2 && al16(d_xi) && al16(dvec)) {
+        const int ntiles = (int)(g.N / kGtBM);
+        const int grid = std::min(ntiles, h->nsm);
+        const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
+        if (gt_ncol == 1)
+            k_gather_tma<T, 1><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        else if (gt_ncol == 2)
+            k_gather_tma<T, 2><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        else
+            k_gather_tma<T, 3><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        red_blocks = grid;
+    } else if (h->bm_gather == 64)
         k_gather<T, 64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(64, g.np), h->stream>>>(
             planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
     else
         k_gather<T, 32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(32, g.np), h->stream>>>(
             planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
     if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
-    k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, h->nblk_gather, h->sums.p);
+    k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, red_blocks, h->sums.p);
     h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft_t)
     stage_mark(h, 5);
     return check_cuda(cudaGetLastError(), "reduce launch");
@@ -330,7 +349,13 @@ int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal,
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
     int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, kGatherSums * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
     if (rc) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(h->h_kerr, h->kerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "flag copy"))) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "evaluation"))) return rc;
+    if (*h->h_kerr) {
+        cudaMemsetAsync(h->kerr.p, 0, sizeof(int), h->stream);
+        set_error("a pipeline wait in the gather timed out (bulk copy never completed)");
+        return MDFT_E_CUDA;
+    }
     if (h->timing) {
         for (int i = 0; i < ST_COUNT; ++i) {
             float ms = 0;
@@ -463,7 +488,26 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     }
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
     h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
-    if ((rc = alloc_check(h->partial.alloc(kGatherSums * (size_t)h->nblk_gather), "partials", 8 * kGatherSums * h->nblk_gather))) return rc;
+    cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, d->device);
+    {
+        // persistent bulk-copy gather: N in whole 32-point tiles, no <= 96, stages that fit
+        const int ncol = (g.no + 31) / 32;
+        const bool shape_ok = g.N % kGtBM == 0 && ncol <= 3;
+        h->gt_ncol64 = (shape_ok && gather_tma_smem_bytes<double>(g.np, g.no, ncol) <= dyn_max) ? ncol : 0;
+        h->gt_ncol32 = (shape_ok && gather_tma_smem_bytes<float>(g.np, g.no, ncol) <= dyn_max) ? ncol : 0;
+        const void *fns[] = {(const void *)k_gather_tma<double, 1>, (const void *)k_gather_tma<double, 2>,
+                             (const void *)k_gather_tma<double, 3>, (const void *)k_gather_tma<float, 1>,
+                             (const void *)k_gather_tma<float, 2>,  (const void *)k_gather_tma<float, 3>};
+        for (const void *fn : fns)
+            if ((rc = allow_smem(fn, maxsmem))) return rc;
+    }
+    {
+        const size_t rows = std::max<long long>(h->nblk_gather, h->nsm);
+        if ((rc = alloc_check(h->partial.alloc(kGatherSums * rows), "partials", 8 * kGatherSums * rows))) return rc;
+    }
+    if ((rc = alloc_check(h->kerr.alloc(1), "error flag", 4))) return rc;
+    cudaMemset(h->kerr.p, 0, sizeof(int));
+    if ((rc = check_cuda(cudaMallocHost(&h->h_kerr, sizeof(int)), "pinned flag"))) return rc;
     if ((rc = alloc_check(h->sums.alloc(8), "sums", 64))) return rc;
     if ((rc = check_cuda(cudaMallocHost(&h->h_sums, 8 * sizeof(double)), "pinned sums"))) return rc;
     if ((rc = alloc_check(h->vpart.alloc((size_t)kMaxRows * kRedBlocks), "reduction partials", 8 * kMaxRows * kRedBlocks))) return rc;
@@ -520,6 +564,8 @@ int mdft_destroy(mdft_handle *h) {
     h->vsc.free();
     if (h->h_vsc) cudaFreeHost(h->h_vsc);
     if (h->h_sums) cudaFreeHost(h->h_sums);
+    if (h->h_kerr) cudaFreeHost(h->h_kerr);
+    h->kerr.free();
     for (int i = 0; i <= ST_COUNT; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->stream) cudaStreamDestroy(h->stream);

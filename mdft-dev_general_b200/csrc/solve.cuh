@@ -388,10 +388,12 @@ constexpr double kMixedNoiseRel = 1e-6;
 
 struct LbfgsHist {
     int m = 0, col = 0, head = 0;
-    double theta = 1.0, gg = 0.0;
+    bool f32 = false;                          // pairs stored in FP32 (mixed solves)
+    double theta = 1.0, gg = 0.0, sty = 0.0;  // sty: s.y of the pair formed last, from the stored values
     std::vector<double> sy, yy, sg, yg;
-    void reset(int mm) {
+    void reset(int mm, bool single = false) {
         m = mm;
+        f32 = single;
         col = 0;
         head = 0;
         theta = 1.0;
@@ -405,15 +407,31 @@ struct LbfgsHist {
 
 constexpr int kRowsBase = 64;  // first device scalar slot of the history inner products
 
-template <int K>
-void launch_pair_dots(int mode, const PairDotsArgs &a, cudaStream_t st) {
+template <typename TS, int K, int VEC>
+void launch_pair_dots_v(int mode, const PairDotsArgs &a, cudaStream_t st) {
     const unsigned G = vec_grid();
-    if (mode == 0) k_pair_dots<K, 0><<<G, kRedThreads, 0, st>>>(a);
-    else if (mode == 1) k_pair_dots<K, 1><<<G, kRedThreads, 0, st>>>(a);
-    else k_pair_dots<K, 2><<<G, kRedThreads, 0, st>>>(a);
+    if (mode == 0) k_pair_dots<TS, K, 0, VEC><<<G, kRedThreads, 0, st>>>(a);
+    else if (mode == 1) k_pair_dots<TS, K, 1, VEC><<<G, kRedThreads, 0, st>>>(a);
+    else k_pair_dots<TS, K, 2, VEC><<<G, kRedThreads, 0, st>>>(a);
+}
+template <int K>
+void launch_pair_dots(bool f32, int mode, const PairDotsArgs &a, cudaStream_t st) {
+    const bool v2 = a.n % 2 == 0;
+    if (f32) {
+        if (v2) launch_pair_dots_v<float, K, 2>(mode, a, st);
+        else launch_pair_dots_v<float, K, 1>(mode, a, st);
+    } else {
+        if (v2) launch_pair_dots_v<double, K, 2>(mode, a, st);
+        else launch_pair_dots_v<double, K, 1>(mode, a, st);
+    }
 }
 
-int pair_rows_of(int K, int mode) { return mode == 0 ? 2 * K + 1 : (mode == 1 ? 4 * K + 4 : 4 * K + 1); }
+int pair_rows_of(int K, int mode) { return mode == 0 ? 2 * K + 1 : (mode == 1 ? 4 * K + 5 : 4 * K + 1); }
+
+// slot j of the S or Y history in the storage type of H
+inline void *hist_slot(const LbfgsHist &H, double *base, int j, long long n) {
+    return H.f32 ? (void *)(reinterpret_cast<float *>(base) + (size_t)j * n) : (void *)(base + (size_t)j * n);
+}
 
 // Inner products of the history with the gradient g; with t >= 0 the new pair
 // s_t = stp d, y_t = g - gold is formed in slot t first and its products with the older
@@ -438,24 +456,24 @@ int pair_dots(mdft_handle *h, LbfgsHist &H, const double *g, const double *gold,
         a.gold = gold;
         a.d = d;
         for (int k = 0; k < kk[gi]; ++k) {
-            a.s[k] = L.S.p + (size_t)olds[kPairGroup * gi + k] * n;
-            a.y[k] = L.Y.p + (size_t)olds[kPairGroup * gi + k] * n;
+            a.s[k] = hist_slot(H, L.S.p, olds[kPairGroup * gi + k], n);
+            a.y[k] = hist_slot(H, L.Y.p, olds[kPairGroup * gi + k], n);
         }
-        a.snew = t >= 0 ? L.S.p + (size_t)t * n : nullptr;
-        a.ynew = t >= 0 ? L.Y.p + (size_t)t * n : nullptr;
+        a.snew = t >= 0 ? hist_slot(H, L.S.p, t, n) : nullptr;
+        a.ynew = t >= 0 ? hist_slot(H, L.Y.p, t, n) : nullptr;
         a.stp = stp;
         a.n = n;
         a.part = h->vpart.p;
         switch (kk[gi]) {
-            case 0: launch_pair_dots<0>(mode[gi], a, st); break;
-            case 1: launch_pair_dots<1>(mode[gi], a, st); break;
-            case 2: launch_pair_dots<2>(mode[gi], a, st); break;
-            case 3: launch_pair_dots<3>(mode[gi], a, st); break;
-            case 4: launch_pair_dots<4>(mode[gi], a, st); break;
-            case 5: launch_pair_dots<5>(mode[gi], a, st); break;
-            case 6: launch_pair_dots<6>(mode[gi], a, st); break;
-            case 7: launch_pair_dots<7>(mode[gi], a, st); break;
-            default: launch_pair_dots<8>(mode[gi], a, st); break;
+            case 0: launch_pair_dots<0>(H.f32, mode[gi], a, st); break;
+            case 1: launch_pair_dots<1>(H.f32, mode[gi], a, st); break;
+            case 2: launch_pair_dots<2>(H.f32, mode[gi], a, st); break;
+            case 3: launch_pair_dots<3>(H.f32, mode[gi], a, st); break;
+            case 4: launch_pair_dots<4>(H.f32, mode[gi], a, st); break;
+            case 5: launch_pair_dots<5>(H.f32, mode[gi], a, st); break;
+            case 6: launch_pair_dots<6>(H.f32, mode[gi], a, st); break;
+            case 7: launch_pair_dots<7>(H.f32, mode[gi], a, st); break;
+            default: launch_pair_dots<8>(H.f32, mode[gi], a, st); break;
         }
         const int rows = pair_rows_of(kk[gi], mode[gi]);
         k_finish_rows<<<rows, 256, 0, st>>>(h->vpart.p, (int)vec_grid(), h->vsc.p + off);
@@ -489,6 +507,7 @@ int pair_dots(mdft_handle *h, LbfgsHist &H, const double *g, const double *gold,
             H.yy[(size_t)t * m + t] = r[b + 4 * K + 1];
             H.yg[t] = r[b + 4 * K + 2];
             H.sg[t] = r[b + 4 * K + 3];
+            H.sty = r[b + 4 * K + 4];
         }
     }
     for (int c = 0; c < H.col; ++c) {
@@ -502,8 +521,15 @@ int pair_dots(mdft_handle *h, LbfgsHist &H, const double *g, const double *gold,
 }
 
 template <int K>
-void launch_direction(const DirArgs &a, cudaStream_t st) {
-    k_direction<K><<<vec_grid(), kRedThreads, 0, st>>>(a);
+void launch_direction(bool f32, const DirArgs &a, cudaStream_t st) {
+    const bool v2 = a.n % 2 == 0;
+    if (f32) {
+        if (v2) k_direction<float, K, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<float, K, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    } else {
+        if (v2) k_direction<double, K, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<double, K, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    }
 }
 
 // d = -H g with H the inverse of the compact L-BFGS matrix, H0 = I/theta:
@@ -516,7 +542,7 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
     const int k = H.col, m = H.m;
     cudaStream_t st = h->stream;
     const double gam = 1.0 / H.theta;
-    std::vector<const double *> vec;
+    std::vector<const void *> vec;
     std::vector<double> coef;
     if (k > 0) {
         std::vector<int> idx(k);
@@ -540,9 +566,9 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
             top[a] = s / R(a, a);
         }
         for (int a = 0; a < k; ++a) {
-            vec.push_back(L.S.p + (size_t)idx[a] * n);
+            vec.push_back(hist_slot(H, L.S.p, idx[a], n));
             coef.push_back(-top[a]);
-            vec.push_back(L.Y.p + (size_t)idx[a] * n);
+            vec.push_back(hist_slot(H, L.Y.p, idx[a], n));
             coef.push_back(gam * u[a]);
         }
         for (double c : coef)
@@ -568,15 +594,15 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
         a.n = n;
         a.part = (li == nl - 1) ? h->vpart.p : nullptr;
         switch (K) {
-            case 0: launch_direction<0>(a, st); break;
-            case 2: launch_direction<2>(a, st); break;
-            case 4: launch_direction<4>(a, st); break;
-            case 6: launch_direction<6>(a, st); break;
-            case 8: launch_direction<8>(a, st); break;
-            case 10: launch_direction<10>(a, st); break;
-            case 12: launch_direction<12>(a, st); break;
-            case 14: launch_direction<14>(a, st); break;
-            default: launch_direction<16>(a, st); break;
+            case 0: launch_direction<0>(H.f32, a, st); break;
+            case 2: launch_direction<2>(H.f32, a, st); break;
+            case 4: launch_direction<4>(H.f32, a, st); break;
+            case 6: launch_direction<6>(H.f32, a, st); break;
+            case 8: launch_direction<8>(H.f32, a, st); break;
+            case 10: launch_direction<10>(H.f32, a, st); break;
+            case 12: launch_direction<12>(H.f32, a, st); break;
+            case 14: launch_direction<14>(H.f32, a, st); break;
+            default: launch_direction<16>(H.f32, a, st); break;
         }
         h->launches += 1;
     }
@@ -624,7 +650,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     const long long n = L.n;
     const int m = o->m;
     cudaStream_t st = h->stream;
-    if (H.m != m) H.reset(m);
+    if (H.m != m) H.reset(m, H.f32);
     double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
@@ -657,7 +683,8 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 ++nfgv;
                 iback = ifun - 1;
                 if (iback >= 20) break;
-                k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                if (n % 2 == 0) k_trial2<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n / 2);
+                else k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
                 h->launches += 1;
                 if ((rc = eval_fg(h, xt, gt, L.d.p, &f, &gd, &gmax_t))) return rc;
                 const double stp_eval = stp;
@@ -712,8 +739,10 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
             H.head = (H.head + 1) % m;
         }
         if ((rc = pair_dots(h, H, gc, gt, L.d.p, stp, t))) return rc;
-        H.sy[(size_t)t * m + t] = dr;
-        H.theta = H.yy[(size_t)t * m + t] / dr;
+        // FP64 history: s.y = dr as the reference's matupd; FP32 history: s.y of the stored pair
+        const double sty = H.f32 ? H.sty : dr;
+        H.sy[(size_t)t * m + t] = sty;
+        H.theta = H.yy[(size_t)t * m + t] / sty;
     }
 done:
     if (xc != L.x.p) cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
@@ -740,7 +769,7 @@ int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_resu
     const int saved = h->eval_prec;
     int rc;
     LbfgsHist H;
-    H.reset(o->m);
+    H.reset(o->m, o->precision == MDFT_PREC_MIXED);
     res->evaluations_mixed = 0;
     if (o->precision == MDFT_PREC_MIXED) {
         h->eval_prec = MDFT_PREC_MIXED;
