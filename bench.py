@@ -43,9 +43,9 @@ CK_SEED = 20260001
 PGTOL = 1e-4
 PGTOL_REF = 1e-6
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel (FP64 path),
-# from the ncu captures summarised in profiles/ (None until captured for this kernel)
-NCU_TRAFFIC_BYTES = {}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from the ncu
+# capture summarised in profiles/ncu_oz_gather_project_fp32_64cubed_mmax3.md (absent: null)
+NCU_TRAFFIC_BYTES = {("mixed", "oz"): 67.3e6, ("mixed", "gather"): 562.0e6, ("mixed", "project"): 213.9e6}
 
 
 def parse():
@@ -198,7 +198,7 @@ def reference_arm(args, rank, world):
 
 # evaluations per FP64 solve of the bench workload (updated from the GPU run; used only
 # to scale the CPU per-evaluation time to solutes/s)
-EVALS_PER_SOLVE_FP64 = 60
+EVALS_PER_SOLVE_FP64 = 173  # FP64 solves to max|df| <= 1e-4: 204, 168, 148 evaluations
 
 
 def main():
@@ -310,7 +310,7 @@ def main():
     dom = max(per, key=per.get)
     peak, peak_kind = measured_peak_hbm()
     achieved = sb[dom] / (per[dom] * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC_BYTES.get(dom)
+    traffic = NCU_TRAFFIC_BYTES.get((args.form, dom)) if n == N_GRID else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind, "stage_ms": per,
             "algorithmic_bytes": sb[dom]}

@@ -22,6 +22,12 @@ namespace mdft {
 constexpr int kRecInts = 10;  // dest, fill, sign, special, (x, u) x 3
 constexpr int kRecDbls = 3;   // coefficients
 
+// Term encodings (one int per term): rotation terms jp | r1 << 8 | r2 << 19 (jp < 256,
+// r < 2048); OZ terms ia | jp << 12 | direct << 20 (ia < 4096).  build_oz_tables checks the
+// ranges.
+__host__ __device__ inline int pack_rot_term(int jp, int r1, int r2) { return jp | (r1 << 8) | (r2 << 19); }
+__host__ __device__ inline int pack_oz_term(int ia, int jp, int direct) { return ia | (jp << 12) | (direct << 20); }
+
 struct OzTables {
     std::vector<int> ints;
     std::vector<double> dbls;
@@ -33,8 +39,9 @@ struct OzTables {
 // value = sum_t c_t X_t (x) U_t with X a level-1 entry and U a level l-1 entry (or the zero
 // slot); R[dest] = value and R[fill] = (s Re, -s Im), except at (l,0,0) where the
 // reference's symmetric fill negates Im in place.
-inline void build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
+inline bool build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
     const int M = g.mmax, mrso = g.mrso, np = g.np;
+    if (np >= 256 || rot_off(M + 1) + 1 >= 2048 || ct.ncoef >= 4096) return false;  // term encodings
     auto pidx = [&](int m, int mup, int mu2) { return g.pidx(m, mup, mu2); };
     auto ridx = [](int l, int m, int m1) { return rot_off(l) + (m + l) * (2 * l + 1) + (m1 + l); };
     T.nrot = rot_off(M + 1);
@@ -43,28 +50,16 @@ inline void build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
     for (int o = 0; o < np; ++o) {
         const int m = g.pm[o], khi = g.pmup[o], mu2 = g.pmu[o] / mrso;
         // forward rotation of output (m, khi, mu2): sum over mup (:505-523)
-        for (int mup = -m; mup <= m; ++mup) {
-            fwd.push_back(pidx(m, mup, mu2));
-            fwd.push_back(ridx(m, mup, khi));
-            fwd.push_back(ridx(m, mup, -khi));
-        }
-        fwd_off.push_back((int)fwd.size() / 3);
+        for (int mup = -m; mup <= m; ++mup) fwd.push_back(pack_rot_term(pidx(m, mup, mu2), ridx(m, mup, khi), ridx(m, mup, -khi)));
+        fwd_off.push_back((int)fwd.size());
         // OZ sum of output (m, khi, mu2) (:561-606)
         int ia = ct.ia_start[o];
         for (int n = std::abs(khi); n <= M; ++n)
-            for (int nu2 = -n / mrso; nu2 <= n / mrso; ++nu2, ++ia) {
-                ozt.push_back(ia);
-                ozt.push_back(pidx(n, khi, std::abs(nu2)));
-                ozt.push_back(nu2 < 0 ? 1 : 0);
-            }
-        oz_off.push_back((int)ozt.size() / 3);
+            for (int nu2 = -n / mrso; nu2 <= n / mrso; ++nu2, ++ia) ozt.push_back(pack_oz_term(ia, pidx(n, khi, std::abs(nu2)), nu2 < 0 ? 1 : 0));
+        oz_off.push_back((int)ozt.size());
         // back rotation of output (m, mup, mu2): sum over khi (:626-641)
-        for (int k = -m; k <= m; ++k) {
-            bwd.push_back(pidx(m, k, mu2));
-            bwd.push_back(ridx(m, khi, k));
-            bwd.push_back(ridx(m, khi, -k));
-        }
-        bwd_off.push_back((int)bwd.size() / 3);
+        for (int k = -m; k <= m; ++k) bwd.push_back(pack_rot_term(pidx(m, k, mu2), ridx(m, khi, k), ridx(m, khi, -k)));
+        bwd_off.push_back((int)bwd.size());
         sign.push_back(neg1pow(m));
     }
     RotCoef rc;
@@ -129,6 +124,7 @@ inline void build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
     T.lvl_off = put(lvl);
     T.rec_int = put(rint);
     T.dbls = rdbl;
+    return true;
 }
 
 struct Oz2Args {
@@ -178,7 +174,9 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
     const int per_warp = (a.nrot + 1) + a.ncoef + 6 * np;
     for (int i = threadIdx.x; i < a.n_ints; i += blockDim.x) si[i] = gints[i];
     for (int i = threadIdx.x; i < a.n_dbls; i += blockDim.x) sd[i] = (T)gdbls[i];
-    const long long k0 = (long long)blockIdx.x * W;
+    // persistent: the tables are staged once, then the CTA walks groups of W points
+    for (long long k0 = (long long)blockIdx.x * W; k0 < a.nk; k0 += (long long)gridDim.x * W) {
+    __syncthreads();  // tables staged / the previous group's stores have read wbase
     // coalesced load of the W points (side 0) and their partners (side 1)
     for (int e = threadIdx.x; e < 2 * np * W; e += blockDim.x) {
         const int side = e / (np * W), rem = e % (np * W), ip = rem / W, j = rem % W;
@@ -317,7 +315,7 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
                 C s, t;
                 s.x = s.y = t.x = t.y = 0;
                 for (int k = off[o]; k < off[o + 1]; ++k) {
-                    const int jp = tm[3 * k], r1i = tm[3 * k + 1], r2i = tm[3 * k + 2];
+                    const int tt = tm[k], jp = tt & 255, r1i = (tt >> 8) & 2047, r2i = tt >> 19;
                     cfma(s, dq[jp], Rw[r1i]);
                     cfma(t, dmq[jp], Rw[r2i]);
                 }
@@ -336,7 +334,7 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
                 C s, t;
                 s.x = s.y = t.x = t.y = 0;
                 for (int k = off[ip]; k < off[ip + 1]; ++k) {
-                    const int ia = tm[3 * k], jp = tm[3 * k + 1], direct = tm[3 * k + 2];
+                    const int tt = tm[k], ia = tt & 4095, jp = (tt >> 12) & 255, direct = tt >> 20;
                     const C ce = ceff[ia];
                     if (direct) {
                         cfma(s, ce, rq[jp]);
@@ -369,7 +367,7 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
                 C s, t;
                 s.x = s.y = t.x = t.y = 0;
                 for (int k = off[o]; k < off[o + 1]; ++k) {
-                    const int jp = tm[3 * k], r1i = tm[3 * k + 1], r2i = tm[3 * k + 2];
+                    const int tt = tm[k], jp = tt & 255, r1i = (tt >> 8) & 2047, r2i = tt >> 19;
                     cfmac(s, gq[jp], Rw[r1i]);
                     cfmac(t, gmq[jp], Rw[r2i]);
                 }
@@ -395,6 +393,7 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
         else kidx = ((long long)((a.nz - jz) % a.nz) * a.ny + (a.ny - jy) % a.ny) * a.nx + (a.nx - jx) % a.nx;
         planes[(size_t)ip * a.N + kidx] = wbase[(size_t)j * per_warp + (a.nrot + 1) + a.ncoef + side * np + ip];
     }
+    }  // group loop
 }
 
 }  // namespace mdft

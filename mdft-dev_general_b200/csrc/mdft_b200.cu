@@ -518,7 +518,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         if (h->fft[ax].smem > (size_t)maxsmem) { set_error("FFT tile does not fit in shared memory"); return MDFT_E_ARG; }
     {
         OzTables tb;
-        build_oz_tables(g, h->ct, tb);
+        if (!build_oz_tables(g, h->ct, tb)) { set_error("OZ term tables exceed their index encoding"); return MDFT_E_ARG; }
         if ((rc = alloc_check(h->oz_ints.alloc(tb.ints.size()), "OZ tables", tb.ints.size() * 4))) return rc;
         if ((rc = alloc_check(h->oz_dbls.alloc(std::max<size_t>(1, tb.dbls.size())), "OZ tables", tb.dbls.size() * 8))) return rc;
         cudaMemcpy(h->oz_ints.p, tb.ints.data(), tb.ints.size() * 4, cudaMemcpyHostToDevice);
@@ -537,11 +537,18 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         while (h->oz_warps > 1 && oz2_smem_bytes<double>(oz, h->oz_warps) > dyn_max) h->oz_warps /= 2;
         h->oz_smem = oz2_smem_bytes<double>(oz, h->oz_warps);
         if (h->oz_smem > dyn_max) { set_error("OZ tile does not fit in shared memory"); return MDFT_E_ARG; }
-        h->oz_grid = (int)((oz.nk + h->oz_warps - 1) / h->oz_warps);
+        // persistent grid: as many CTAs as fit on the device at once (tables staged once per CTA)
+        auto oz_grid_of = [&](const void *fn, int warps, size_t smem) {
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * warps, smem);
+            const long long groups = (oz.nk + warps - 1) / warps;
+            return (int)std::min<long long>(groups, (long long)std::max(1, per_sm) * h->nsm);
+        };
+        h->oz_grid = oz_grid_of((const void *)k_oz2<double>, h->oz_warps, h->oz_smem);
         h->oz_warps32 = 8;
         while (h->oz_warps32 > 1 && oz2_smem_bytes<float>(oz, h->oz_warps32) > dyn_max) h->oz_warps32 /= 2;
         h->oz_smem32 = oz2_smem_bytes<float>(oz, h->oz_warps32);
-        h->oz_grid32 = (int)((oz.nk + h->oz_warps32 - 1) / h->oz_warps32);
+        h->oz_grid32 = oz_grid_of((const void *)k_oz2<float>, h->oz_warps32, h->oz_smem32);
     }
     h->eval_prec = h->precision;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "create"))) return rc;
