@@ -1,0 +1,328 @@
+// Rotated OZ step for FP32 evaluations (S3-S5 of src/module_energy_cproj_mrso.f90:441-674,
+// same arithmetic as k_oz2<float>), one thread per (q, -q) pair.
+//
+// Every index of the step -- projection positions, rotation-matrix entries, the terms of the
+// two rotations and of the OZ sums -- is a compile-time function of (MMAX, MRSO), so with the
+// loops unrolled the rotation matrices live in registers and the projections in a per-thread
+// shared-memory slice addressed with immediates.  Only the independent half of each level
+// of R(q) is computed and kept (the recursion's dest entries); the filled half is derived on
+// use as (s Re, -s Im), s = (-1)^(m+m1), as the reference's symmetric fill stores it.
+//
+// Neighbouring threads take neighbouring k-points of one (iz) plane, so the loads of q and
+// of its partner -q from the projection planes are coalesced without staging.  The first
+// c(k) coefficient of each output (ia0) and the recursion coefficients come in as kernel
+// parameters (uniform across the warp).
+#pragma once
+
+#include "common.cuh"
+#include "k_fft.cuh"
+#include "k_oz.cuh"
+#include "k_oz2.cuh"
+
+namespace mdft {
+
+constexpr int kOzpThreads = 128;
+constexpr int kOzpMaxNp = 64;
+constexpr int kOzpMaxRec = 48;
+
+struct OzpParams {
+    int ia0[kOzpMaxNp];        // first c coefficient of each output's OZ sum
+    float rc[3 * kOzpMaxRec];  // recursion coefficients, three per computed entry
+};
+
+template <int MM, int MR> struct OzShape {
+    __host__ __device__ static constexpr int np() {
+        int s = 0;
+        for (int m = 0; m <= MM; ++m) s += (2 * m + 1) * (m / MR + 1);
+        return s;
+    }
+    __host__ __device__ static constexpr int pidx(int m, int mup, int mu2) {
+        int off = 0;
+        for (int k = 0; k < m; ++k) off += (2 * k + 1) * (k / MR + 1);
+        return off + (mup + m) * (m / MR + 1) + mu2;
+    }
+    __host__ __device__ static constexpr int m1min(int m) { return m > 0 ? 1 : 0; }
+    __host__ __device__ static constexpr int level_count(int l) {
+        int c = 0;
+        for (int m = -l; m <= l; ++m) c += l - m1min(m) + 1;
+        return c;
+    }
+    // position of the computed entry (l, m, m1), l >= 2, among all computed entries
+    __host__ __device__ static constexpr int hidx(int l, int m, int m1) {
+        int off = 0;
+        for (int k = 2; k < l; ++k) off += level_count(k);
+        for (int mm = -l; mm < m; ++mm) off += l - m1min(mm) + 1;
+        return off + (m1 - m1min(m));
+    }
+    __host__ __device__ static constexpr int nhalf() {
+        int c = 0;
+        for (int l = 2; l <= MM; ++l) c += level_count(l);
+        return c;
+    }
+};
+
+template <int MM, int MR, int NH>
+__device__ __forceinline__ float2 ozp_rget(const float2 (&R1)[9], const float2 (&Rh)[NH], int l, int m, int m1) {
+    using S = OzShape<MM, MR>;
+    if (l == 0) return make_float2(1.f, 0.f);
+    if (l == 1) return R1[(m + 1) * 3 + (m1 + 1)];
+    if (m1 >= S::m1min(m)) return Rh[S::hidx(l, m, m1)];
+    const float2 v = Rh[S::hidx(l, -m, -m1)];
+    const float s = ((m + m1) & 1) ? -1.f : 1.f;
+    return make_float2(s * v.x, -s * v.y);
+}
+
+__device__ __forceinline__ void ozp_fma(float2 &acc, float2 a, float2 b) {  // acc += a*b
+    acc.x += a.x * b.x - a.y * b.y;
+    acc.y += a.x * b.y + a.y * b.x;
+}
+__device__ __forceinline__ void ozp_fmac(float2 &acc, float2 a, float2 b) {  // acc += a*conj(b)
+    acc.x += a.x * b.x + a.y * b.y;
+    acc.y += a.y * b.x - a.x * b.y;
+}
+
+template <int MM, int MR>
+__global__ void __launch_bounds__(kOzpThreads) k_ozp(float2 *__restrict__ planes, const float2 *__restrict__ ctab, Oz2Args a,
+                                                     OzpParams pp) {
+    using S = OzShape<MM, MR>;
+    constexpr int NP = S::np();
+    constexpr int NH = S::nhalf() > 0 ? S::nhalf() : 1;
+    constexpr int B = kOzpThreads;
+    extern __shared__ __align__(16) float2 ozp_smem[];  // [2 NP][B]: q side, then -q side
+    const int t = threadIdx.x;
+    float2 *sq = ozp_smem + t;            // element ip of the q side: sq[ip * B]
+    float2 *smq = ozp_smem + NP * B + t;  // element ip of the -q side
+    const long long kk = (long long)blockIdx.x * B + t;
+    if (kk >= a.nk) return;
+    const int ix = (int)(kk % a.nx), iy = (int)((kk / a.nx) % a.ny), iz = (int)(kk / ((long long)a.nx * a.ny));
+    const int ixm = (a.nx - ix) % a.nx, iym = (a.ny - iy) % a.ny, izm = (a.nz - iz) % a.nz;
+    if ((iz == 0 || 2 * iz == a.nz) && (long long)iy * a.nx + ix > (long long)iym * a.nx + ixm) return;  // partner is the q
+    const bool selfconj = ix == ixm && iy == iym && iz == izm;
+    const bool nyq = (2 * ix == a.nx) || (2 * iy == a.ny) || (2 * iz == a.nz);
+    const long long kq = ((long long)iz * a.ny + iy) * a.nx + ix;
+    const long long km = ((long long)izm * a.ny + iym) * a.nx + ixm;
+
+    const double qx = (ix <= a.nx / 2 ? ix : ix - a.nx) * a.twopi_lx;
+    const double qy = (iy <= a.ny / 2 ? iy : iy - a.ny) * a.twopi_ly;
+    const double qz = (iz <= a.nz / 2 ? iz : iz - a.nz) * a.twopi_lz;
+
+    // ---- R(q): l = 1 block, then the recursion of src/module_rotation.f90:119-247 ----
+    float2 R1[9];
+    float2 Rh[NH];
+    {
+        float r3[3], r2[3], r1[3];
+        if (qx == 0.0 && qy == 0.0 && qz == 0.0) { r3[0] = 0; r3[1] = 0; r3[2] = 1; }
+        else { r3[0] = (float)qx; r3[1] = (float)qy; r3[2] = (float)qz; }
+        if (r3[0] != 0.f || r3[1] != 0.f) { r2[0] = -r3[1]; r2[1] = r3[0]; r2[2] = 0; }
+        else { r2[0] = 0; r2[1] = r3[2]; r2[2] = -r3[1]; }
+        const float n3 = sqrtf(r3[0] * r3[0] + r3[1] * r3[1] + r3[2] * r3[2]);
+        const float n2 = sqrtf(r2[0] * r2[0] + r2[1] * r2[1] + r2[2] * r2[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { r3[i] /= n3; r2[i] /= n2; }
+        r1[0] = r2[1] * r3[2] - r2[2] * r3[1];
+        r1[1] = r2[2] * r3[0] - r2[0] * r3[2];
+        r1[2] = r2[0] * r3[1] - r2[1] * r3[0];
+        const float sqrt2 = 1.4142135623730950488016887242097f;
+        R1[0] = make_float2((r2[1] + r1[0]) * 0.5f, (r1[1] - r2[0]) * 0.5f);   // (-1,-1)
+        R1[1] = make_float2(r3[0] / sqrt2, r3[1] / sqrt2);                    // (-1, 0)
+        R1[2] = make_float2((r2[1] - r1[0]) * 0.5f, (-r1[1] - r2[0]) * 0.5f);  // (-1, 1)
+        R1[3] = make_float2(r1[2] / sqrt2, -r2[2] / sqrt2);                   // ( 0,-1)
+        R1[4] = make_float2(r3[2], 0.f);                                      // ( 0, 0)
+        R1[5] = make_float2(-r1[2] / sqrt2, -r2[2] / sqrt2);                  // ( 0, 1)
+        R1[6] = make_float2((r2[1] - r1[0]) * 0.5f, (r1[1] + r2[0]) * 0.5f);   // ( 1,-1)
+        R1[7] = make_float2(-r3[0] / sqrt2, r3[1] / sqrt2);                   // ( 1, 0)
+        R1[8] = make_float2((r2[1] + r1[0]) * 0.5f, (r2[0] - r1[1]) * 0.5f);   // ( 1, 1)
+    }
+    if constexpr (MM >= 1) {
+#pragma unroll
+        for (int l = 2; l <= MM; ++l) {
+#pragma unroll
+            for (int m = -l; m <= l; ++m) {
+#pragma unroll
+                for (int m1 = S::m1min(m); m1 <= l; ++m1) {
+                    const int e = S::hidx(l, m, m1);
+                    const int l1 = l - 1;
+                    // terms t = 0..2: coefficient, level-1 entry X, level l-1 entry U
+                    float2 val = make_float2(0.f, 0.f);
+                    auto term = [&](int tt, int xm, int xm1, int um, int um1) {
+                        if (um < -l1 || um > l1 || um1 < -l1 || um1 > l1) return;
+                        const float2 X = R1[(xm + 1) * 3 + (xm1 + 1)];
+                        const float2 U = ozp_rget<MM, MR, NH>(R1, Rh, l1, um, um1);
+                        const float cf = pp.rc[3 * e + tt];
+                        val.x += cf * (X.x * U.x - X.y * U.y);
+                        val.y += cf * (X.x * U.y + X.y * U.x);
+                    };
+                    if (m1 < l) {
+                        if (m == -l) term(0, -1, 0, m + 1, m1);
+                        else if (m == l) term(0, 1, 0, m - 1, m1);
+                        else { term(0, 0, 0, m, m1); term(1, 1, 0, m - 1, m1); term(2, -1, 0, m + 1, m1); }
+                    } else {
+                        if (m == -l) term(0, -1, 1, m + 1, m1 - 1);
+                        else if (m == l) term(0, 1, 1, m - 1, m1 - 1);
+                        else { term(0, 0, 1, m, m1 - 1); term(1, 1, 1, m - 1, m1 - 1); term(2, -1, 1, m + 1, m1 - 1); }
+                    }
+                    Rh[e] = (m == 0 && m1 == 0) ? make_float2(val.x, -val.y) : val;
+                }
+            }
+        }
+        // flush |Re|, |Im| < epsilon(1.) (:491-492); the filled half follows its source
+        auto flush = [](float2 &v) {
+            if (fabsf(v.x) < (float)kEpsSp) v.x = 0.f;
+            if (fabsf(v.y) < (float)kEpsSp) v.y = 0.f;
+        };
+#pragma unroll
+        for (int i = 0; i < 9; ++i) flush(R1[i]);
+#pragma unroll
+        for (int i = 0; i < NH; ++i) flush(Rh[i]);
+    }
+
+    // ---- forward rotation (:505-523), block (m, mu2) at a time, into shared memory ----
+#pragma unroll
+    for (int m = 0; m <= MM; ++m)
+#pragma unroll
+        for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+            float2 dq[2 * MM + 1], dmq[2 * MM + 1];
+#pragma unroll
+            for (int mup = -m; mup <= m; ++mup) {
+                const size_t off = (size_t)S::pidx(m, mup, mu2) * a.N;
+                dq[mup + m] = planes[off + kq];
+                dmq[mup + m] = planes[off + km];
+            }
+            const float sg = (m & 1) ? -1.f : 1.f;
+#pragma unroll
+            for (int khi = -m; khi <= m; ++khi) {
+                float2 s = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int mup = -m; mup <= m; ++mup) {
+                    ozp_fma(s, dq[mup + m], ozp_rget<MM, MR, NH>(R1, Rh, m, mup, khi));
+                    ozp_fma(u, dmq[mup + m], ozp_rget<MM, MR, NH>(R1, Rh, m, mup, -khi));
+                }
+                const int o = S::pidx(m, khi, mu2);
+                sq[o * B] = s;
+                smq[o * B] = make_float2(sg * u.x, sg * u.y);
+            }
+        }
+
+    // ---- interpolated c (:534-539) and the OZ sums (:561-606), one chi block at a time ----
+    const double nrm = sqrt(qx * qx + qy * qy + qz * qz);
+    const double eff = nrm / a.dq + 1.0;
+    const int iq = (int)eff;
+    const float alpha = (float)(eff - iq);
+    const float2 *c0 = ctab + (size_t)(iq - 1) * a.ncoef;
+    const float2 *c1 = ctab + (size_t)iq * a.ncoef;
+#pragma unroll
+    for (int khi = -MM; khi <= MM; ++khi) {
+        constexpr int BMAX = 2 * (MM / MR + 1) * (MM + 1);
+        float2 gs[BMAX], gm[BMAX];
+        int nb = 0;
+#pragma unroll
+        for (int m = (khi < 0 ? -khi : khi); m <= MM; ++m)
+#pragma unroll
+            for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+                const int ip = S::pidx(m, khi, mu2);
+                float2 s = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
+                int k = 0;
+#pragma unroll
+                for (int n = (khi < 0 ? -khi : khi); n <= MM; ++n)
+#pragma unroll
+                    for (int nu2 = -n / MR; nu2 <= n / MR; ++nu2, ++k) {
+                        const int ia = pp.ia0[ip] + k;
+                        const float2 A0 = c0[ia], A1 = c1[ia];
+                        float2 ce;
+                        ce.x = alpha * A1.x + (1.f - alpha) * A0.x;
+                        ce.y = alpha * A1.y + (1.f - alpha) * A0.y;
+                        const int jp = S::pidx(n, khi, nu2 < 0 ? -nu2 : nu2);
+                        if (nu2 < 0) {
+                            ozp_fma(s, ce, sq[jp * B]);
+                            ozp_fma(u, ce, smq[jp * B]);
+                        } else {
+                            ozp_fmac(s, ce, smq[jp * B]);
+                            ozp_fmac(u, ce, sq[jp * B]);
+                        }
+                    }
+                gs[nb] = s;
+                gm[nb] = u;
+                ++nb;
+            }
+        // the block's inputs are no longer needed: write gamma in place
+        nb = 0;
+#pragma unroll
+        for (int m = (khi < 0 ? -khi : khi); m <= MM; ++m)
+#pragma unroll
+            for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+                const int ip = S::pidx(m, khi, mu2);
+                sq[ip * B] = gs[nb];
+                smq[ip * B] = gm[nb];
+                ++nb;
+            }
+    }
+
+    // ---- back rotation with conj(R) (:611-641), straight to the planes ----
+#pragma unroll
+    for (int m = 0; m <= MM; ++m)
+#pragma unroll
+        for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+            float2 g[2 * MM + 1], gmv[2 * MM + 1];
+#pragma unroll
+            for (int k = -m; k <= m; ++k) {
+                g[k + m] = sq[S::pidx(m, k, mu2) * B];
+                gmv[k + m] = smq[S::pidx(m, k, mu2) * B];
+            }
+            const float sg = (m & 1) ? -1.f : 1.f;
+#pragma unroll
+            for (int khi = -m; khi <= m; ++khi) {  // output (m, mup = khi, mu2)
+                float2 s = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int k = -m; k <= m; ++k) {
+                    ozp_fmac(s, g[k + m], ozp_rget<MM, MR, NH>(R1, Rh, m, khi, k));
+                    ozp_fmac(u, gmv[k + m], ozp_rget<MM, MR, NH>(R1, Rh, m, khi, -k));
+                }
+                u.x *= sg;
+                u.y *= sg;
+                if (selfconj && nyq) u.y = -u.y;
+                const size_t off = (size_t)S::pidx(m, khi, mu2) * a.N;
+                if (!selfconj) planes[off + kq] = s;
+                planes[off + km] = u;
+            }
+        }
+}
+
+inline size_t ozp_smem_bytes(int np) { return sizeof(float2) * 2 * (size_t)np * kOzpThreads; }
+
+// Host: parameters of k_ozp for this grid and c table; false when the shape is not covered
+// (then k_oz2<float> runs).  The coefficients and term order mirror build_oz_tables.
+inline bool build_ozp_params(const Grid &g, const CTable &ct, OzpParams &p) {
+    if (g.np > kOzpMaxNp) return false;
+    std::memset(&p, 0, sizeof p);
+    for (int o = 0; o < g.np; ++o) p.ia0[o] = ct.ia_start[o];
+    RotCoef rc;
+    build_rot_coef(rc);
+    int e = 0;
+    for (int l = 2; l <= g.mmax; ++l)
+        for (int m = -l; m <= l; ++m)
+            for (int m1 = (m > 0 ? 1 : 0); m1 <= l; ++m1, ++e) {
+                if (e >= kOzpMaxRec) return false;
+                double c[3] = {0, 0, 0};
+                if (m1 < l) {
+                    if (m == -l) c[0] = rc.b[l][-m + kRMax][m1 + kRMax];
+                    else if (m == l) c[0] = rc.b[l][m + kRMax][m1 + kRMax];
+                    else {
+                        c[0] = rc.a[l][m + kRMax][m1 + kRMax];
+                        c[1] = rc.b[l][m + kRMax][m1 + kRMax];
+                        c[2] = rc.b[l][-m + kRMax][m1 + kRMax];
+                    }
+                } else {
+                    if (m == -l) c[0] = rc.d[l][-m + kRMax];
+                    else if (m == l) c[0] = rc.d[l][m + kRMax];
+                    else {
+                        c[0] = rc.c[l][m + kRMax];
+                        c[1] = rc.d[l][m + kRMax];
+                        c[2] = rc.d[l][-m + kRMax];
+                    }
+                }
+                for (int t = 0; t < 3; ++t) p.rc[3 * e + t] = (float)c[t];
+            }
+    return true;
+}
+
+}  // namespace mdft

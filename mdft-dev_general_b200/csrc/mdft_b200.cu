@@ -18,6 +18,7 @@
 #include "k_vec.cuh"
 #include "k_lbfgs.cuh"
 #include "k_gather_tma.cuh"
+#include "k_ozp.cuh"
 #include "k_vext.cuh"
 
 namespace mdft {
@@ -77,6 +78,8 @@ struct mdft_handle {
     DevBuf<int> oz_ints;
     DevBuf<double> oz_dbls;
     int oz_grid = 0, oz_warps = 8, oz_grid32 = 0, oz_warps32 = 8;
+    bool ozp_ok = false;  // FP32 evaluations use the thread-per-pair k_ozp
+    OzpParams ozp{};
     size_t oz_smem = 0, oz_smem32 = 0;
     // timing
     bool timing = false;
@@ -263,6 +266,34 @@ int launch_fft_t(mdft_handle *h, typename Cplx<T>::t *planes, const void *const 
     return check_cuda(cudaGetLastError(), "fft launch");
 }
 
+// FP32 OZ, thread per pair: the instantiation for (mmax, mrso)
+template <int MM, int MR>
+const void *ozp_fn() { return (const void *)k_ozp<MM, MR>; }
+const void *ozp_kernel(int mmax, int mrso) {
+    if (mrso == 2) {
+        switch (mmax) {
+            case 0: return ozp_fn<0, 2>();
+            case 1: return ozp_fn<1, 2>();
+            case 2: return ozp_fn<2, 2>();
+            case 3: return ozp_fn<3, 2>();
+        }
+    } else if (mrso == 1) {
+        switch (mmax) {
+            case 0: return ozp_fn<0, 1>();
+            case 1: return ozp_fn<1, 1>();
+            case 2: return ozp_fn<2, 1>();
+        }
+    }
+    return nullptr;
+}
+void launch_ozp(mdft_handle *h, float2 *planes, const float2 *ctab, const Oz2Args &oz) {
+    const Grid &g = h->g;
+    const unsigned grid = (unsigned)((oz.nk + kOzpThreads - 1) / kOzpThreads);
+    const size_t smem = ozp_smem_bytes(g.np);
+    void *args[] = {(void *)&planes, (void *)&ctab, (void *)&oz, (void *)&h->ozp};
+    cudaLaunchKernel(ozp_kernel(g.mmax, g.mrso), dim3(grid), dim3(kOzpThreads), args, smem, h->stream);
+}
+
 void stage_mark(mdft_handle *h, int i) {
     if (h->timing) cudaEventRecord(h->ev[i], h->stream);
 }
@@ -294,8 +325,11 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     Oz2Args oz = h->oz;
     oz.quirks = dbl ? 1 : 0;
     const int ozw = dbl ? h->oz_warps : h->oz_warps32;
-    k_oz2<T><<<dbl ? h->oz_grid : h->oz_grid32, 32 * ozw, dbl ? h->oz_smem : h->oz_smem32, h->stream>>>(planes, ctab, h->oz_ints.p,
-                                                                                                       h->oz_dbls.p, oz);
+    if (!dbl && h->ozp_ok)
+        launch_ozp(h, (float2 *)planes, (const float2 *)ctab, oz);
+    else
+        k_oz2<T><<<dbl ? h->oz_grid : h->oz_grid32, 32 * ozw, dbl ? h->oz_smem : h->oz_smem32, h->stream>>>(planes, ctab, h->oz_ints.p,
+                                                                                                           h->oz_dbls.p, oz);
     if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
     stage_mark(h, 3);
     if ((rc = launch_fft_t<T>(h, planes, tw, -1))) return rc;
@@ -549,6 +583,12 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         while (h->oz_warps32 > 1 && oz2_smem_bytes<float>(oz, h->oz_warps32) > dyn_max) h->oz_warps32 /= 2;
         h->oz_smem32 = oz2_smem_bytes<float>(oz, h->oz_warps32);
         h->oz_grid32 = oz_grid_of((const void *)k_oz2<float>, h->oz_warps32, h->oz_smem32);
+        // thread-per-pair FP32 OZ where an instantiation exists and its slice fits
+        const void *fn = ozp_kernel(g.mmax, g.mrso);
+        if (fn && build_ozp_params(g, h->ct, h->ozp) && ozp_smem_bytes(g.np) <= dyn_max) {
+            if ((rc = allow_smem(fn, maxsmem))) return rc;
+            h->ozp_ok = true;
+        }
     }
     h->eval_prec = h->precision;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "create"))) return rc;
