@@ -147,9 +147,11 @@ __global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cpl
                     }
                 }
             }
-            // Epilogue without branches on the data, so that the twelve FP64 logs of a
-            // thread are independent and interleave.  Columns past no have weight 0 and
-            // read a valid element (e = 0); their results are not stored.
+            // Epilogue without branches on the data, so that the logs of a thread are
+            // independent and interleave.  Columns past no have weight 0 and read a valid
+            // element (e = 0); their results are not stored.  FP64 evaluations do the
+            // per-element arithmetic in FP64; FP32 evaluations in FP32 (the pipeline's own
+            // precision).  The sums are FP64 in both.
             const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * kGtBM;
 #pragma unroll
             for (int p = 0; p < 4; ++p)
@@ -158,24 +160,25 @@ __global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cpl
                     const int io = lane + 32 * c;
                     const bool valid = io < no;
                     const size_t e = valid ? (size_t)(4 * warp + p) * no + io : 0;
-                    const double wio = wv[c];
-                    const double vexc = pre * wio * (double)acc[p][c];
-                    const double x = xs[e];
-                    const double x2 = x * x;
-                    fexc += (x2 * a.rho0 - a.rho0) * vexc;
-                    const double dexc = 2.0 * a.rho0 * x * vexc;
-                    double did = 0.0;
+                    const T wio = (T)wv[c], r0 = (T)a.rho0;
+                    const T vexc = (T)pre * wio * acc[p][c];
+                    const T x = (T)xs[e];
+                    const T x2 = x * x;
+                    fexc += (double)((x2 * r0 - r0) * vexc);
+                    const T dexc = (T)2 * r0 * x * vexc;
+                    T did = (T)0;
                     if (want_v) {
-                        const double v = vs[e];
-                        const double rho = x2 * a.rho0;
-                        const bool occ = rho > kEpsDp;
-                        const double lg = log(occ ? x2 : 1.0);  // log(rho / rho0)
-                        fid += a.kT * a.dv * wio * (occ ? rho * lg - rho + a.rho0 : a.rho0);
-                        fext += occ ? a.dv * wio * rho * v : 0.0;
-                        did = occ ? wio * 2.0 * a.rho0 * x * (a.kT * lg + v) : 0.0;
+                        const T v = (T)vs[e];
+                        const T rho = x2 * r0;
+                        const bool occ = (double)rho > kEpsDp;
+                        const T lg = log(occ ? x2 : (T)1);  // log(rho / rho0)
+                        const T kTdv = (T)(a.kT * a.dv), dv = (T)a.dv, kT = (T)a.kT;
+                        fid += (double)(kTdv * wio * (occ ? rho * lg - rho + r0 : r0));
+                        fext += occ ? (double)(dv * wio * rho * v) : 0.0;
+                        did = occ ? wio * (T)2 * r0 * x * (kT * lg + v) : (T)0;
                     }
                     if (a.df_mode == 1) {
-                        const double gv = did + dexc;
+                        const double gv = (double)(did + dexc);
                         if (valid) df[pt0 * no + e] = gv;
                         if (want_d) gdv = fma(gv, ds[e], gdv);
                         gmx = fmax(gmx, fabs(gv));

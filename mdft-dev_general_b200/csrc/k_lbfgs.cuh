@@ -4,8 +4,9 @@
 // no bounds) is formed as  d = cg g + sum_i a_i s_i + sum_i b_i y_i  with the 2m+1
 // coefficients computed on the host from small Gram matrices (Byrd, Nocedal and Schnabel,
 // Math. Prog. 63 (1994), eq. 3.1 in inverse form).  A step therefore reads each history
-// vector twice -- once for its inner products with the new gradient (k_pair_dots, which also
-// forms and stores the new pair), once for the combination (k_direction) -- instead of the
+// vector twice -- once for its inner products with the trial gradient (k_pair_dots, run
+// right after each trial evaluation, before the one host synchronisation of the step), once
+// for the combination (k_direction, which also stores the accepted pair) -- instead of the
 // four passes per pair of the two-loop recursion.
 //
 // History storage TS: double (FP64 solves, the reference's arithmetic) or float (mixed
@@ -21,23 +22,24 @@
 namespace mdft {
 
 constexpr int kPairGroup = 8;                 // history slots read per k_pair_dots launch
-constexpr int kMaxRows = 4 * kPairGroup + 5;  // reduction rows of one launch
+constexpr int kMaxRows = 4 * kPairGroup + 5;  // reduction rows of one k_pair_dots launch
 
-// MODE 0: rows s_i.g [0,K), y_i.g [K,2K), g.g [2K]
-// MODE 1: forms s_new = stp d and y_new = g - gold (stored), rows as MODE 0 plus
-//         s_i.y_new [2K+1,3K+1), y_i.y_new [3K+1,4K+1), y_new.y_new, y_new.g, s_new.g, s_new.y_new
-// MODE 2: y_new read back from ynew; rows as MODE 1 without the last four
+// Inner products of the history slots s_i, y_i (K of them) with a gradient g:
+//   rows s_i.g [0,K), y_i.g [K,2K), g.g [2K]
+// PAIR: also with the candidate pair s_n = stp d, y_n = g - gold, formed on the fly and
+//   rounded to the storage type exactly as k_direction will store it (nothing is written):
+//   rows s_i.y_n [2K+1,3K+1), y_i.y_n [3K+1,4K+1)
+// SELF (with PAIR): the candidate's own rows y_n.y_n, y_n.g, s_n.g, s_n.y_n [4K+1,4K+5)
 struct PairDotsArgs {
     const double *g, *gold, *d;
     const void *s[kPairGroup], *y[kPairGroup];
-    void *snew, *ynew;
     double stp;
     long long n;
     double *part;  // [rows][gridDim.x]
 };
 
-template <int K, int MODE> __host__ __device__ constexpr int pair_rows() {
-    return MODE == 0 ? 2 * K + 1 : (MODE == 1 ? 4 * K + 5 : 4 * K + 1);
+__host__ __device__ constexpr int pair_rows(int K, bool pair, bool self) {
+    return 2 * K + 1 + (pair ? 2 * K : 0) + (pair && self ? 4 : 0);
 }
 
 template <int R>
@@ -62,24 +64,20 @@ template <typename TS> struct Pair2;
 template <> struct Pair2<double> { using t = double2; };
 template <> struct Pair2<float> { using t = float2; };
 
-// one element i: sk, yk are the old slots' values there
-template <typename TS, int K, int MODE>
-__device__ __forceinline__ void pair_dots_elem(const PairDotsArgs &a, TS *snew, TS *ynew, long long i, double gi, double goldi,
-                                               double di, double (&acc)[pair_rows<K, MODE>()], const TS *sk, const TS *yk) {
+// one element: sk, yk are the slots' values there
+template <typename TS, int K, bool PAIR, bool SELF>
+__device__ __forceinline__ void pair_dots_elem(double stp, double gi, double goldi, double di, double (&acc)[pair_rows(K, PAIR, SELF)],
+                                               const TS *sk, const TS *yk) {
     double yn = 0.0;
-    if constexpr (MODE == 1) {
-        const TS ys = (TS)(gi - goldi);
-        const TS ss = (TS)((a.stp == 1.0) ? di : a.stp * di);
-        snew[i] = ss;
-        ynew[i] = ys;
-        yn = (double)ys;
-        const double sn = (double)ss;
-        acc[4 * K + 1] = fma(yn, yn, acc[4 * K + 1]);
-        acc[4 * K + 2] = fma(yn, gi, acc[4 * K + 2]);
-        acc[4 * K + 3] = fma(sn, gi, acc[4 * K + 3]);
-        acc[4 * K + 4] = fma(sn, yn, acc[4 * K + 4]);
-    } else if constexpr (MODE == 2) {
-        yn = (double)ynew[i];
+    if constexpr (PAIR) {
+        yn = (double)(TS)(gi - goldi);
+        if constexpr (SELF) {
+            const double sn = (double)(TS)((stp == 1.0) ? di : stp * di);
+            acc[4 * K + 1] = fma(yn, yn, acc[4 * K + 1]);
+            acc[4 * K + 2] = fma(yn, gi, acc[4 * K + 2]);
+            acc[4 * K + 3] = fma(sn, gi, acc[4 * K + 3]);
+            acc[4 * K + 4] = fma(sn, yn, acc[4 * K + 4]);
+        }
     }
     acc[2 * K] = fma(gi, gi, acc[2 * K]);
 #pragma unroll
@@ -87,16 +85,16 @@ __device__ __forceinline__ void pair_dots_elem(const PairDotsArgs &a, TS *snew, 
         const double si = (double)sk[k], yi = (double)yk[k];
         acc[k] = fma(si, gi, acc[k]);
         acc[K + k] = fma(yi, gi, acc[K + k]);
-        if constexpr (MODE != 0) {
+        if constexpr (PAIR) {
             acc[2 * K + 1 + k] = fma(si, yn, acc[2 * K + 1 + k]);
             acc[3 * K + 1 + k] = fma(yi, yn, acc[3 * K + 1 + k]);
         }
     }
 }
 
-template <typename TS, int K, int MODE, int VEC>
+template <typename TS, int K, bool PAIR, bool SELF, int VEC>
 __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
-    constexpr int R = pair_rows<K, MODE>();
+    constexpr int R = pair_rows(K, PAIR, SELF);
     constexpr int KK = K > 0 ? K : 1;
     double acc[R];
 #pragma unroll
@@ -107,7 +105,6 @@ __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
         sv[k] = static_cast<const TS *>(a.s[k]);
         yv[k] = static_cast<const TS *>(a.y[k]);
     }
-    TS *snew = static_cast<TS *>(a.snew), *ynew = static_cast<TS *>(a.ynew);
     const long long stride = (long long)gridDim.x * blockDim.x;
     if constexpr (VEC == 1) {
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
@@ -117,8 +114,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
                 sk[k] = sv[k][i];
                 yk[k] = yv[k][i];
             }
-            pair_dots_elem<TS, K, MODE>(a, snew, ynew, i, a.g[i], MODE == 1 ? a.gold[i] : 0.0, MODE == 1 ? a.d[i] : 0.0, acc, sk,
-                                        yk);
+            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, a.g[i], PAIR ? a.gold[i] : 0.0, PAIR && SELF ? a.d[i] : 0.0, acc, sk, yk);
         }
     } else {
         using P2 = typename Pair2<TS>::t;
@@ -126,10 +122,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
         for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += stride) {
             const double2 g2 = reinterpret_cast<const double2 *>(a.g)[j];
             double2 go2 = make_double2(0.0, 0.0), d2 = make_double2(0.0, 0.0);
-            if constexpr (MODE == 1) {
-                go2 = reinterpret_cast<const double2 *>(a.gold)[j];
-                d2 = reinterpret_cast<const double2 *>(a.d)[j];
-            }
+            if constexpr (PAIR) go2 = reinterpret_cast<const double2 *>(a.gold)[j];
+            if constexpr (PAIR && SELF) d2 = reinterpret_cast<const double2 *>(a.d)[j];
             TS s0[KK], y0[KK], s1[KK], y1[KK];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -139,63 +133,95 @@ __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
                 y0[k] = yp.x;
                 y1[k] = yp.y;
             }
-            pair_dots_elem<TS, K, MODE>(a, snew, ynew, 2 * j, g2.x, go2.x, d2.x, acc, s0, y0);
-            pair_dots_elem<TS, K, MODE>(a, snew, ynew, 2 * j + 1, g2.y, go2.y, d2.y, acc, s1, y1);
+            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, g2.x, go2.x, d2.x, acc, s0, y0);
+            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, g2.y, go2.y, d2.y, acc, s1, y1);
         }
     }
     block_rows_store<R>(acc, a.part);
 }
 
-// d = (accumulate ? d : cg g) + sum_k cv_k v_k ; with part: rows g.d, d.d
+// d = (accumulate ? d : cg g) + sum_k cv_k v_k.  NEWPAIR (first launch only): the accepted
+// pair s_n = stp d_old, y_n = g - gold is formed from the d being replaced, rounded to the
+// storage type, stored in snew/ynew and added with coefficients cs_n, cy_n.
 struct DirArgs {
-    const double *g;
-    double cg;
+    const double *g, *gold;
+    double cg, stp, cs_n, cy_n;
     const void *v[2 * kPairGroup];
     double cv[2 * kPairGroup];
+    void *snew, *ynew;
     double *d;
     int accumulate;
     long long n;
-    double *part;
 };
 
-template <typename TS, int K, int VEC>
+template <typename TS, int K, bool NEWPAIR>
+__device__ __forceinline__ double direction_elem(const DirArgs &a, double gi, double goldi, double dold, const TS *vk, TS &sn,
+                                                 TS &yn) {
+    double di = a.accumulate ? dold : a.cg * gi;
+    if constexpr (NEWPAIR) {
+        sn = (TS)((a.stp == 1.0) ? dold : a.stp * dold);
+        yn = (TS)(gi - goldi);
+        di = fma(a.cs_n, (double)sn, di);
+        di = fma(a.cy_n, (double)yn, di);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) di = fma(a.cv[k], (double)vk[k], di);
+    return di;
+}
+
+template <typename TS, int K, bool NEWPAIR, int VEC>
 __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
-    double acc[2] = {0.0, 0.0};
-    const TS *vv[K > 0 ? K : 1];
+    constexpr int KK = K > 0 ? K : 1;
+    const TS *vv[KK];
 #pragma unroll
     for (int k = 0; k < K; ++k) vv[k] = static_cast<const TS *>(a.v[k]);
+    TS *snew = static_cast<TS *>(a.snew), *ynew = static_cast<TS *>(a.ynew);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    const bool need_g = !a.accumulate || a.part;
+    const bool need_g = !a.accumulate || NEWPAIR;
+    const bool need_d = a.accumulate || NEWPAIR;
     if constexpr (VEC == 1) {
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
-            const double gi = need_g ? a.g[i] : 0.0;
-            double di = a.accumulate ? a.d[i] : a.cg * gi;
+            TS vk[KK], sn = 0, yn = 0;
 #pragma unroll
-            for (int k = 0; k < K; ++k) di = fma(a.cv[k], (double)vv[k][i], di);
+            for (int k = 0; k < K; ++k) vk[k] = vv[k][i];
+            const double di = direction_elem<TS, K, NEWPAIR>(a, need_g ? a.g[i] : 0.0, NEWPAIR ? a.gold[i] : 0.0,
+                                                            need_d ? a.d[i] : 0.0, vk, sn, yn);
             a.d[i] = di;
-            acc[0] = fma(gi, di, acc[0]);
-            acc[1] = fma(di, di, acc[1]);
+            if constexpr (NEWPAIR) {
+                snew[i] = sn;
+                ynew[i] = yn;
+            }
         }
     } else {
         using P2 = typename Pair2<TS>::t;
         const long long n2 = a.n / 2;
         for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += stride) {
             const double2 g2 = need_g ? reinterpret_cast<const double2 *>(a.g)[j] : make_double2(0.0, 0.0);
-            double2 d2 = a.accumulate ? reinterpret_cast<const double2 *>(a.d)[j] : make_double2(a.cg * g2.x, a.cg * g2.y);
+            const double2 go2 = NEWPAIR ? reinterpret_cast<const double2 *>(a.gold)[j] : make_double2(0.0, 0.0);
+            const double2 d2 = need_d ? reinterpret_cast<const double2 *>(a.d)[j] : make_double2(0.0, 0.0);
+            TS v0[KK], v1[KK];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 const P2 v = reinterpret_cast<const P2 *>(vv[k])[j];
-                d2.x = fma(a.cv[k], (double)v.x, d2.x);
-                d2.y = fma(a.cv[k], (double)v.y, d2.y);
+                v0[k] = v.x;
+                v1[k] = v.y;
             }
-            reinterpret_cast<double2 *>(a.d)[j] = d2;
-            acc[0] = fma(g2.x, d2.x, acc[0]);
-            acc[1] = fma(d2.x, d2.x, acc[1]);
-            acc[0] = fma(g2.y, d2.y, acc[0]);
-            acc[1] = fma(d2.y, d2.y, acc[1]);
+            TS s0 = 0, y0 = 0, s1 = 0, y1 = 0;
+            double2 r;
+            r.x = direction_elem<TS, K, NEWPAIR>(a, g2.x, go2.x, d2.x, v0, s0, y0);
+            r.y = direction_elem<TS, K, NEWPAIR>(a, g2.y, go2.y, d2.y, v1, s1, y1);
+            reinterpret_cast<double2 *>(a.d)[j] = r;
+            if constexpr (NEWPAIR) {
+                P2 sp, yp;
+                sp.x = s0;
+                sp.y = s1;
+                yp.x = y0;
+                yp.y = y1;
+                reinterpret_cast<P2 *>(snew)[j] = sp;
+                reinterpret_cast<P2 *>(ynew)[j] = yp;
+            }
         }
     }
-    if (a.part) block_rows_store<2>(acc, a.part);
 }
 
 // xt = x + stp d   (lnsrlb: x = z at stp = 1, else stp d + t)

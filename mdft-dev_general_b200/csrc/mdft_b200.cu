@@ -19,6 +19,7 @@
 #include "k_lbfgs.cuh"
 #include "k_gather_tma.cuh"
 #include "k_ozp.cuh"
+#include "k_project_tma.cuh"
 #include "k_vext.cuh"
 
 namespace mdft {
@@ -71,6 +72,7 @@ struct mdft_handle {
     long long nblk_project = 0, nblk_gather = 0;
     int nsm = 148;
     int gt_ncol64 = 0, gt_ncol32 = 0;  // k_gather_tma columns of 32 per precision (0: not usable)
+    bool pt_ok64 = false, pt_ok32 = false;  // k_project_tma usable per precision
     DevBuf<int> kerr;                  // set by a pipeline kernel whose bounded wait ran out
     int *h_kerr = nullptr;
     FftAxis fft[3];
@@ -313,7 +315,11 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     for (int ax = 0; ax < 3; ++ax) tw[ax] = dbl ? (const void *)h->tw64[ax].p : (const void *)h->tw32[ax].p;
     stage_mark(h, 0);
     AngularArgs aa{g.N, g.no, g.np, g.rho0};
-    if (h->bm_project == 64)
+    if ((dbl ? h->pt_ok64 : h->pt_ok32) && ((uintptr_t)d_xi & 15u) == 0) {
+        const int ntiles = (int)(g.N / kPtBM);
+        k_project_tma<T><<<std::min(ntiles, h->nsm), 256, project_tma_smem_bytes<T>(g.np, g.no), h->stream>>>(d_xi, A, planes,
+                                                                                                             h->kerr.p, aa, ntiles);
+    } else if (h->bm_project == 64)
         k_project<T, 64><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(64, g.no), h->stream>>>(d_xi, A, planes, aa);
     else
         k_project<T, 32><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(32, g.no), h->stream>>>(d_xi, A, planes, aa);
@@ -387,7 +393,7 @@ int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "evaluation"))) return rc;
     if (*h->h_kerr) {
         cudaMemsetAsync(h->kerr.p, 0, sizeof(int), h->stream);
-        set_error("a pipeline wait in the gather timed out (bulk copy never completed)");
+        set_error("a pipeline wait in the projection or gather timed out (bulk copy never completed)");
         return MDFT_E_CUDA;
     }
     if (h->timing) {
@@ -529,6 +535,12 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         const bool shape_ok = g.N % kGtBM == 0 && ncol <= 3;
         h->gt_ncol64 = (shape_ok && gather_tma_smem_bytes<double>(g.np, g.no, ncol) <= dyn_max) ? ncol : 0;
         h->gt_ncol32 = (shape_ok && gather_tma_smem_bytes<float>(g.np, g.no, ncol) <= dyn_max) ? ncol : 0;
+        // persistent bulk-copy projection: N in whole 64-point tiles, np <= 32
+        const bool pshape = g.N % kPtBM == 0 && g.np <= 32;
+        h->pt_ok64 = pshape && project_tma_smem_bytes<double>(g.np, g.no) <= dyn_max;
+        h->pt_ok32 = pshape && project_tma_smem_bytes<float>(g.np, g.no) <= dyn_max;
+        if ((rc = allow_smem((const void *)k_project_tma<double>, maxsmem))) return rc;
+        if ((rc = allow_smem((const void *)k_project_tma<float>, maxsmem))) return rc;
         const void *fns[] = {(const void *)k_gather_tma<double, 1>, (const void *)k_gather_tma<double, 2>,
                              (const void *)k_gather_tma<double, 3>, (const void *)k_gather_tma<float, 1>,
                              (const void *)k_gather_tma<float, 2>,  (const void *)k_gather_tma<float, 3>};

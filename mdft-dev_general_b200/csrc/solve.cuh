@@ -10,13 +10,15 @@ constexpr double kQfact = 1.602176565e-19 * 1.602176565e-19 * 1.0e-3 * 6.0221412
 
 inline unsigned vec_grid() { return kRedBlocks; }
 
-// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g| (both taken in
-// the gather pass that writes g).
-int eval_fg(mdft_handle *h, const double *x, double *g, const double *dvec, double *f, double *gd, double *gmax) {
-    int rc = run_pipeline(h, x, g, 1, 1, dvec);
-    if (rc) return rc;
+// Evaluation in two halves so that more work can be queued before the synchronise:
+// eval_launch queues the pipeline at x (gradient into g; with dvec also g.dvec and max|g|
+// from the gather pass), eval_finish waits and reads f, g.dvec and max|g|.
+int eval_launch(mdft_handle *h, const double *x, double *g, const double *dvec) { return run_pipeline(h, x, g, 1, 1, dvec); }
+
+int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
     double fid, fext, fexc;
-    if ((rc = finish_sums(h, &fid, &fext, &fexc))) return rc;
+    int rc = finish_sums(h, &fid, &fext, &fexc);
+    if (rc) return rc;
     *f = combine(h, fid, fext, fexc);
     const double gdv = h->h_sums[3], gmx = h->h_sums[4];
     if (gd) *gd = gdv;
@@ -26,6 +28,13 @@ int eval_fg(mdft_handle *h, const double *x, double *g, const double *dvec, doub
         return MDFT_E_NUMERIC;
     }
     return 0;
+}
+
+// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.
+int eval_fg(mdft_handle *h, const double *x, double *g, const double *dvec, double *f, double *gd, double *gmax) {
+    int rc = eval_launch(h, x, g, dvec);
+    if (rc) return rc;
+    return eval_finish(h, f, gd, gmax);
 }
 
 int lbfgs_alloc(mdft_handle *h, int m) {
@@ -407,136 +416,174 @@ struct LbfgsHist {
 
 constexpr int kRowsBase = 64;  // first device scalar slot of the history inner products
 
-template <typename TS, int K, int VEC>
-void launch_pair_dots_v(int mode, const PairDotsArgs &a, cudaStream_t st) {
-    const unsigned G = vec_grid();
-    if (mode == 0) k_pair_dots<TS, K, 0, VEC><<<G, kRedThreads, 0, st>>>(a);
-    else if (mode == 1) k_pair_dots<TS, K, 1, VEC><<<G, kRedThreads, 0, st>>>(a);
-    else k_pair_dots<TS, K, 2, VEC><<<G, kRedThreads, 0, st>>>(a);
-}
-template <int K>
-void launch_pair_dots(bool f32, int mode, const PairDotsArgs &a, cudaStream_t st) {
-    const bool v2 = a.n % 2 == 0;
-    if (f32) {
-        if (v2) launch_pair_dots_v<float, K, 2>(mode, a, st);
-        else launch_pair_dots_v<float, K, 1>(mode, a, st);
-    } else {
-        if (v2) launch_pair_dots_v<double, K, 2>(mode, a, st);
-        else launch_pair_dots_v<double, K, 1>(mode, a, st);
-    }
-}
-
-int pair_rows_of(int K, int mode) { return mode == 0 ? 2 * K + 1 : (mode == 1 ? 4 * K + 5 : 4 * K + 1); }
-
 // slot j of the S or Y history in the storage type of H
 inline void *hist_slot(const LbfgsHist &H, double *base, int j, long long n) {
     return H.f32 ? (void *)(reinterpret_cast<float *>(base) + (size_t)j * n) : (void *)(base + (size_t)j * n);
 }
 
-// Inner products of the history with the gradient g; with t >= 0 the new pair
-// s_t = stp d, y_t = g - gold is formed in slot t first and its products with the older
-// slots enter the Gram matrices (the caller sets sy[t][t] and theta).  Blocks on the result.
-int pair_dots(mdft_handle *h, LbfgsHist &H, const double *g, const double *gold, const double *d, double stp, int t) {
+template <typename TS, int K, bool PAIR, bool SELF>
+void launch_dots_v(const PairDotsArgs &a, cudaStream_t st) {
+    if (a.n % 2 == 0) k_pair_dots<TS, K, PAIR, SELF, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    else k_pair_dots<TS, K, PAIR, SELF, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+}
+template <int K>
+void launch_dots(bool f32, bool pair, bool self, const PairDotsArgs &a, cudaStream_t st) {
+    if (f32) {
+        if (!pair) launch_dots_v<float, K, false, false>(a, st);
+        else if (self) launch_dots_v<float, K, true, true>(a, st);
+        else launch_dots_v<float, K, true, false>(a, st);
+    } else {
+        if (!pair) launch_dots_v<double, K, false, false>(a, st);
+        else if (self) launch_dots_v<double, K, true, true>(a, st);
+        else launch_dots_v<double, K, true, false>(a, st);
+    }
+}
+
+// Inner products of the history with a gradient g, launched without waiting: `slots` are
+// the history slots read; with pair, also those of the candidate pair (stp d, g - gold).
+// The row layout of each launch goes to `plan`; the rows land in h->vsc from kRowsBase on
+// and are copied to h->h_vsc in the same stream (read them after the next synchronise).
+struct DotsPlan {
+    std::vector<int> slots;
+    bool pair = false;
+    std::vector<int> base, kk;
+    int end = kRowsBase;
+};
+int launch_history_dots(mdft_handle *h, const LbfgsHist &H, const double *g, const double *gold, const double *d, double stp,
+                        DotsPlan &P) {
     LbfgsState &L = h->lb;
     const long long n = L.n;
-    const int m = H.m;
     cudaStream_t st = h->stream;
-    std::vector<int> olds;
-    for (int c = 0; c < H.col; ++c)
-        if (H.slot(c) != t) olds.push_back(H.slot(c));
-    const int nold = (int)olds.size();
-    const int ngroups = std::max(1, (nold + kPairGroup - 1) / kPairGroup);
-    std::vector<int> base(ngroups), kk(ngroups), mode(ngroups);
+    const int ns = (int)P.slots.size();
+    const int ngroups = std::max(1, (ns + kPairGroup - 1) / kPairGroup);
+    P.base.assign(ngroups, 0);
+    P.kk.assign(ngroups, 0);
     int off = kRowsBase;
     for (int gi = 0; gi < ngroups; ++gi) {
-        kk[gi] = std::min(kPairGroup, nold - kPairGroup * gi);
-        mode[gi] = t < 0 ? 0 : (gi == 0 ? 1 : 2);
+        const int K = std::min(kPairGroup, ns - kPairGroup * gi);
+        const bool self = P.pair && gi == 0;
+        const int rows = pair_rows(K, P.pair, self);
+        if (off + rows > kScalarSlots) {
+            set_error("history too long for the scalar slots");
+            return MDFT_E_ARG;
+        }
         PairDotsArgs a{};
         a.g = g;
         a.gold = gold;
         a.d = d;
-        for (int k = 0; k < kk[gi]; ++k) {
-            a.s[k] = hist_slot(H, L.S.p, olds[kPairGroup * gi + k], n);
-            a.y[k] = hist_slot(H, L.Y.p, olds[kPairGroup * gi + k], n);
+        for (int k = 0; k < K; ++k) {
+            a.s[k] = hist_slot(H, L.S.p, P.slots[kPairGroup * gi + k], n);
+            a.y[k] = hist_slot(H, L.Y.p, P.slots[kPairGroup * gi + k], n);
         }
-        a.snew = t >= 0 ? hist_slot(H, L.S.p, t, n) : nullptr;
-        a.ynew = t >= 0 ? hist_slot(H, L.Y.p, t, n) : nullptr;
         a.stp = stp;
         a.n = n;
         a.part = h->vpart.p;
-        switch (kk[gi]) {
-            case 0: launch_pair_dots<0>(H.f32, mode[gi], a, st); break;
-            case 1: launch_pair_dots<1>(H.f32, mode[gi], a, st); break;
-            case 2: launch_pair_dots<2>(H.f32, mode[gi], a, st); break;
-            case 3: launch_pair_dots<3>(H.f32, mode[gi], a, st); break;
-            case 4: launch_pair_dots<4>(H.f32, mode[gi], a, st); break;
-            case 5: launch_pair_dots<5>(H.f32, mode[gi], a, st); break;
-            case 6: launch_pair_dots<6>(H.f32, mode[gi], a, st); break;
-            case 7: launch_pair_dots<7>(H.f32, mode[gi], a, st); break;
-            default: launch_pair_dots<8>(H.f32, mode[gi], a, st); break;
+        switch (K) {
+            case 0: launch_dots<0>(H.f32, P.pair, self, a, st); break;
+            case 1: launch_dots<1>(H.f32, P.pair, self, a, st); break;
+            case 2: launch_dots<2>(H.f32, P.pair, self, a, st); break;
+            case 3: launch_dots<3>(H.f32, P.pair, self, a, st); break;
+            case 4: launch_dots<4>(H.f32, P.pair, self, a, st); break;
+            case 5: launch_dots<5>(H.f32, P.pair, self, a, st); break;
+            case 6: launch_dots<6>(H.f32, P.pair, self, a, st); break;
+            case 7: launch_dots<7>(H.f32, P.pair, self, a, st); break;
+            default: launch_dots<8>(H.f32, P.pair, self, a, st); break;
         }
-        const int rows = pair_rows_of(kk[gi], mode[gi]);
         k_finish_rows<<<rows, 256, 0, st>>>(h->vpart.p, (int)vec_grid(), h->vsc.p + off);
         h->launches += 2;
-        base[gi] = off;
+        P.base[gi] = off;
+        P.kk[gi] = K;
         off += rows;
     }
+    P.end = off;
     int rc = check_cuda(cudaGetLastError(), "history inner products");
     if (rc) return rc;
-    if (off > kScalarSlots) {
-        set_error("history too long for the scalar slots");
-        return MDFT_E_ARG;
-    }
-    if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc + kRowsBase, h->vsc.p + kRowsBase, (off - kRowsBase) * sizeof(double),
-                                         cudaMemcpyDeviceToHost, st), "history inner products"))) return rc;
-    if ((rc = check_cuda(cudaStreamSynchronize(st), "history inner products"))) return rc;
+    return check_cuda(cudaMemcpyAsync(h->h_vsc + kRowsBase, h->vsc.p + kRowsBase, (off - kRowsBase) * sizeof(double),
+                                      cudaMemcpyDeviceToHost, st), "history inner products");
+}
+
+// Candidate pair's products read back by read_history_dots
+struct PairRows {
+    std::vector<double> s_yn, y_yn;  // by slot
+    double yy = 0, yg = 0, sg = 0, sy = 0;
+};
+
+// After the synchronise: s_i.g, y_i.g and g.g into H; the candidate's products into R.
+int read_history_dots(const mdft_handle *h, LbfgsHist &H, const DotsPlan &P, PairRows *R) {
     const double *r = h->h_vsc;
-    for (int gi = 0; gi < ngroups; ++gi) {
-        const int K = kk[gi], b = base[gi];
-        for (int k = 0; k < K; ++k) {
-            const int j = olds[kPairGroup * gi + k];
-            H.sg[j] = r[b + k];
-            H.yg[j] = r[b + K + k];
-            if (mode[gi] != 0) {
-                H.sy[(size_t)j * m + t] = r[b + 2 * K + 1 + k];
-                H.yy[(size_t)j * m + t] = H.yy[(size_t)t * m + j] = r[b + 3 * K + 1 + k];
-            }
-        }
-        if (gi == 0) H.gg = r[b + 2 * K];
-        if (mode[gi] == 1) {
-            H.yy[(size_t)t * m + t] = r[b + 4 * K + 1];
-            H.yg[t] = r[b + 4 * K + 2];
-            H.sg[t] = r[b + 4 * K + 3];
-            H.sty = r[b + 4 * K + 4];
-        }
-    }
-    for (int c = 0; c < H.col; ++c) {
-        const int j = H.slot(c);
-        if (!std::isfinite(H.sg[j]) || !std::isfinite(H.yg[j])) {
+    for (int i = kRowsBase; i < P.end; ++i)
+        if (!std::isfinite(r[i])) {
             set_error("non-finite history inner product");
             return MDFT_E_NUMERIC;
+        }
+    if (R) {
+        R->s_yn.assign(H.m, 0.0);
+        R->y_yn.assign(H.m, 0.0);
+    }
+    for (size_t gi = 0; gi < P.base.size(); ++gi) {
+        const int K = P.kk[gi], b = P.base[gi];
+        for (int k = 0; k < K; ++k) {
+            const int j = P.slots[kPairGroup * gi + k];
+            H.sg[j] = r[b + k];
+            H.yg[j] = r[b + K + k];
+            if (P.pair && R) {
+                R->s_yn[j] = r[b + 2 * K + 1 + k];
+                R->y_yn[j] = r[b + 3 * K + 1 + k];
+            }
+        }
+        if (gi == 0) {
+            H.gg = r[b + 2 * K];
+            if (P.pair && R) {
+                R->yy = r[b + 4 * K + 1];
+                R->yg = r[b + 4 * K + 2];
+                R->sg = r[b + 4 * K + 3];
+                R->sy = r[b + 4 * K + 4];
+            }
         }
     }
     return 0;
 }
 
-template <int K>
-void launch_direction(bool f32, const DirArgs &a, cudaStream_t st) {
+// Blocking form: products of every current slot with g (no candidate pair).
+int history_dots_now(mdft_handle *h, LbfgsHist &H, const double *g) {
+    DotsPlan P;
+    for (int c = 0; c < H.col; ++c) P.slots.push_back(H.slot(c));
+    int rc = launch_history_dots(h, H, g, nullptr, nullptr, 0.0, P);
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "history inner products"))) return rc;
+    return read_history_dots(h, H, P, nullptr);
+}
+
+template <int K, bool NP>
+void launch_direction_k(bool f32, const DirArgs &a, cudaStream_t st) {
     const bool v2 = a.n % 2 == 0;
     if (f32) {
-        if (v2) k_direction<float, K, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<float, K, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        if (v2) k_direction<float, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<float, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     } else {
-        if (v2) k_direction<double, K, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<double, K, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        if (v2) k_direction<double, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     }
 }
+template <int K>
+void launch_direction(bool f32, bool np, const DirArgs &a, cudaStream_t st) {
+    if (np) launch_direction_k<K, true>(f32, a, st);
+    else launch_direction_k<K, false>(f32, a, st);
+}
+
+// Pair accepted in the last step and not yet stored: k_direction forms it from the
+// direction it replaces (s = stp d) and the previous gradient (y = g - gold).
+struct PendingPair {
+    int slot = -1;
+    const double *gold = nullptr;
+    double stp = 1.0;
+};
 
 // d = -H g with H the inverse of the compact L-BFGS matrix, H0 = I/theta:
 //   H g = g/theta + S top - Y u/theta,  u = R^-1 S'g,  top = R^-T ((D + Y'Y/theta) u - Y'g/theta)
-// (R = upper triangle of S'Y, D its diagonal; no history: d = -g/theta).  Returns g.d and
-// d.d (blocking).
-int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, double *gd, double *dd) {
+// (R = upper triangle of S'Y, D its diagonal; no history: d = -g/theta).  The slope g.d and
+// d.d come from the Gram data (no synchronise); a pending pair is stored on the way.
+int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, const PendingPair &pend, double *gd, double *dd) {
     LbfgsState &L = h->lb;
     const long long n = L.n;
     const int k = H.col, m = H.m;
@@ -544,6 +591,8 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
     const double gam = 1.0 / H.theta;
     std::vector<const void *> vec;
     std::vector<double> coef;
+    double cs_n = 0.0, cy_n = 0.0;
+    double slope = -gam * H.gg, dnorm2 = gam * gam * H.gg;
     if (k > 0) {
         std::vector<int> idx(k);
         for (int c = 0; c < k; ++c) idx[c] = H.slot(c);
@@ -566,16 +615,22 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
             top[a] = s / R(a, a);
         }
         for (int a = 0; a < k; ++a) {
-            vec.push_back(hist_slot(H, L.S.p, idx[a], n));
-            coef.push_back(-top[a]);
-            vec.push_back(hist_slot(H, L.Y.p, idx[a], n));
-            coef.push_back(gam * u[a]);
-        }
-        for (double c : coef)
-            if (!std::isfinite(c)) {
+            const double cs = -top[a], cy = gam * u[a];
+            if (!std::isfinite(cs) || !std::isfinite(cy)) {
                 set_error("non-finite search-direction coefficient");
                 return MDFT_E_NUMERIC;
             }
+            slope += cs * H.sg[idx[a]] + cy * H.yg[idx[a]];
+            if (idx[a] == pend.slot) {
+                cs_n = cs;
+                cy_n = cy;
+                continue;
+            }
+            vec.push_back(hist_slot(H, L.S.p, idx[a], n));
+            coef.push_back(cs);
+            vec.push_back(hist_slot(H, L.Y.p, idx[a], n));
+            coef.push_back(cy);
+        }
     }
     const int nv = (int)vec.size();
     constexpr int kV = 2 * kPairGroup;
@@ -584,6 +639,15 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
         DirArgs a{};
         a.g = g;
         a.cg = -gam;
+        const bool np = li == 0 && pend.slot >= 0;
+        if (np) {
+            a.gold = pend.gold;
+            a.stp = pend.stp;
+            a.cs_n = cs_n;
+            a.cy_n = cy_n;
+            a.snew = hist_slot(H, L.S.p, pend.slot, n);
+            a.ynew = hist_slot(H, L.Y.p, pend.slot, n);
+        }
         const int K = std::min(kV, nv - kV * li);
         for (int j = 0; j < K; ++j) {
             a.v[j] = vec[kV * li + j];
@@ -592,33 +656,26 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, do
         a.d = d;
         a.accumulate = li > 0;
         a.n = n;
-        a.part = (li == nl - 1) ? h->vpart.p : nullptr;
         switch (K) {
-            case 0: launch_direction<0>(H.f32, a, st); break;
-            case 2: launch_direction<2>(H.f32, a, st); break;
-            case 4: launch_direction<4>(H.f32, a, st); break;
-            case 6: launch_direction<6>(H.f32, a, st); break;
-            case 8: launch_direction<8>(H.f32, a, st); break;
-            case 10: launch_direction<10>(H.f32, a, st); break;
-            case 12: launch_direction<12>(H.f32, a, st); break;
-            case 14: launch_direction<14>(H.f32, a, st); break;
-            default: launch_direction<16>(H.f32, a, st); break;
+            case 0: launch_direction<0>(H.f32, np, a, st); break;
+            case 2: launch_direction<2>(H.f32, np, a, st); break;
+            case 4: launch_direction<4>(H.f32, np, a, st); break;
+            case 6: launch_direction<6>(H.f32, np, a, st); break;
+            case 8: launch_direction<8>(H.f32, np, a, st); break;
+            case 10: launch_direction<10>(H.f32, np, a, st); break;
+            case 12: launch_direction<12>(H.f32, np, a, st); break;
+            case 14: launch_direction<14>(H.f32, np, a, st); break;
+            default: launch_direction<16>(H.f32, np, a, st); break;
         }
         h->launches += 1;
     }
-    k_finish_rows<<<2, 256, 0, st>>>(h->vpart.p, (int)vec_grid(), h->vsc.p + 2);
-    h->launches += 1;
-    int rc = check_cuda(cudaGetLastError(), "direction");
-    if (rc) return rc;
-    if ((rc = check_cuda(cudaMemcpyAsync(h->h_vsc + 2, h->vsc.p + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "direction"))) return rc;
-    if ((rc = check_cuda(cudaStreamSynchronize(st), "direction"))) return rc;
-    *gd = h->h_vsc[2];
-    *dd = h->h_vsc[3];
-    if (!std::isfinite(*gd) || !std::isfinite(*dd)) {
+    *gd = slope;
+    *dd = dnorm2;
+    if (!std::isfinite(slope)) {
         set_error("non-finite search direction");
         return MDFT_E_NUMERIC;
     }
-    return 0;
+    return check_cuda(cudaGetLastError(), "direction");
 }
 
 // MDFT_TRACE: one stderr line per accepted iteration with F, max|df| and the particle
@@ -657,15 +714,17 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0;
     int iter = 0, nfgv = 0, status = 3;
     const bool fresh = H.col == 0;
+    PendingPair pend;
     if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax))) return rc;
     nfgv = 1;
     trace_iter(h, xc, 0, nfgv, f, gmax, 0.0);
     double sbgnrm = gmax;
     if (sbgnrm <= o->pgtol) { status = 0; goto done; }
-    if (H.col > 0 && (rc = pair_dots(h, H, gc, nullptr, nullptr, 0.0, -1))) return rc;
+    if ((rc = history_dots_now(h, H, gc))) return rc;  // s_i.g, y_i.g, g.g at the start point
     while (iter < o->itermax) {
-        // ---- search direction ----
-        if ((rc = direction(h, H, gc, L.d.p, &gd, &dd))) return rc;
+        // ---- search direction (stores the pair accepted last step) ----
+        if ((rc = direction(h, H, gc, L.d.p, pend, &gd, &dd))) return rc;
+        pend = PendingPair();
         // ---- line search (lnsrlb) ----
         const double stpmx = big;
         stp = (iter == 0 && fresh) ? std::min(1.0 / std::sqrt(dd), stpmx) : 1.0;
@@ -673,6 +732,13 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         gdold = gd;
         int ifun = 0, iback = 0, info = 0;
         double gmax_t = gmax;
+        // the slot a pair accepted in this step would take, and the slots that stay
+        const int tnext = H.col < m ? H.slot(H.col) : H.head;
+        DotsPlan P;
+        P.pair = true;
+        for (int c = 0; c < H.col; ++c)
+            if (H.slot(c) != tnext) P.slots.push_back(H.slot(c));
+        PairRows PR;
         LineSearch LS;
         if (gd >= 0.0) {
             info = -4;
@@ -686,7 +752,11 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 if (n % 2 == 0) k_trial2<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n / 2);
                 else k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
                 h->launches += 1;
-                if ((rc = eval_fg(h, xt, gt, L.d.p, &f, &gd, &gmax_t))) return rc;
+                if ((rc = eval_launch(h, xt, gt, L.d.p))) return rc;
+                // the history's products with this trial gradient, queued before the one
+                // synchronise of the step (used if the trial is accepted)
+                if ((rc = launch_history_dots(h, H, gt, gc, L.d.p, stp, P))) return rc;
+                if ((rc = eval_finish(h, &f, &gd, &gmax_t))) return rc;
                 const double stp_eval = stp;
                 task = dcsrch(f, gd, stp, ftol, gtol, xtol, 0.0, stpmx, false, LS);
                 // Approximate Wolfe test (Hager and Zhang, SIAM J. Optim. 16 (2005) 170, eq. 4.1):
@@ -698,11 +768,12 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                     stp = stp_eval;
                     task = LS_CONV;
                 }
+                if (task != LS_FG) stp = stp_eval;
             }
             if (task == LS_ERROR) info = -1;
         }
         if (info != 0 || iback >= 20) {
-            f = fold;  // x and g stay at the last accepted point
+            f = fold;  // x and g stay at the last accepted point (H.gg still belongs to it)
             if (h->trace) std::fprintf(stderr, "mdft-trace line search failed (info %d, iback %d, col %d)\n", info, iback, H.col);
             if (H.col == 0 || stop_on_ls_fail) {
                 status = 2;
@@ -726,25 +797,35 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         double dr, ddum;
         if (stp == 1.0) { dr = gd - gdold; ddum = -gdold; }
         else { dr = (gd - gdold) * stp; ddum = -gdold * stp; }
-        if (dr <= epsmch * ddum) {  // update skipped: refresh the products with the new g
-            if (H.col > 0 && (rc = pair_dots(h, H, gc, nullptr, nullptr, 0.0, -1))) return rc;
+        if (dr <= epsmch * ddum) {  // update skipped: products of every slot with the new g
+            if ((rc = history_dots_now(h, H, gc))) return rc;
             continue;
         }
-        int t;
-        if (H.col < m) {
-            t = H.slot(H.col);
-            ++H.col;
-        } else {
-            t = H.head;
-            H.head = (H.head + 1) % m;
+        if ((rc = read_history_dots(h, H, P, &PR))) return rc;
+        if (H.col < m) ++H.col;
+        else H.head = (H.head + 1) % m;
+        const int t = tnext;
+        for (int j : P.slots) {
+            H.sy[(size_t)j * m + t] = PR.s_yn[j];
+            H.yy[(size_t)j * m + t] = H.yy[(size_t)t * m + j] = PR.y_yn[j];
         }
-        if ((rc = pair_dots(h, H, gc, gt, L.d.p, stp, t))) return rc;
+        H.yy[(size_t)t * m + t] = PR.yy;
+        H.sg[t] = PR.sg;
+        H.yg[t] = PR.yg;
         // FP64 history: s.y = dr as the reference's matupd; FP32 history: s.y of the stored pair
-        const double sty = H.f32 ? H.sty : dr;
+        const double sty = H.f32 ? PR.sy : dr;
         H.sy[(size_t)t * m + t] = sty;
-        H.theta = H.yy[(size_t)t * m + t] / sty;
+        H.theta = PR.yy / sty;
+        pend.slot = t;
+        pend.gold = gt;  // the previous gradient (buffers swapped above)
+        pend.stp = stp;
     }
 done:
+    if (pend.slot >= 0) {
+        // the last accepted pair is part of H (a later phase may continue with it): store it
+        double gd2, dd2;
+        if ((rc = direction(h, H, gc, L.d.p, pend, &gd2, &dd2))) return rc;
+    }
     if (xc != L.x.p) cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
     if (gc != h->df.p) cudaMemcpyAsync(h->df.p, gc, n * 8, cudaMemcpyDeviceToDevice, st);
     if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;

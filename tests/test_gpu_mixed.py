@@ -1,9 +1,9 @@
-"""Mixed-precision path (FP32 projections, FFTs and OZ; FP64 ideal term, reductions and
-L-BFGS) against the FP64 oracle and the FP64 engine.
+"""Mixed-precision path (FP32 projections, FFTs, OZ and per-element arithmetic; FP64 sums,
+L-BFGS vectors and the final check) against the FP64 oracle and the FP64 engine.
 
-Tolerances: energy 2e-6 of |F| and gradient 1e-4 of max|df| for one evaluation (FP32
-arithmetic on the excess term); a mixed solve's dG within 0.1 kJ/mol of the FP64 solve
-(the bar of the throughput metric)."""
+Tolerances: energy 2e-6 of |F|, the ideal and external terms 1e-7 of |F| (FP32 per-element
+arithmetic, FP64 sums) and gradient 1e-4 of max|df| for one evaluation; a mixed solve's dG
+within 0.1 kJ/mol of the FP64 solve (the bar of the throughput metric)."""
 import numpy as np
 import pytest
 
@@ -31,7 +31,7 @@ def test_mixed_energy_gradient(tmp_path, name):
     f0, df0, t0 = o.energy_grad(xi)
     f1, df1, t1 = e.energy_and_gradient(xi)
     assert abs(f1 - f0) <= 2e-6 * abs(f0), (f1, f0)
-    assert abs(t1[0] - t0[0]) <= 1e-12 * abs(f0) and abs(t1[1] - t0[1]) <= 1e-12 * abs(f0)  # FP64 terms
+    assert abs(t1[0] - t0[0]) <= 1e-7 * abs(f0) and abs(t1[1] - t0[1]) <= 1e-7 * abs(f0), (t1, t0)
     assert np.abs(df1 - df0).max() <= 1e-4 * np.abs(df0).max()
     e.close()
 
