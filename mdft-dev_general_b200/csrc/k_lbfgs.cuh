@@ -152,7 +152,13 @@ struct DirArgs {
     double *d;
     int accumulate;
     long long n;
+    const double *x;  // non-null (last launch): also the first trial point xt = x + stp_t d
+    double *xt;
+    double stp_t;
 };
+
+// the trial point of lnsrlb: x = z at stp = 1, else stp d + t
+__device__ __forceinline__ double trial_elem(double x, double d, double stp) { return (stp == 1.0) ? x + d : fma(stp, d, x); }
 
 template <typename TS, int K, bool NEWPAIR>
 __device__ __forceinline__ double direction_elem(const DirArgs &a, double gi, double goldi, double dold, const TS *vk, TS &sn,
@@ -187,6 +193,7 @@ __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
             const double di = direction_elem<TS, K, NEWPAIR>(a, need_g ? a.g[i] : 0.0, NEWPAIR ? a.gold[i] : 0.0,
                                                             need_d ? a.d[i] : 0.0, vk, sn, yn);
             a.d[i] = di;
+            if (a.x) a.xt[i] = trial_elem(a.x[i], di, a.stp_t);
             if constexpr (NEWPAIR) {
                 snew[i] = sn;
                 ynew[i] = yn;
@@ -211,6 +218,10 @@ __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
             r.x = direction_elem<TS, K, NEWPAIR>(a, g2.x, go2.x, d2.x, v0, s0, y0);
             r.y = direction_elem<TS, K, NEWPAIR>(a, g2.y, go2.y, d2.y, v1, s1, y1);
             reinterpret_cast<double2 *>(a.d)[j] = r;
+            if (a.x) {
+                const double2 xv = reinterpret_cast<const double2 *>(a.x)[j];
+                reinterpret_cast<double2 *>(a.xt)[j] = make_double2(trial_elem(xv.x, r.x, a.stp_t), trial_elem(xv.y, r.y, a.stp_t));
+            }
             if constexpr (NEWPAIR) {
                 P2 sp, yp;
                 sp.x = s0;
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
 __global__ void k_trial(double *__restrict__ xt, const double *__restrict__ x, const double *__restrict__ d, double stp,
                         long long n) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        xt[i] = (stp == 1.0) ? x[i] + d[i] : fma(stp, d[i], x[i]);
+        xt[i] = trial_elem(x[i], d[i], stp);
 }
 
 // the same on element pairs (n even, 16-byte aligned vectors); n2 = n / 2
@@ -237,8 +248,8 @@ __global__ void k_trial2(double *__restrict__ xt, const double *__restrict__ x, 
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += (long long)gridDim.x * blockDim.x) {
         const double2 xv = reinterpret_cast<const double2 *>(x)[j], dv = reinterpret_cast<const double2 *>(d)[j];
         double2 r;
-        r.x = (stp == 1.0) ? xv.x + dv.x : fma(stp, dv.x, xv.x);
-        r.y = (stp == 1.0) ? xv.y + dv.y : fma(stp, dv.y, xv.y);
+        r.x = trial_elem(xv.x, dv.x, stp);
+        r.y = trial_elem(xv.y, dv.y, stp);
         reinterpret_cast<double2 *>(xt)[j] = r;
     }
 }

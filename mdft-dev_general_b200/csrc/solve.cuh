@@ -583,7 +583,9 @@ struct PendingPair {
 //   H g = g/theta + S top - Y u/theta,  u = R^-1 S'g,  top = R^-T ((D + Y'Y/theta) u - Y'g/theta)
 // (R = upper triangle of S'Y, D its diagonal; no history: d = -g/theta).  The slope g.d and
 // d.d come from the Gram data (no synchronise); a pending pair is stored on the way.
-int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, const PendingPair &pend, double *gd, double *dd) {
+// With x non-null the last launch also writes the first trial point xt = x + stp_t d.
+int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, const PendingPair &pend, double *gd, double *dd,
+              const double *x = nullptr, double *xt = nullptr, double stp_t = 1.0) {
     LbfgsState &L = h->lb;
     const long long n = L.n;
     const int k = H.col, m = H.m;
@@ -656,6 +658,11 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, co
         a.d = d;
         a.accumulate = li > 0;
         a.n = n;
+        if (li == nl - 1 && x) {
+            a.x = x;
+            a.xt = xt;
+            a.stp_t = stp_t;
+        }
         switch (K) {
             case 0: launch_direction<0>(H.f32, np, a, st); break;
             case 2: launch_direction<2>(H.f32, np, a, st); break;
@@ -722,12 +729,14 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     if (sbgnrm <= o->pgtol) { status = 0; goto done; }
     if ((rc = history_dots_now(h, H, gc))) return rc;  // s_i.g, y_i.g, g.g at the start point
     while (iter < o->itermax) {
-        // ---- search direction (stores the pair accepted last step) ----
-        if ((rc = direction(h, H, gc, L.d.p, pend, &gd, &dd))) return rc;
+        // ---- search direction (stores the pair accepted last step) and the first trial ----
+        const double stpmx = big;
+        // lnsrlb's first step: 1/|d| on the first iteration from an empty history, where
+        // d = -g/theta and |d|^2 = g.g/theta^2, else 1
+        stp = (iter == 0 && fresh) ? std::min(1.0 / std::sqrt(H.gg / (H.theta * H.theta)), stpmx) : 1.0;
+        if ((rc = direction(h, H, gc, L.d.p, pend, &gd, &dd, xc, xt, stp))) return rc;
         pend = PendingPair();
         // ---- line search (lnsrlb) ----
-        const double stpmx = big;
-        stp = (iter == 0 && fresh) ? std::min(1.0 / std::sqrt(dd), stpmx) : 1.0;
         fold = f;
         gdold = gd;
         int ifun = 0, iback = 0, info = 0;
@@ -749,9 +758,11 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 ++nfgv;
                 iback = ifun - 1;
                 if (iback >= 20) break;
-                if (n % 2 == 0) k_trial2<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n / 2);
-                else k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
-                h->launches += 1;
+                if (ifun > 1) {  // the first trial point came with the direction
+                    if (n % 2 == 0) k_trial2<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n / 2);
+                    else k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                    h->launches += 1;
+                }
                 if ((rc = eval_launch(h, xt, gt, L.d.p))) return rc;
                 // the history's products with this trial gradient, queued before the one
                 // synchronise of the step (used if the trial is accepted)
