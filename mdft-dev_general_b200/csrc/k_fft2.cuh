@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "k_fft.cuh"
+#include "k_tma.cuh"
 
 namespace mdft {
 
@@ -140,6 +141,75 @@ __global__ void __launch_bounds__(xy_threads<T, N>(), (xy_threads<T, N>() <= 512
 }
 
 template <typename T, int N> __host__ __device__ constexpr size_t xy_smem_bytes() { return sizeof(typename Cplx<T>::t) * (N + (size_t)N * (N + 1)); }
+
+// Persistent form of k_fft_xy: each CTA walks the planes blockIdx.x, +gridDim.x, ...  A plane
+// (N x N contiguous values) arrives by one bulk copy into one of two shared-memory buffers
+// while the other is transformed, and leaves by one bulk store.  The Stockham passes read
+// and write the unpadded plane without bank conflicts (x: consecutive threads take
+// consecutive points of a line; y: consecutive lines).  Waits are bounded; a wait that runs
+// out sets *err and the CTA stops.
+template <typename T, int N> __host__ __device__ constexpr size_t xy_tma_smem_bytes() {
+    return sizeof(typename Cplx<T>::t) * (2 * (size_t)N * N + N);
+}
+template <typename T, int N> __host__ __device__ constexpr bool xy_tma_fits() { return xy_tma_smem_bytes<T, N>() <= 200 * 1024; }
+
+template <typename T, int N>
+__global__ void __launch_bounds__(xy_threads<T, N>()) k_fft_xy_tma(typename Cplx<T>::t *__restrict__ data,
+                                                                  const typename Cplx<T>::t *__restrict__ tw, int sign,
+                                                                  long long nplanes, int *__restrict__ err) {
+    using C = typename Cplx<T>::t;
+    constexpr int THREADS = xy_threads<T, N>();
+    constexpr uint32_t kPlane = (uint32_t)(sizeof(C) * N * N);
+    extern __shared__ __align__(128) unsigned char xyt_smem[];
+    C *buf0 = reinterpret_cast<C *>(xyt_smem);
+    C *twl = buf0 + 2 * N * N;
+    __shared__ uint64_t full[2];
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x;
+    const long long nmine = (long long)blockIdx.x < nplanes ? (nplanes - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_fence_init();
+        abort_flag = 0;
+        if (nmine > 0) {
+            mbar_arrive_expect_tx(&full[0], kPlane);
+            bulk_load(buf0, data + (size_t)blockIdx.x * N * N, kPlane, &full[0]);
+        }
+    }
+    for (int i = tid; i < N; i += THREADS) twl[i] = tw[i];
+    __syncthreads();
+    long long i = 0;
+    for (; i < nmine; ++i) {
+        const int s = (int)(i & 1);
+        C *buf = buf0 + s * N * N;
+        const long long p = blockIdx.x + i * gridDim.x;
+        if (tid == 0 && i + 1 < nmine) {
+            bulk_wait_read_all();  // the other buffer's last store has been read out
+            mbar_arrive_expect_tx(&full[s ^ 1], kPlane);
+            bulk_load(buf0 + (s ^ 1) * N * N, data + (size_t)(p + gridDim.x) * N * N, kPlane, &full[s ^ 1]);
+        }
+        if (!mbar_wait(&full[s], (uint32_t)((i >> 1) & 1))) abort_flag = 1;
+        __syncthreads();
+        if (abort_flag) break;
+        fft_lines<T, N, 0, N, THREADS, false>(buf, 1, N, twl, sign);  // along x: line = y
+        fft_lines<T, N, 0, N, THREADS, true>(buf, N, 1, twl, sign);   // along y: line = x
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            bulk_store(data + (size_t)p * N * N, buf, kPlane);
+            bulk_commit();
+        }
+    }
+    if (tid == 0) {
+        if (abort_flag) {
+            atomicExch(err, 1);
+            // the copy issued for the next plane gets a bounded wait before the CTA exits
+            if (i + 1 < nmine) (void)mbar_wait(&full[(i + 1) & 1], (uint32_t)(((i + 1) >> 1) & 1));
+        }
+        bulk_wait_all();
+    }
+}
 
 template <typename T> __host__ __device__ constexpr int z_tl() { return sizeof(T) == 8 ? 16 : 32; }
 

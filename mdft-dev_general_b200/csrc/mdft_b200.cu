@@ -73,6 +73,7 @@ struct mdft_handle {
     int nsm = 148;
     int gt_ncol64 = 0, gt_ncol32 = 0;  // k_gather_tma columns of 32 per precision (0: not usable)
     bool pt_ok64 = false, pt_ok32 = false;  // k_project_tma usable per precision
+    int xy_grid_cap64 = 0, xy_grid_cap32 = 0;  // CTAs of the persistent xy FFT (resident count)
     DevBuf<int> kerr;                  // set by a pipeline kernel whose bounded wait ran out
     int *h_kerr = nullptr;
     FftAxis fft[3];
@@ -184,11 +185,20 @@ int setup_fft(mdft_handle *h) {
 // generic per-axis kernel otherwise.
 template <typename T, int N>
 cudaError_t fft_xy_n(typename Cplx<T>::t *data, long long nplanes, const typename Cplx<T>::t *tw, int sign, cudaStream_t st,
-                     bool prepare) {
-    if (prepare)
-        return cudaFuncSetAttribute(k_fft_xy<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem_bytes<T, N>());
-    k_fft_xy<T, N><<<(unsigned)nplanes, xy_threads<T, N>(), xy_smem_bytes<T, N>(), st>>>(data, tw, sign);
-    return cudaGetLastError();
+                     bool prepare, int grid_cap, int *err) {
+    if constexpr (xy_tma_fits<T, N>()) {
+        // persistent bulk-copy form: grid_cap CTAs at most (the device's resident count)
+        if (prepare)
+            return cudaFuncSetAttribute(k_fft_xy_tma<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_tma_smem_bytes<T, N>());
+        const long long grid = std::min<long long>(nplanes, std::max(1, grid_cap));
+        k_fft_xy_tma<T, N><<<(unsigned)grid, xy_threads<T, N>(), xy_tma_smem_bytes<T, N>(), st>>>(data, tw, sign, nplanes, err);
+        return cudaGetLastError();
+    } else {
+        if (prepare)
+            return cudaFuncSetAttribute(k_fft_xy<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xy_smem_bytes<T, N>());
+        k_fft_xy<T, N><<<(unsigned)nplanes, xy_threads<T, N>(), xy_smem_bytes<T, N>(), st>>>(data, tw, sign);
+        return cudaGetLastError();
+    }
 }
 template <typename T, int N>
 cudaError_t fft_z_n(typename Cplx<T>::t *data, long long nplanes, int nx, int ny, const typename Cplx<T>::t *tw, int sign,
@@ -200,19 +210,45 @@ cudaError_t fft_z_n(typename Cplx<T>::t *data, long long nplanes, int nx, int ny
     return cudaGetLastError();
 }
 
+// resident CTAs per SM of the persistent xy FFT for length n (0: not used for n)
+template <typename T, int N>
+int xy_tma_per_sm_n() {
+    if constexpr (xy_tma_fits<T, N>()) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_fft_xy_tma<T, N>, xy_threads<T, N>(), xy_tma_smem_bytes<T, N>());
+        return b;
+    } else {
+        return 0;
+    }
+}
+template <typename T>
+int xy_tma_per_sm(int n) {
+    switch (n) {
+    case 8: return xy_tma_per_sm_n<T, 8>();
+    case 12: return xy_tma_per_sm_n<T, 12>();
+    case 16: return xy_tma_per_sm_n<T, 16>();
+    case 24: return xy_tma_per_sm_n<T, 24>();
+    case 32: return xy_tma_per_sm_n<T, 32>();
+    case 48: return xy_tma_per_sm_n<T, 48>();
+    case 64: return xy_tma_per_sm_n<T, 64>();
+    case 96: return xy_tma_per_sm_n<T, 96>();
+    default: return 0;
+    }
+}
+
 // returns cudaErrorNotSupported when no specialised kernel exists for n
 template <typename T>
 cudaError_t fft_xy(int n, typename Cplx<T>::t *data, long long nplanes, const typename Cplx<T>::t *tw, int sign, cudaStream_t st,
-                   bool prepare) {
+                   bool prepare, int grid_cap = 0, int *err = nullptr) {
     switch (n) {
-    case 8: return fft_xy_n<T, 8>(data, nplanes, tw, sign, st, prepare);
-    case 12: return fft_xy_n<T, 12>(data, nplanes, tw, sign, st, prepare);
-    case 16: return fft_xy_n<T, 16>(data, nplanes, tw, sign, st, prepare);
-    case 24: return fft_xy_n<T, 24>(data, nplanes, tw, sign, st, prepare);
-    case 32: return fft_xy_n<T, 32>(data, nplanes, tw, sign, st, prepare);
-    case 48: return fft_xy_n<T, 48>(data, nplanes, tw, sign, st, prepare);
-    case 64: return fft_xy_n<T, 64>(data, nplanes, tw, sign, st, prepare);
-    case 96: return fft_xy_n<T, 96>(data, nplanes, tw, sign, st, prepare);
+    case 8: return fft_xy_n<T, 8>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 12: return fft_xy_n<T, 12>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 16: return fft_xy_n<T, 16>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 24: return fft_xy_n<T, 24>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 32: return fft_xy_n<T, 32>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 48: return fft_xy_n<T, 48>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 64: return fft_xy_n<T, 64>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
+    case 96: return fft_xy_n<T, 96>(data, nplanes, tw, sign, st, prepare, grid_cap, err);
     default: return cudaErrorNotSupported;
     }
 }
@@ -240,7 +276,8 @@ int launch_fft_t(mdft_handle *h, typename Cplx<T>::t *planes, const void *const 
     const Grid &g = h->g;
     bool xy_done = false;
     if (g.nx == g.ny && sizeof(C) * (size_t)g.nx * (g.nx + 2) <= 200 * 1024) {
-        cudaError_t e = fft_xy<T>(g.nx, planes, (long long)g.np * g.nz, (const C *)tw[0], sign, h->stream, false);
+        cudaError_t e = fft_xy<T>(g.nx, planes, (long long)g.np * g.nz, (const C *)tw[0], sign, h->stream, false,
+                                  sizeof(T) == 8 ? h->xy_grid_cap64 : h->xy_grid_cap32, h->kerr.p);
         if (e == cudaSuccess) { xy_done = true; h->launches += 1; }
         else if (e != cudaErrorNotSupported) return check_cuda(e, "fft xy launch");
         else cudaGetLastError();
@@ -529,6 +566,8 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     h->nblk_project = (g.N + h->bm_project - 1) / h->bm_project;
     h->nblk_gather = (g.N + h->bm_gather - 1) / h->bm_gather;
     cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, d->device);
+    h->xy_grid_cap64 = h->nsm * std::max(1, xy_tma_per_sm<double>(g.nx));
+    h->xy_grid_cap32 = h->nsm * std::max(1, xy_tma_per_sm<float>(g.nx));
     {
         // persistent bulk-copy gather: N in whole 32-point tiles, no <= 96, stages that fit
         const int ncol = (g.no + 31) / 32;
