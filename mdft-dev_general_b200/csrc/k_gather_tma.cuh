@@ -1,13 +1,14 @@
 // S7 gather fused with the ideal + external term (same arithmetic as k_gather), as a
-// persistent pipeline: one CTA per SM walks the 32-point tiles blockIdx.x, +gridDim.x, ...
+// persistent pipeline: each resident CTA walks the tiles blockIdx.x, +gridDim.x, ...
 // For each tile, warp 0 issues bulk copies of the tile's projection chunks (np runs of 32
 // complex values), xi, vext and the search direction (three contiguous 32 x no runs of
 // FP64) into one of two shared-memory stages; the copies of the next tile are in flight
 // while the current one is computed.  The gamma -> orientation matrix B (2np x no) stays
 // in shared memory for the whole launch.
 //
-// Warp w owns points 4w..4w+3 of a tile and lane l the orientations l, l+32, l+64 (NCOL
-// columns of 32), so the matrix products read the projections as broadcasts and B
+// Tiles of BM points (32 for FP64, one CTA per SM; 16 for FP32, two CTAs per SM).  Warp w
+// owns points PW w .. PW w + PW-1 (PW = BM/8) and lane l the orientations l, l+32, l+64
+// (NCOL columns of 32), so the matrix products read the projections as broadcasts and B
 // without bank conflicts, and each epilogue store of df is a coalesced 256-byte run.
 // Partial sums (F_id, F_ext, F_exc sum, df.d, max|df|) are kept per thread across tiles
 // and reduced once per CTA in a fixed order.
@@ -23,13 +24,15 @@
 
 namespace mdft {
 
-constexpr int kGtBM = 32;     // points per tile
+constexpr int kGtBM = 32;     // points per tile (FP64); FP32 uses kGtBM32 and two CTAs per SM
+constexpr int kGtBM32 = 16;
 constexpr int kGtStages = 2;  // pipeline depth
 constexpr int kGtThreads = 256;
 
+template <typename T> __host__ __device__ constexpr int gt_bm() { return sizeof(T) == 8 ? kGtBM : kGtBM32; }
 template <typename T>
 __host__ __device__ inline size_t gt_stage_bytes(int np, int no) {
-    return (size_t)np * kGtBM * sizeof(typename Cplx<T>::t) + 3 * (size_t)kGtBM * no * sizeof(double);
+    return (size_t)np * gt_bm<T>() * sizeof(typename Cplx<T>::t) + 3 * (size_t)gt_bm<T>() * no * sizeof(double);
 }
 template <typename T>
 __host__ __device__ inline size_t gt_b_bytes(int np, int ncol) {
@@ -40,35 +43,40 @@ inline size_t gather_tma_smem_bytes(int np, int no, int ncol) {
     return gt_b_bytes<T>(np, ncol) + kGtStages * gt_stage_bytes<T>(np, no);
 }
 
-// four consecutive complex values from shared memory (32- or 64-byte aligned)
-__device__ __forceinline__ void load4(const float2 *p, float2 (&v)[4]) {
-    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
-    v[0] = make_float2(a.x, a.y);
-    v[1] = make_float2(a.z, a.w);
-    v[2] = make_float2(b.x, b.y);
-    v[3] = make_float2(b.z, b.w);
-}
-__device__ __forceinline__ void load4(const double2 *p, double2 (&v)[4]) {
+// PW consecutive complex values from shared memory (PW*sizeof(C)-byte aligned)
+template <int PW>
+__device__ __forceinline__ void loadpw(const float2 *p, float2 (&v)[PW]) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = p[k];
+    for (int k = 0; k < PW; k += 2) {
+        const float4 a = reinterpret_cast<const float4 *>(p)[k / 2];
+        v[k] = make_float2(a.x, a.y);
+        v[k + 1] = make_float2(a.z, a.w);
+    }
+}
+template <int PW>
+__device__ __forceinline__ void loadpw(const double2 *p, double2 (&v)[PW]) {
+#pragma unroll
+    for (int k = 0; k < PW; ++k) v[k] = p[k];
 }
 
 template <typename T, int NCOL>
-__global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cplx<T>::t *__restrict__ planes,
+__global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_tma(const typename Cplx<T>::t *__restrict__ planes,
                                                               const T *__restrict__ B, const double *__restrict__ xi,
                                                               const double *__restrict__ vext, const double *__restrict__ w,
                                                               double *__restrict__ df, double *__restrict__ partial,
                                                               int *__restrict__ err, GatherArgs a, int ntiles) {
     using C = typename Cplx<T>::t;
     constexpr int NC = 32 * NCOL;
+    constexpr int BM = gt_bm<T>();   // points per tile
+    constexpr int PW = BM / 8;       // points per warp
     const int no = a.no, np = a.np, K = 2 * np;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     extern __shared__ __align__(128) unsigned char gt_smem[];
     T *Bs = reinterpret_cast<T *>(gt_smem);
     unsigned char *stage0 = gt_smem + gt_b_bytes<T>(np, NCOL);
     const size_t sbytes = gt_stage_bytes<T>(np, no);
-    const size_t plbytes = (size_t)np * kGtBM * sizeof(C);
-    const size_t fbytes = (size_t)kGtBM * no * sizeof(double);
+    const size_t plbytes = (size_t)np * BM * sizeof(C);
+    const size_t fbytes = (size_t)BM * no * sizeof(double);
     __shared__ uint64_t full[kGtStages];
     __shared__ int abort_flag;
     __shared__ double red[kGatherSums][kGtThreads / 32];
@@ -79,14 +87,14 @@ __global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cpl
 
     auto issue = [&](int i) {  // warp 0: copies of this CTA's i-th tile into stage i % S
         const int s = i % kGtStages;
-        const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * kGtBM;
+        const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * BM;
         unsigned char *st = stage0 + s * sbytes;
         if (lane == 0) mbar_arrive_expect_tx(&full[s], tx);
         __syncwarp();
         const int ncopy = np + 3;
         for (int c = lane; c < ncopy; c += 32) {
             if (c < np) {
-                bulk_load(st + (size_t)c * kGtBM * sizeof(C), planes + (size_t)c * a.N + pt0, (uint32_t)(kGtBM * sizeof(C)), &full[s]);
+                bulk_load(st + (size_t)c * BM * sizeof(C), planes + (size_t)c * a.N + pt0, (uint32_t)(BM * sizeof(C)), &full[s]);
             } else if (c == np) {
                 bulk_load(st + plbytes, xi + pt0 * no, (uint32_t)fbytes, &full[s]);
             } else if (c == np + 1) {
@@ -125,23 +133,23 @@ __global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cpl
             const unsigned char *st = stage0 + s * sbytes;
             const C *pl = reinterpret_cast<const C *>(st);
             const double *xs = reinterpret_cast<const double *>(st + plbytes);
-            const double *vs = xs + (size_t)kGtBM * no;
-            const double *ds = vs + (size_t)kGtBM * no;
-            T acc[4][NCOL];
+            const double *vs = xs + (size_t)BM * no;
+            const double *ds = vs + (size_t)BM * no;
+            T acc[PW][NCOL];
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
+            for (int p = 0; p < PW; ++p)
 #pragma unroll
                 for (int c = 0; c < NCOL; ++c) acc[p][c] = (T)0;
 #pragma unroll 4
             for (int ip = 0; ip < np; ++ip) {
-                C av[4];
-                load4(pl + ip * kGtBM + 4 * warp, av);
+                C av[PW];
+                loadpw<PW>(pl + ip * BM + PW * warp, av);
                 const T *br = Bs + (size_t)(2 * ip) * NC + lane;
 #pragma unroll
                 for (int c = 0; c < NCOL; ++c) {
                     const T bre = br[32 * c], bim = br[NC + 32 * c];
 #pragma unroll
-                    for (int p = 0; p < 4; ++p) {
+                    for (int p = 0; p < PW; ++p) {
                         acc[p][c] = fma(av[p].x, bre, acc[p][c]);
                         acc[p][c] = fma(av[p].y, bim, acc[p][c]);
                     }
@@ -152,14 +160,14 @@ __global__ void __launch_bounds__(kGtThreads, 1) k_gather_tma(const typename Cpl
             // element (e = 0); their results are not stored.  FP64 evaluations do the
             // per-element arithmetic in FP64; FP32 evaluations in FP32 (the pipeline's own
             // precision).  The sums are FP64 in both.
-            const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * kGtBM;
+            const long long pt0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * BM;
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
+            for (int p = 0; p < PW; ++p)
 #pragma unroll
                 for (int c = 0; c < NCOL; ++c) {
                     const int io = lane + 32 * c;
                     const bool valid = io < no;
-                    const size_t e = valid ? (size_t)(4 * warp + p) * no + io : 0;
+                    const size_t e = valid ? (size_t)(PW * warp + p) * no + io : 0;
                     const T wio = (T)wv[c], r0 = (T)a.rho0;
                     const T vexc = (T)pre * wio * acc[p][c];
                     const T x = (T)xs[e];

@@ -394,8 +394,8 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     auto al16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
     long long red_blocks = h->nblk_gather;
     if (gt_ncol > 0 && ga.df_mode != 2 && al16(d_xi) && al16(dvec)) {
-        const int ntiles = (int)(g.N / kGtBM);
-        const int grid = std::min(ntiles, h->nsm);
+        const int ntiles = (int)(g.N / gt_bm<T>());
+        const int grid = std::min(ntiles, h->nsm * (dbl ? 1 : 2));
         const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
         if (gt_ncol == 1)
             k_gather_tma<T, 1><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
@@ -571,7 +571,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     {
         // persistent bulk-copy gather: N in whole 32-point tiles, no <= 96, stages that fit
         const int ncol = (g.no + 31) / 32;
-        const bool shape_ok = g.N % kGtBM == 0 && ncol <= 3;
+        const bool shape_ok = g.N % kGtBM == 0 && ncol <= 3;  // kGtBM32 divides kGtBM
         h->gt_ncol64 = (shape_ok && gather_tma_smem_bytes<double>(g.np, g.no, ncol) <= dyn_max) ? ncol : 0;
         h->gt_ncol32 = (shape_ok && gather_tma_smem_bytes<float>(g.np, g.no, ncol) <= dyn_max) ? ncol : 0;
         // persistent bulk-copy projection: N in whole 64-point tiles, np <= 32
@@ -587,7 +587,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
             if ((rc = allow_smem(fn, maxsmem))) return rc;
     }
     {
-        const size_t rows = std::max<long long>(h->nblk_gather, h->nsm);
+        const size_t rows = std::max<long long>(h->nblk_gather, 2 * h->nsm);
         if ((rc = alloc_check(h->partial.alloc(kGatherSums * rows), "partials", 8 * kGatherSums * rows))) return rc;
     }
     if ((rc = alloc_check(h->kerr.alloc(1), "error flag", 4))) return rc;
