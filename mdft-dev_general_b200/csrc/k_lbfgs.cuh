@@ -9,8 +9,9 @@
 // for the combination (k_direction, which also stores the accepted pair) -- instead of the
 // four passes per pair of the two-loop recursion.
 //
-// History storage TS: double (FP64 solves, the reference's arithmetic) or float (mixed
-// solves: pairs are rounded to FP32 when stored and every product uses the stored values).
+// History storage TS: double (FP64 solves, the reference's arithmetic) or __nv_bfloat16
+// (mixed solves: pairs are rounded to BF16 when stored and every product, in FP64, uses the
+// stored values, so the compact matrix stays the exact BFGS matrix of the stored pairs).
 // VEC = 2: a thread takes element pairs (n even; all vectors are then 2-element aligned).
 // Every reduction is two-stage with the fixed grid kRedBlocks and a fixed summation order
 // for a given (grid, VEC), so results are reproducible run to run.
@@ -18,6 +19,8 @@
 
 #include "common.cuh"
 #include "k_vec.cuh"
+
+#include <cuda_bf16.h>
 
 namespace mdft {
 
@@ -63,6 +66,7 @@ __device__ __forceinline__ void block_rows_store(double (&acc)[R], double *part)
 template <typename TS> struct Pair2;
 template <> struct Pair2<double> { using t = double2; };
 template <> struct Pair2<float> { using t = float2; };
+template <> struct Pair2<__nv_bfloat16> { using t = __nv_bfloat162; };
 
 // one element: sk, yk are the slots' values there
 template <typename TS, int K, bool PAIR, bool SELF>

@@ -397,12 +397,12 @@ constexpr double kMixedNoiseRel = 1e-6;
 
 struct LbfgsHist {
     int m = 0, col = 0, head = 0;
-    bool f32 = false;                          // pairs stored in FP32 (mixed solves)
+    bool low = false;                          // pairs stored in BF16 (mixed solves)
     double theta = 1.0, gg = 0.0, sty = 0.0;  // sty: s.y of the pair formed last, from the stored values
     std::vector<double> sy, yy, sg, yg;
-    void reset(int mm, bool single = false) {
+    void reset(int mm, bool lowp = false) {
         m = mm;
-        f32 = single;
+        low = lowp;
         col = 0;
         head = 0;
         theta = 1.0;
@@ -418,7 +418,7 @@ constexpr int kRowsBase = 64;  // first device scalar slot of the history inner 
 
 // slot j of the S or Y history in the storage type of H
 inline void *hist_slot(const LbfgsHist &H, double *base, int j, long long n) {
-    return H.f32 ? (void *)(reinterpret_cast<float *>(base) + (size_t)j * n) : (void *)(base + (size_t)j * n);
+    return H.low ? (void *)(reinterpret_cast<__nv_bfloat16 *>(base) + (size_t)j * n) : (void *)(base + (size_t)j * n);
 }
 
 template <typename TS, int K, bool PAIR, bool SELF>
@@ -427,11 +427,11 @@ void launch_dots_v(const PairDotsArgs &a, cudaStream_t st) {
     else k_pair_dots<TS, K, PAIR, SELF, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
 }
 template <int K>
-void launch_dots(bool f32, bool pair, bool self, const PairDotsArgs &a, cudaStream_t st) {
-    if (f32) {
-        if (!pair) launch_dots_v<float, K, false, false>(a, st);
-        else if (self) launch_dots_v<float, K, true, true>(a, st);
-        else launch_dots_v<float, K, true, false>(a, st);
+void launch_dots(bool low, bool pair, bool self, const PairDotsArgs &a, cudaStream_t st) {
+    if (low) {
+        if (!pair) launch_dots_v<__nv_bfloat16, K, false, false>(a, st);
+        else if (self) launch_dots_v<__nv_bfloat16, K, true, true>(a, st);
+        else launch_dots_v<__nv_bfloat16, K, true, false>(a, st);
     } else {
         if (!pair) launch_dots_v<double, K, false, false>(a, st);
         else if (self) launch_dots_v<double, K, true, true>(a, st);
@@ -479,15 +479,15 @@ int launch_history_dots(mdft_handle *h, const LbfgsHist &H, const double *g, con
         a.n = n;
         a.part = h->vpart.p;
         switch (K) {
-            case 0: launch_dots<0>(H.f32, P.pair, self, a, st); break;
-            case 1: launch_dots<1>(H.f32, P.pair, self, a, st); break;
-            case 2: launch_dots<2>(H.f32, P.pair, self, a, st); break;
-            case 3: launch_dots<3>(H.f32, P.pair, self, a, st); break;
-            case 4: launch_dots<4>(H.f32, P.pair, self, a, st); break;
-            case 5: launch_dots<5>(H.f32, P.pair, self, a, st); break;
-            case 6: launch_dots<6>(H.f32, P.pair, self, a, st); break;
-            case 7: launch_dots<7>(H.f32, P.pair, self, a, st); break;
-            default: launch_dots<8>(H.f32, P.pair, self, a, st); break;
+            case 0: launch_dots<0>(H.low, P.pair, self, a, st); break;
+            case 1: launch_dots<1>(H.low, P.pair, self, a, st); break;
+            case 2: launch_dots<2>(H.low, P.pair, self, a, st); break;
+            case 3: launch_dots<3>(H.low, P.pair, self, a, st); break;
+            case 4: launch_dots<4>(H.low, P.pair, self, a, st); break;
+            case 5: launch_dots<5>(H.low, P.pair, self, a, st); break;
+            case 6: launch_dots<6>(H.low, P.pair, self, a, st); break;
+            case 7: launch_dots<7>(H.low, P.pair, self, a, st); break;
+            default: launch_dots<8>(H.low, P.pair, self, a, st); break;
         }
         k_finish_rows<<<rows, 256, 0, st>>>(h->vpart.p, (int)vec_grid(), h->vsc.p + off);
         h->launches += 2;
@@ -555,20 +555,20 @@ int history_dots_now(mdft_handle *h, LbfgsHist &H, const double *g) {
 }
 
 template <int K, bool NP>
-void launch_direction_k(bool f32, const DirArgs &a, cudaStream_t st) {
+void launch_direction_k(bool low, const DirArgs &a, cudaStream_t st) {
     const bool v2 = a.n % 2 == 0;
-    if (f32) {
-        if (v2) k_direction<float, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<float, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    if (low) {
+        if (v2) k_direction<__nv_bfloat16, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<__nv_bfloat16, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     } else {
         if (v2) k_direction<double, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
         else k_direction<double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     }
 }
 template <int K>
-void launch_direction(bool f32, bool np, const DirArgs &a, cudaStream_t st) {
-    if (np) launch_direction_k<K, true>(f32, a, st);
-    else launch_direction_k<K, false>(f32, a, st);
+void launch_direction(bool low, bool np, const DirArgs &a, cudaStream_t st) {
+    if (np) launch_direction_k<K, true>(low, a, st);
+    else launch_direction_k<K, false>(low, a, st);
 }
 
 // Pair accepted in the last step and not yet stored: k_direction forms it from the
@@ -664,15 +664,15 @@ int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, co
             a.stp_t = stp_t;
         }
         switch (K) {
-            case 0: launch_direction<0>(H.f32, np, a, st); break;
-            case 2: launch_direction<2>(H.f32, np, a, st); break;
-            case 4: launch_direction<4>(H.f32, np, a, st); break;
-            case 6: launch_direction<6>(H.f32, np, a, st); break;
-            case 8: launch_direction<8>(H.f32, np, a, st); break;
-            case 10: launch_direction<10>(H.f32, np, a, st); break;
-            case 12: launch_direction<12>(H.f32, np, a, st); break;
-            case 14: launch_direction<14>(H.f32, np, a, st); break;
-            default: launch_direction<16>(H.f32, np, a, st); break;
+            case 0: launch_direction<0>(H.low, np, a, st); break;
+            case 2: launch_direction<2>(H.low, np, a, st); break;
+            case 4: launch_direction<4>(H.low, np, a, st); break;
+            case 6: launch_direction<6>(H.low, np, a, st); break;
+            case 8: launch_direction<8>(H.low, np, a, st); break;
+            case 10: launch_direction<10>(H.low, np, a, st); break;
+            case 12: launch_direction<12>(H.low, np, a, st); break;
+            case 14: launch_direction<14>(H.low, np, a, st); break;
+            default: launch_direction<16>(H.low, np, a, st); break;
         }
         h->launches += 1;
     }
@@ -714,7 +714,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     const long long n = L.n;
     const int m = o->m;
     cudaStream_t st = h->stream;
-    if (H.m != m) H.reset(m, H.f32);
+    if (H.m != m) H.reset(m, H.low);
     double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
@@ -823,8 +823,8 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         H.yy[(size_t)t * m + t] = PR.yy;
         H.sg[t] = PR.sg;
         H.yg[t] = PR.yg;
-        // FP64 history: s.y = dr as the reference's matupd; FP32 history: s.y of the stored pair
-        const double sty = H.f32 ? PR.sy : dr;
+        // FP64 history: s.y = dr as the reference's matupd; BF16 history: s.y of the stored pair
+        const double sty = H.low ? PR.sy : dr;
         H.sy[(size_t)t * m + t] = sty;
         H.theta = PR.yy / sty;
         pend.slot = t;
