@@ -8,7 +8,8 @@ U[0.2,1.0], q ~ N(0,0.3) shifted to 0) in SPC/E-like 3-site water, 64^3 grid,
 L-BFGS (m=5, stop at max|df| <= 1e-4 in FP64; the reference's F-decrease test
 is off, it stops ~1 kJ/mol short of the converged dG) -> pressure correction -> dG.
 Every run re-solves its solutes in FP64 to max|df| <= 1e-6 and reports the largest
-|dG - dG_FP64| (the metric's 0.1 kJ/mol bar).  Synthetic inputs stand in for the reference's data.
+|dG - dG_FP64| (the metric's 0.1 kJ/mol bar).  The steps' solutes are solved through
+mdft_solve_batch on --workers engine handles (default 3), so that solves overlap on the GPU.  Synthetic inputs stand in for the reference's data.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -51,7 +52,7 @@ NCU_TRAFFIC_BYTES = {("mixed", "oz"): 67.3e6, ("mixed", "gather"): 562.0e6, ("mi
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -59,6 +60,8 @@ def parse():
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 excess pipeline then an FP64 polish; fp64: plain FP64 solve")
     ap.add_argument("--pgtol", type=float, default=PGTOL, help="stop at max|df| <= pgtol (FP64 gradient)")
+    ap.add_argument("--workers", type=int, default=3,
+                    help="concurrent solves per GPU (engine handles, each with its own buffers and stream)")
     ap.add_argument("--pgtol-mixed", type=float, default=0.0, help="FP32-phase stop (<=0: the final pgtol)")
     ap.add_argument("--polish", type=int, default=1, help="mixed: 1 = FP64 iterations until pgtol, 0 = one FP64 evaluation")
     ap.add_argument("--solves", type=int, default=0,
@@ -210,7 +213,7 @@ def main():
         return reference_arm(args, rank, world)
     import torch
     import torch.distributed as dist
-    from mdft_b200 import Engine, PREC_FP64, PREC_MIXED, synth
+    from mdft_b200 import Engine, PREC_FP64, PREC_MIXED, solve_batch, synth
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -248,48 +251,58 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- value: solute in, dG out; density stays in HBM ----
-    results = []
-    for i in range(args.warmup):
-        results.append(eng.solve(sols[i], sv, rvdw=rvdw, **opts))
-    l0 = eng.launch_count
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        ev0.record(stream)
-        for i in range(args.warmup, args.warmup + args.steps):
-            results.append(eng.solve(sols[i], sv, rvdw=rvdw, **opts))
-        ev1.record(stream)
+    # ---- W engine handles solve the steps' solutes concurrently (mdft_solve_batch) ----
+    W = max(1, args.workers)
+    engines = [eng] + [Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec)
+                       for _ in range(W - 1)]
+    streams = [torch.cuda.ExternalStream(e.stream) for e in engines]
+
+    def timed_batch(idx, xi_bufs=None):
+        """solve sols[idx] on the W handles; device time from an event before every stream's
+        first kernel to one after every stream's last."""
+        master = torch.cuda.current_stream()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(master)
+        for st in streams:
+            st.wait_event(ev0)
+        res = solve_batch(engines, [sols[i] for i in idx], sv, rvdw=rvdw, xi_out=xi_bufs, **opts)
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            master.wait_event(e)
+        ev1.record(master)
         barrier()
-    launches = eng.launch_count - l0
-    t_ms = ev0.elapsed_time(ev1)
+        return res, ev0.elapsed_time(ev1)
+
+    # ---- value: solute in, dG out; density stays in HBM ----
+    # warm-up: every handle solves at least one solute (first-solve allocations happen here)
+    warm = list(range(args.warmup))
+    solve_batch(engines, [sols[i] for i in warm], sv, rvdw=rvdw, handles=[i % W for i in warm], **opts)
+    l0 = sum(e.launch_count for e in engines)
+    barrier()
+    steps_idx = list(range(args.warmup, args.warmup + args.steps))
+    with Clocks(local) as clk:
+        timed, t_ms = timed_batch(steps_idx)
+    launches = sum(e.launch_count for e in engines) - l0
     t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     t_ms = float(t.item())
     value = world * args.steps / (t_ms / 1e3)
-    timed = results[args.warmup:]
     evals = [r["evaluations"] for r in timed]
 
-    # ---- e2e: the same call with the converged density returned to pinned host memory ----
-    xi_pinned = torch.empty(int(np.prod(eng.shape)), dtype=torch.float64, pin_memory=True)
-    xi_host = xi_pinned.numpy()
-    for i in range(min(2, args.warmup)):
-        eng.solve(sols[i], sv, rvdw=rvdw, xi_out=xi_host, **opts)
+    # ---- e2e: the same call with each converged density returned to pinned host memory ----
+    xi_pinned = [torch.empty(int(np.prod(eng.shape)), dtype=torch.float64, pin_memory=True) for _ in steps_idx]
+    xi_host = [b.numpy().reshape(eng.shape) for b in xi_pinned]
     barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.warmup, args.warmup + args.steps):
-        eng.solve(sols[i], sv, rvdw=rvdw, xi_out=xi_host, **opts)
-    e1.record(stream)
-    barrier()
-    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    _, te_ms = timed_batch(steps_idx, xi_bufs=xi_host)
+    te = torch.tensor([te_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps / (float(te.item()) / 1e3)
     s0 = sols[0]
     h2d = 8 * (4 * s0.nsite + 4 * 3 * 2)  # solute q, sig, eps, xyz + solvent sites
-    d2h = xi_host.nbytes + 8 * 6
+    d2h = xi_host[0].nbytes + 8 * 6
 
     # ---- FP64 reference dG of the timed solutes, converged to PGTOL_REF (outside the timed regions) ----
     ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
@@ -299,7 +312,7 @@ def main():
     dg_err = [abs(r["dG"] - d) for r, d in zip(timed, dg_ref)]
 
     # ---- roofline of the dominant stage: per-stage CUDA events over evaluations at a converged density ----
-    xi_ref = xi_host.reshape(eng.shape).copy()
+    xi_ref = xi_host[0].copy()
     eng.set_timing(True)
     for _ in range(5):
         eng.energy_and_gradient(xi_ref)  # in the engine's evaluation precision
@@ -337,7 +350,8 @@ def main():
                            "stop": "max|df|<=%g in FP64 (line-search stall accepted); dG checked against FP64 "
                                    "solves to max|df|<=%g" % (args.pgtol, PGTOL_REF),
                            "l2": "inputs larger than L2 (176 MB per field)",
-                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "parallelism": ("replicas" if world > 1 else "single GPU") + ", %d concurrent solves per GPU" % W,
+                           "workers": W,
                            "evaluations_per_solve": evals,
                            "fp32_evaluations_per_solve": [r.get("evaluations_mixed", 0) for r in timed],
                            "dG": [r["dG"] for r in timed], "dG_fp64": dg_ref,
@@ -345,7 +359,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line))
-    eng.close()
+    for e in engines:
+        e.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -178,6 +178,29 @@ int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, co
 
 int mdft_pressure_correction_device(mdft_handle *h, const double *d_xi, double ftot, double lj_tail, double *out);
 
+/* One solute of a batch: sites as in mdft_solve; handle = index into the batch's handle
+ * array to solve it on, or -1 for the next free handle; xi_out: host buffer for its
+ * converged density (may be NULL). */
+typedef struct mdft_solute {
+    int nsite;
+    const double *q, *sig, *eps, *xyz;
+    int handle;
+    double *xi_out;
+} mdft_solute;
+
+/* A batch of independent solves (no counterpart in the reference, which solves one solute
+ * per run).  Each handle gets one host worker thread that runs mdft_solve for the solutes
+ * assigned to it and then for unassigned ones (handle -1) as they come free, so solves on
+ * different handles -- each with its own device buffers and stream -- run concurrently on
+ * the GPU.  Handles may differ in grid and mmax (a solute with handle -1 must fit every
+ * handle).  out: 6 doubles per solute as mdft_solve's; res: one result per solute; rc (may
+ * be NULL): each solute's mdft_solve return code.  Returns MDFT_OK when every solve succeeded,
+ * else the first failing code with its message in mdft_last_error.  The handles must not be
+ * used by other threads during the call. */
+int mdft_solve_batch(mdft_handle *const *handles, int nhandles, const mdft_solute *solutes, int nsolutes, int nsolvsite,
+                     const double *sq, const double *ssig, const double *seps, const double *sxyz, double rvdw, double eps_r,
+                     const mdft_minimize_opts *opts, double *out, mdft_minimize_result *res, int *rc);
+
 /* Per-stage device time (ms) of the last evaluations, when timing is on:
  * stage order {project, fft_forward, oz, fft_inverse, gather}; count = calls. */
 int mdft_set_timing(mdft_handle *h, int on);

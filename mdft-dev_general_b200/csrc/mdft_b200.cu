@@ -6,7 +6,10 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <memory>
+#include <string>
+#include <thread>
 
 #include "common.cuh"
 #include "setup_host.cuh"

@@ -1038,3 +1038,62 @@ int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, co
 }
 
 }  // extern "C"
+
+extern "C" int mdft_solve_batch(mdft_handle *const *handles, int nhandles, const mdft_solute *solutes, int nsolutes,
+                                int nsv, const double *sq, const double *ssig, const double *seps, const double *sxyz, double rvdw,
+                                double eps_r, const mdft_minimize_opts *opts, double *out, mdft_minimize_result *res, int *rc) {
+    if (!handles || nhandles <= 0 || (nsolutes > 0 && !solutes) || !opts || (nsolutes > 0 && (!out || !res))) {
+        set_error("null argument or no handle");
+        return MDFT_E_ARG;
+    }
+    for (int k = 0; k < nhandles; ++k)
+        if (!handles[k]) { set_error("null handle %d", k); return MDFT_E_ARG; }
+    for (int i = 0; i < nsolutes; ++i)
+        if (solutes[i].handle < -1 || solutes[i].handle >= nhandles) {
+            set_error("solute %d: handle %d out of range", i, solutes[i].handle);
+            return MDFT_E_ARG;
+        }
+    std::vector<int> codes(nsolutes, MDFT_OK);
+    std::vector<std::string> msgs(nsolutes);
+    std::atomic<int> next_free{0};
+    auto worker = [&](int k) {
+        mdft_handle *h = handles[k];
+        if (cudaSetDevice(h->device) != cudaSuccess) {
+            for (int i = 0; i < nsolutes; ++i)
+                if (solutes[i].handle == k) { codes[i] = MDFT_E_CUDA; msgs[i] = "cudaSetDevice failed"; }
+            return;
+        }
+        auto run = [&](int i) {
+            const mdft_solute &u = solutes[i];
+            codes[i] = mdft_solve(h, u.nsite, u.q, u.sig, u.eps, u.xyz, nsv, sq, ssig, seps, sxyz, rvdw, eps_r, opts, u.xi_out,
+                                  out + 6 * (size_t)i, res + i);
+            if (codes[i]) msgs[i] = last_error();
+        };
+        for (int i = 0; i < nsolutes; ++i)
+            if (solutes[i].handle == k) run(i);
+        // unassigned solutes, in order, to whichever handle is free
+        for (;;) {
+            int i = next_free.fetch_add(1);
+            while (i < nsolutes && solutes[i].handle != -1) i = next_free.fetch_add(1);
+            if (i >= nsolutes) break;
+            run(i);
+        }
+    };
+    if (nhandles == 1) {
+        worker(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int k = 0; k < nhandles; ++k) pool.emplace_back(worker, k);
+        for (auto &t : pool) t.join();
+    }
+    int first = MDFT_OK;
+    for (int i = 0; i < nsolutes; ++i) {
+        if (rc) rc[i] = codes[i];
+        if (codes[i] && first == MDFT_OK) {
+            first = codes[i];
+            set_error("solute %d: %s", i, msgs[i].c_str());
+        }
+    }
+    return first;
+}
+

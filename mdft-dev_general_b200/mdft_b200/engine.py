@@ -60,6 +60,11 @@ class _MinRes(C.Structure):
 
 _DP = C.POINTER(C.c_double)
 
+
+class _Solute(C.Structure):
+    _fields_ = [("nsite", C.c_int), ("q", _DP), ("sig", _DP), ("eps", _DP), ("xyz", _DP), ("handle", C.c_int),
+                ("xi_out", _DP)]
+
 # every entry point declared in include/mdft_b200.h: name -> (restype, argtypes)
 SIGNATURES = {
     "mdft_create": (C.c_int, [C.POINTER(_Desc), C.POINTER(C.c_void_p)]),
@@ -87,6 +92,8 @@ SIGNATURES = {
     "mdft_pressure_correction_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, _DP]),
     "mdft_solve": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP, C.c_double,
                              C.c_double, C.POINTER(_MinOpts), _DP, _DP, C.POINTER(_MinRes)]),
+    "mdft_solve_batch": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.c_int, C.c_int, _DP, _DP, _DP, _DP,
+                                   C.c_double, C.c_double, C.POINTER(_MinOpts), _DP, C.c_void_p, C.POINTER(C.c_int)]),
     "mdft_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "mdft_get_stage_times": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int)]),
 }
@@ -292,3 +299,32 @@ class Engine:
         cnt = C.c_int()
         _check(lib().mdft_get_stage_times(self.h, _p(ms), C.byref(cnt)))
         return dict(zip(("project", "fft_forward", "oz", "fft_inverse", "gather"), ms)), cnt.value
+
+
+def solve_batch(engines, solutes, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
+                pgtol_mixed=0.0, polish=1, handles=None, xi_out=None):
+    """Solve many solutes concurrently: one host worker per engine (each engine has its own
+    device buffers and stream), solutes assigned by `handles` (index per solute, -1 or None:
+    the next free engine).  xi_out: optional list of host arrays (or None entries) for the
+    converged densities.  Returns one result dict per solute, as Engine.solve's."""
+    n = len(solutes)
+    keep = []
+    arr = (_Solute * max(1, n))()
+    for i, s in enumerate(solutes):
+        q, sg, ep, xyz = (np.ascontiguousarray(v, dtype=np.float64) for v in (s.q, s.sig, s.eps, s.xyz))
+        xo = None if xi_out is None else xi_out[i]
+        keep += [q, sg, ep, xyz, xo]
+        arr[i] = _Solute(len(q), _p(q), _p(sg), _p(ep), _p(xyz), -1 if handles is None else int(handles[i]), _p(xo))
+    hs = (C.c_void_p * len(engines))(*[e.h for e in engines])
+    vq, vs, ve, vx = (np.array(v, dtype=np.float64) for v in (solvent.q, solvent.sig, solvent.eps, solvent.xyz))
+    o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
+    out = np.zeros(6 * max(1, n))
+    res = (_MinRes * max(1, n))()
+    rc = (C.c_int * max(1, n))()
+    _check(lib().mdft_solve_batch(hs, len(engines), C.cast(arr, C.c_void_p), n, len(vq), _p(vq), _p(vs), _p(ve), _p(vx),
+                                  float(rvdw), float(solvent.eps_r), C.byref(o), _p(out), C.cast(res, C.c_void_p), rc))
+    del keep
+    return [dict(dG=out[6 * i], f=out[6 * i + 1], pmv=out[6 * i + 2], lj_tail=out[6 * i + 3], pbulk=out[6 * i + 4],
+                 deltaN=out[6 * i + 5], pgnorm=res[i].pgnorm, iterations=res[i].iterations, evaluations=res[i].evaluations,
+                 status=res[i].status, evaluations_mixed=res[i].evaluations_mixed) for i in range(n)]
+

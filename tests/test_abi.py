@@ -39,3 +39,20 @@ def test_argument_errors_without_gpu():
     assert L.mdft_create(ctypes.byref(d), ctypes.byref(h)) == -2
     assert b"cannot open" in L.mdft_last_error()
     assert L.mdft_destroy(None) == 0
+
+
+def test_batch_argument_errors_without_gpu():
+    L = engine.lib()
+    o = engine._MinOpts(5, 1e-4, -1.0, 100, 0, 0.0, 1)
+    out = (ctypes.c_double * 6)()
+    res = (engine._MinRes * 1)()
+    # no handle
+    assert L.mdft_solve_batch(None, 0, None, 0, 0, None, None, None, None, 10.0, 71.0, ctypes.byref(o), None, None, None) == -1
+    # a solute pointing past the handle array is rejected before any handle is touched
+    hs = (ctypes.c_void_p * 1)(ctypes.c_void_p(1))
+    sol = (engine._Solute * 1)()
+    sol[0] = engine._Solute(1, None, None, None, None, 3, None)
+    rc = L.mdft_solve_batch(hs, 1, ctypes.cast(sol, ctypes.c_void_p), 1, 0, None, None, None, None, 10.0, 71.0,
+                            ctypes.byref(o), ctypes.cast(out, engine._DP), ctypes.cast(res, ctypes.c_void_p), None)
+    assert rc == -1
+    assert b"out of range" in L.mdft_last_error()
