@@ -9,7 +9,8 @@ L-BFGS (m=5, stop at max|df| <= 1e-4 in FP64; the reference's F-decrease test
 is off, it stops ~1 kJ/mol short of the converged dG) -> pressure correction -> dG.
 Every run re-solves its solutes in FP64 to max|df| <= 1e-6 and reports the largest
 |dG - dG_FP64| (the metric's 0.1 kJ/mol bar).  The steps' solutes are solved through
-mdft_solve_batch on --workers engine handles (default 3), so that solves overlap on the GPU.  Synthetic inputs stand in for the reference's data.
+mdft_solve_batch on --workers engine handles (default 3), so that solves overlap
+on the GPU.  Synthetic inputs stand in for the reference's data.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
