@@ -38,7 +38,8 @@ struct GatherArgs {
     double rho0, kT, dv, prefactor, cst;  // prefactor = -kT 2 (4 pi^2)/mrso/n0, cst = 1/N
     int do_ideal;                         // add F_id, F_ext and their gradient
     int df_mode;                          // 0 none, 1 store (id + exc), 2 accumulate exc
-    const double *dvec;                   // df_mode 1: also df.dvec (null: df.df is not wanted -> 0)
+    const void *dvec;                     // df_mode 1: also df.dvec (null: df.df is not wanted -> 0);
+                                          // FP64, or the type of df in k_gather_tma
 };
 
 template <typename T> struct Vec4;
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
             if (a.df_mode == 1) {
                 const double gv = did + dexc;
                 df[g] = gv;
-                if (a.dvec) gdv = fma(gv, a.dvec[g], gdv);
+                if (a.dvec) gdv = fma(gv, static_cast<const double *>(a.dvec)[g], gdv);
                 gmx = fmax(gmx, fabs(gv));
             } else if (a.df_mode == 2) {
                 df[g] = df[g] + dexc;

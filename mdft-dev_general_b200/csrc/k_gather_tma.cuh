@@ -59,11 +59,12 @@ __device__ __forceinline__ void loadpw(const double2 *p, double2 (&v)[PW]) {
     for (int k = 0; k < PW; ++k) v[k] = p[k];
 }
 
-template <typename T, int NCOL>
+// TD: type of df and of the search direction (double, or float for the FP32 L-BFGS vectors)
+template <typename T, int NCOL, typename TD>
 __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_tma(const typename Cplx<T>::t *__restrict__ planes,
                                                               const T *__restrict__ B, const double *__restrict__ xi,
                                                               const double *__restrict__ vext, const double *__restrict__ w,
-                                                              double *__restrict__ df, double *__restrict__ partial,
+                                                              TD *__restrict__ df, double *__restrict__ partial,
                                                               int *__restrict__ err, GatherArgs a, int ntiles) {
     using C = typename Cplx<T>::t;
     constexpr int NC = 32 * NCOL;
@@ -82,7 +83,8 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
     __shared__ double red[kGatherSums][kGtThreads / 32];
 
     const bool want_v = a.do_ideal != 0, want_d = a.df_mode == 1 && a.dvec != nullptr;
-    const uint32_t tx = (uint32_t)(plbytes + fbytes * (1 + (want_v ? 1 : 0) + (want_d ? 1 : 0)));
+    const size_t dbytes = (size_t)BM * no * sizeof(TD);
+    const uint32_t tx = (uint32_t)(plbytes + fbytes * (1 + (want_v ? 1 : 0)) + (want_d ? dbytes : 0));
     const int nmine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
     auto issue = [&](int i) {  // warp 0: copies of this CTA's i-th tile into stage i % S
@@ -100,7 +102,8 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
             } else if (c == np + 1) {
                 if (want_v) bulk_load(st + plbytes + fbytes, vext + pt0 * no, (uint32_t)fbytes, &full[s]);
             } else {
-                if (want_d) bulk_load(st + plbytes + 2 * fbytes, a.dvec + pt0 * no, (uint32_t)fbytes, &full[s]);
+                if (want_d)
+                    bulk_load(st + plbytes + 2 * fbytes, static_cast<const TD *>(a.dvec) + pt0 * no, (uint32_t)dbytes, &full[s]);
             }
         }
     };
@@ -134,7 +137,7 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
             const C *pl = reinterpret_cast<const C *>(st);
             const double *xs = reinterpret_cast<const double *>(st + plbytes);
             const double *vs = xs + (size_t)BM * no;
-            const double *ds = vs + (size_t)BM * no;
+            const TD *ds = reinterpret_cast<const TD *>(vs + (size_t)BM * no);
             T acc[PW][NCOL];
 #pragma unroll
             for (int p = 0; p < PW; ++p)
@@ -187,8 +190,8 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
                     }
                     if (a.df_mode == 1) {
                         const double gv = (double)(did + dexc);
-                        if (valid) df[pt0 * no + e] = gv;
-                        if (want_d) gdv = fma(gv, ds[e], gdv);
+                        if (valid) df[pt0 * no + e] = (TD)gv;
+                        if (want_d) gdv = fma(gv, (double)ds[e], gdv);
                         gmx = fmax(gmx, fabs(gv));
                     }
                 }

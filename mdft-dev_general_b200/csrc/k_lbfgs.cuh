@@ -12,7 +12,8 @@
 // History storage TS: double (FP64 solves, the reference's arithmetic) or __nv_bfloat16
 // (mixed solves: pairs are rounded to BF16 when stored and every product, in FP64, uses the
 // stored values, so the compact matrix stays the exact BFGS matrix of the stored pairs).
-// VEC = 2: a thread takes element pairs (n even; all vectors are then 2-element aligned).
+// Gradient and direction vectors TV: double (FP64 solves) or float (mixed solves); the
+// point x is FP64 in both.  A thread takes V consecutive elements per step (16 bytes of TV).
 // Every reduction is two-stage with the fixed grid kRedBlocks and a fixed summation order
 // for a given (grid, VEC), so results are reproducible run to run.
 #pragma once
@@ -34,7 +35,7 @@ constexpr int kMaxRows = 4 * kPairGroup + 5;  // reduction rows of one k_pair_do
 //   rows s_i.y_n [2K+1,3K+1), y_i.y_n [3K+1,4K+1)
 // SELF (with PAIR): the candidate's own rows y_n.y_n, y_n.g, s_n.g, s_n.y_n [4K+1,4K+5)
 struct PairDotsArgs {
-    const double *g, *gold, *d;
+    const void *g, *gold, *d;  // vector type TV
     const void *s[kPairGroup], *y[kPairGroup];
     double stp;
     long long n;
@@ -63,10 +64,27 @@ __device__ __forceinline__ void block_rows_store(double (&acc)[R], double *part)
     }
 }
 
-template <typename TS> struct Pair2;
-template <> struct Pair2<double> { using t = double2; };
-template <> struct Pair2<float> { using t = float2; };
-template <> struct Pair2<__nv_bfloat16> { using t = __nv_bfloat162; };
+// V consecutive elements moved as one access (V sizeof(T) bytes, naturally aligned)
+template <int B> struct RawT;
+template <> struct RawT<2> { using t = unsigned short; };
+template <> struct RawT<4> { using t = unsigned int; };
+template <> struct RawT<8> { using t = uint2; };
+template <> struct RawT<16> { using t = uint4; };
+struct alignas(32) Raw32 { uint4 a, b; };
+template <> struct RawT<32> { using t = Raw32; };
+template <typename T, int V>
+__device__ __forceinline__ void vload(const T *p, long long j, T (&v)[V]) {
+    using R = typename RawT<V * (int)sizeof(T)>::t;
+    const R r = reinterpret_cast<const R *>(p)[j];
+    __builtin_memcpy(&v[0], &r, sizeof(R));
+}
+template <typename T, int V>
+__device__ __forceinline__ void vstore(T *p, long long j, const T (&v)[V]) {
+    using R = typename RawT<V * (int)sizeof(T)>::t;
+    R r;
+    __builtin_memcpy(&r, &v[0], sizeof(R));
+    reinterpret_cast<R *>(p)[j] = r;
+}
 
 // one element: sk, yk are the slots' values there
 template <typename TS, int K, bool PAIR, bool SELF>
@@ -96,7 +114,8 @@ __device__ __forceinline__ void pair_dots_elem(double stp, double gi, double gol
     }
 }
 
-template <typename TS, int K, bool PAIR, bool SELF, int VEC>
+// V elements per thread and step (V = 1, or 16 bytes of TV when n is a multiple of V)
+template <typename TS, typename TV, int K, bool PAIR, bool SELF, int V>
 __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
     constexpr int R = pair_rows(K, PAIR, SELF);
     constexpr int KK = K > 0 ? K : 1;
@@ -109,36 +128,30 @@ __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
         sv[k] = static_cast<const TS *>(a.s[k]);
         yv[k] = static_cast<const TS *>(a.y[k]);
     }
+    const TV *gp = static_cast<const TV *>(a.g), *gop = static_cast<const TV *>(a.gold), *dp = static_cast<const TV *>(a.d);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    if constexpr (VEC == 1) {
-        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    const long long nv = a.n / V;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += stride) {
+        TV g[V], go[V], d[V];
+        vload<TV, V>(gp, j, g);
+        if constexpr (PAIR) vload<TV, V>(gop, j, go);
+        if constexpr (PAIR && SELF) vload<TV, V>(dp, j, d);
+        TS sc[KK][V], yc[KK][V];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            vload<TS, V>(sv[k], j, sc[k]);
+            vload<TS, V>(yv[k], j, yc[k]);
+        }
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
             TS sk[KK], yk[KK];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                sk[k] = sv[k][i];
-                yk[k] = yv[k][i];
+                sk[k] = sc[k][e];
+                yk[k] = yc[k][e];
             }
-            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, a.g[i], PAIR ? a.gold[i] : 0.0, PAIR && SELF ? a.d[i] : 0.0, acc, sk, yk);
-        }
-    } else {
-        using P2 = typename Pair2<TS>::t;
-        const long long n2 = a.n / 2;
-        for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += stride) {
-            const double2 g2 = reinterpret_cast<const double2 *>(a.g)[j];
-            double2 go2 = make_double2(0.0, 0.0), d2 = make_double2(0.0, 0.0);
-            if constexpr (PAIR) go2 = reinterpret_cast<const double2 *>(a.gold)[j];
-            if constexpr (PAIR && SELF) d2 = reinterpret_cast<const double2 *>(a.d)[j];
-            TS s0[KK], y0[KK], s1[KK], y1[KK];
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const P2 sp = reinterpret_cast<const P2 *>(sv[k])[j], yp = reinterpret_cast<const P2 *>(yv[k])[j];
-                s0[k] = sp.x;
-                s1[k] = sp.y;
-                y0[k] = yp.x;
-                y1[k] = yp.y;
-            }
-            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, g2.x, go2.x, d2.x, acc, s0, y0);
-            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, g2.y, go2.y, d2.y, acc, s1, y1);
+            pair_dots_elem<TS, K, PAIR, SELF>(a.stp, (double)g[e], PAIR ? (double)go[e] : 0.0, PAIR && SELF ? (double)d[e] : 0.0, acc,
+                                              sk, yk);
         }
     }
     block_rows_store<R>(acc, a.part);
@@ -148,15 +161,15 @@ __global__ void __launch_bounds__(kRedThreads) k_pair_dots(PairDotsArgs a) {
 // pair s_n = stp d_old, y_n = g - gold is formed from the d being replaced, rounded to the
 // storage type, stored in snew/ynew and added with coefficients cs_n, cy_n.
 struct DirArgs {
-    const double *g, *gold;
+    const void *g, *gold;  // vector type TV, as d
     double cg, stp, cs_n, cy_n;
     const void *v[2 * kPairGroup];
     double cv[2 * kPairGroup];
     void *snew, *ynew;
-    double *d;
+    void *d;
     int accumulate;
     long long n;
-    const double *x;  // non-null (last launch): also the first trial point xt = x + stp_t d
+    const double *x;  // non-null (last launch): also the first trial point xt = x + stp_t d (FP64)
     double *xt;
     double stp_t;
 };
@@ -179,82 +192,68 @@ __device__ __forceinline__ double direction_elem(const DirArgs &a, double gi, do
     return di;
 }
 
-template <typename TS, int K, bool NEWPAIR, int VEC>
+template <typename TS, typename TV, int K, bool NEWPAIR, int V>
 __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
     constexpr int KK = K > 0 ? K : 1;
     const TS *vv[KK];
 #pragma unroll
     for (int k = 0; k < K; ++k) vv[k] = static_cast<const TS *>(a.v[k]);
     TS *snew = static_cast<TS *>(a.snew), *ynew = static_cast<TS *>(a.ynew);
+    const TV *gp = static_cast<const TV *>(a.g), *gop = static_cast<const TV *>(a.gold);
+    TV *dp = static_cast<TV *>(a.d);
     const long long stride = (long long)gridDim.x * blockDim.x;
     const bool need_g = !a.accumulate || NEWPAIR;
     const bool need_d = a.accumulate || NEWPAIR;
-    if constexpr (VEC == 1) {
-        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
-            TS vk[KK], sn = 0, yn = 0;
+    const long long nv = a.n / V;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += stride) {
+        TV g[V], go[V], d[V];
+        if (need_g) vload<TV, V>(gp, j, g);
+        if constexpr (NEWPAIR) vload<TV, V>(gop, j, go);
+        if (need_d) vload<TV, V>(dp, j, d);
+        TS vc[KK][V];
 #pragma unroll
-            for (int k = 0; k < K; ++k) vk[k] = vv[k][i];
-            const double di = direction_elem<TS, K, NEWPAIR>(a, need_g ? a.g[i] : 0.0, NEWPAIR ? a.gold[i] : 0.0,
-                                                            need_d ? a.d[i] : 0.0, vk, sn, yn);
-            a.d[i] = di;
-            if (a.x) a.xt[i] = trial_elem(a.x[i], di, a.stp_t);
-            if constexpr (NEWPAIR) {
-                snew[i] = sn;
-                ynew[i] = yn;
-            }
+        for (int k = 0; k < K; ++k) vload<TS, V>(vv[k], j, vc[k]);
+        TV r[V];
+        TS sn[V], yn[V];
+        double rd[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            TS vk[KK];
+#pragma unroll
+            for (int k = 0; k < K; ++k) vk[k] = vc[k][e];
+            sn[e] = (TS)0;
+            yn[e] = (TS)0;
+            rd[e] = direction_elem<TS, K, NEWPAIR>(a, need_g ? (double)g[e] : 0.0, NEWPAIR ? (double)go[e] : 0.0,
+                                                   need_d ? (double)d[e] : 0.0, vk, sn[e], yn[e]);
+            r[e] = (TV)rd[e];
         }
-    } else {
-        using P2 = typename Pair2<TS>::t;
-        const long long n2 = a.n / 2;
-        for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += stride) {
-            const double2 g2 = need_g ? reinterpret_cast<const double2 *>(a.g)[j] : make_double2(0.0, 0.0);
-            const double2 go2 = NEWPAIR ? reinterpret_cast<const double2 *>(a.gold)[j] : make_double2(0.0, 0.0);
-            const double2 d2 = need_d ? reinterpret_cast<const double2 *>(a.d)[j] : make_double2(0.0, 0.0);
-            TS v0[KK], v1[KK];
+        vstore<TV, V>(dp, j, r);
+        if (a.x) {
+            double xv[V], xo[V];
+            vload<double, V>(a.x, j, xv);
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const P2 v = reinterpret_cast<const P2 *>(vv[k])[j];
-                v0[k] = v.x;
-                v1[k] = v.y;
-            }
-            TS s0 = 0, y0 = 0, s1 = 0, y1 = 0;
-            double2 r;
-            r.x = direction_elem<TS, K, NEWPAIR>(a, g2.x, go2.x, d2.x, v0, s0, y0);
-            r.y = direction_elem<TS, K, NEWPAIR>(a, g2.y, go2.y, d2.y, v1, s1, y1);
-            reinterpret_cast<double2 *>(a.d)[j] = r;
-            if (a.x) {
-                const double2 xv = reinterpret_cast<const double2 *>(a.x)[j];
-                reinterpret_cast<double2 *>(a.xt)[j] = make_double2(trial_elem(xv.x, r.x, a.stp_t), trial_elem(xv.y, r.y, a.stp_t));
-            }
-            if constexpr (NEWPAIR) {
-                P2 sp, yp;
-                sp.x = s0;
-                sp.y = s1;
-                yp.x = y0;
-                yp.y = y1;
-                reinterpret_cast<P2 *>(snew)[j] = sp;
-                reinterpret_cast<P2 *>(ynew)[j] = yp;
-            }
+            for (int e = 0; e < V; ++e) xo[e] = trial_elem(xv[e], (double)r[e], a.stp_t);
+            vstore<double, V>(a.xt, j, xo);
+        }
+        if constexpr (NEWPAIR) {
+            vstore<TS, V>(snew, j, sn);
+            vstore<TS, V>(ynew, j, yn);
         }
     }
 }
 
-// xt = x + stp d   (lnsrlb: x = z at stp = 1, else stp d + t)
-__global__ void k_trial(double *__restrict__ xt, const double *__restrict__ x, const double *__restrict__ d, double stp,
-                        long long n) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        xt[i] = trial_elem(x[i], d[i], stp);
-}
-
-// the same on element pairs (n even, 16-byte aligned vectors); n2 = n / 2
-__global__ void k_trial2(double *__restrict__ xt, const double *__restrict__ x, const double *__restrict__ d, double stp,
-                         long long n2) {
-    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += (long long)gridDim.x * blockDim.x) {
-        const double2 xv = reinterpret_cast<const double2 *>(x)[j], dv = reinterpret_cast<const double2 *>(d)[j];
-        double2 r;
-        r.x = trial_elem(xv.x, dv.x, stp);
-        r.y = trial_elem(xv.y, dv.y, stp);
-        reinterpret_cast<double2 *>(xt)[j] = r;
+// xt = x + stp d   (lnsrlb: x = z at stp = 1, else stp d + t); d of type TV, V per thread
+template <typename TV, int V>
+__global__ void k_trial(double *__restrict__ xt, const double *__restrict__ x, const TV *__restrict__ d, double stp, long long n) {
+    const long long nv = n / V;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += (long long)gridDim.x * blockDim.x) {
+        double xv[V], xo[V];
+        TV dv[V];
+        vload<double, V>(x, j, xv);
+        vload<TV, V>(d, j, dv);
+#pragma unroll
+        for (int e = 0; e < V; ++e) xo[e] = trial_elem(xv[e], (double)dv[e], stp);
+        vstore<double, V>(xt, j, xo);
     }
 }
 

@@ -343,7 +343,7 @@ void stage_mark(mdft_handle *h, int i) {
 // The excess-term pipeline plus (optionally) the ideal/external term on device
 // arrays, in precision T; leaves {F_id, F_ext, sum_exc, df.dvec, max|df|} in h->sums.
 template <typename T>
-int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const double *dvec) {
+int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const void *dvec, bool vec32) {
     using C = typename Cplx<T>::t;
     const Grid &g = h->g;
     const bool dbl = sizeof(T) == 8;
@@ -396,16 +396,31 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     const int gt_ncol = dbl ? h->gt_ncol64 : h->gt_ncol32;
     auto al16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
     long long red_blocks = h->nblk_gather;
-    if (gt_ncol > 0 && ga.df_mode != 2 && al16(d_xi) && al16(dvec)) {
+    const bool tma_gather = gt_ncol > 0 && ga.df_mode != 2 && al16(d_xi) && al16(dvec);
+    if (vec32 && !tma_gather) {
+        set_error("FP32 gradient vectors need the bulk-copy gather");
+        return MDFT_E_STATE;
+    }
+    if (tma_gather) {
         const int ntiles = (int)(g.N / gt_bm<T>());
         const int grid = std::min(ntiles, h->nsm * (dbl ? 1 : 2));
         const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
-        if (gt_ncol == 1)
-            k_gather_tma<T, 1><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
-        else if (gt_ncol == 2)
-            k_gather_tma<T, 2><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
-        else
-            k_gather_tma<T, 3><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        if (vec32) {
+            float *df32 = reinterpret_cast<float *>(d_df);
+            if (gt_ncol == 1)
+                k_gather_tma<T, 1, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
+            else if (gt_ncol == 2)
+                k_gather_tma<T, 2, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
+            else
+                k_gather_tma<T, 3, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
+        } else {
+            if (gt_ncol == 1)
+                k_gather_tma<T, 1, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+            else if (gt_ncol == 2)
+                k_gather_tma<T, 2, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+            else
+                k_gather_tma<T, 3, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        }
         red_blocks = grid;
     } else if (h->bm_gather == 64)
         k_gather<T, 64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(64, g.np), h->stream>>>(
@@ -420,10 +435,12 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     return check_cuda(cudaGetLastError(), "reduce launch");
 }
 
-// dvec (df_mode 1 only): h_sums[3] = df.dvec, h_sums[4] = max|df| after finish_sums
-int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const double *dvec = nullptr) {
-    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec);
-    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec);
+// dvec (df_mode 1 only): h_sums[3] = df.dvec, h_sums[4] = max|df| after finish_sums.
+// vec32 (bulk-copy gather only): df and dvec are FP32 vectors (the minimiser's mixed solves).
+int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const void *dvec = nullptr,
+                 bool vec32 = false) {
+    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32);
+    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32);
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
@@ -583,9 +600,12 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         h->pt_ok32 = pshape && project_tma_smem_bytes<float>(g.np, g.no) <= dyn_max;
         if ((rc = allow_smem((const void *)k_project_tma<double>, maxsmem))) return rc;
         if ((rc = allow_smem((const void *)k_project_tma<float>, maxsmem))) return rc;
-        const void *fns[] = {(const void *)k_gather_tma<double, 1>, (const void *)k_gather_tma<double, 2>,
-                             (const void *)k_gather_tma<double, 3>, (const void *)k_gather_tma<float, 1>,
-                             (const void *)k_gather_tma<float, 2>,  (const void *)k_gather_tma<float, 3>};
+        const void *fns[] = {(const void *)k_gather_tma<double, 1, double>, (const void *)k_gather_tma<double, 2, double>,
+                             (const void *)k_gather_tma<double, 3, double>, (const void *)k_gather_tma<float, 1, double>,
+                             (const void *)k_gather_tma<float, 2, double>,  (const void *)k_gather_tma<float, 3, double>,
+                             (const void *)k_gather_tma<double, 1, float>,  (const void *)k_gather_tma<double, 2, float>,
+                             (const void *)k_gather_tma<double, 3, float>,  (const void *)k_gather_tma<float, 1, float>,
+                             (const void *)k_gather_tma<float, 2, float>,   (const void *)k_gather_tma<float, 3, float>};
         for (const void *fn : fns)
             if ((rc = allow_smem(fn, maxsmem))) return rc;
     }

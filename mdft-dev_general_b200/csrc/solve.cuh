@@ -13,7 +13,9 @@ inline unsigned vec_grid() { return kRedBlocks; }
 // Evaluation in two halves so that more work can be queued before the synchronise:
 // eval_launch queues the pipeline at x (gradient into g; with dvec also g.dvec and max|g|
 // from the gather pass), eval_finish waits and reads f, g.dvec and max|g|.
-int eval_launch(mdft_handle *h, const double *x, double *g, const double *dvec) { return run_pipeline(h, x, g, 1, 1, dvec); }
+int eval_launch(mdft_handle *h, const double *x, double *g, const void *dvec, bool v32 = false) {
+    return run_pipeline(h, x, g, 1, 1, dvec, v32);
+}
 
 int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
     double fid, fext, fexc;
@@ -30,9 +32,11 @@ int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
     return 0;
 }
 
-// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.
-int eval_fg(mdft_handle *h, const double *x, double *g, const double *dvec, double *f, double *gd, double *gmax) {
-    int rc = eval_launch(h, x, g, dvec);
+// x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.  v32: g and dvec
+// are FP32 vectors (the minimiser's mixed solves).
+int eval_fg(mdft_handle *h, const double *x, double *g, const void *dvec, double *f, double *gd, double *gmax,
+            bool v32 = false) {
+    int rc = eval_launch(h, x, g, dvec, v32);
     if (rc) return rc;
     return eval_finish(h, f, gd, gmax);
 }
@@ -397,7 +401,7 @@ constexpr double kMixedNoiseRel = 1e-6;
 
 struct LbfgsHist {
     int m = 0, col = 0, head = 0;
-    bool low = false;                          // pairs stored in BF16 (mixed solves)
+    bool low = false;  // mixed solves: pairs stored in BF16, gradient and direction vectors in FP32
     double theta = 1.0, gg = 0.0, sty = 0.0;  // sty: s.y of the pair formed last, from the stored values
     std::vector<double> sy, yy, sg, yg;
     void reset(int mm, bool lowp = false) {
@@ -421,21 +425,22 @@ inline void *hist_slot(const LbfgsHist &H, double *base, int j, long long n) {
     return H.low ? (void *)(reinterpret_cast<__nv_bfloat16 *>(base) + (size_t)j * n) : (void *)(base + (size_t)j * n);
 }
 
-template <typename TS, int K, bool PAIR, bool SELF>
+template <typename TS, typename TV, int K, bool PAIR, bool SELF>
 void launch_dots_v(const PairDotsArgs &a, cudaStream_t st) {
-    if (a.n % 2 == 0) k_pair_dots<TS, K, PAIR, SELF, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-    else k_pair_dots<TS, K, PAIR, SELF, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    constexpr int V = 16 / (int)sizeof(TV);
+    if (a.n % V == 0) k_pair_dots<TS, TV, K, PAIR, SELF, V><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    else k_pair_dots<TS, TV, K, PAIR, SELF, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
 }
 template <int K>
 void launch_dots(bool low, bool pair, bool self, const PairDotsArgs &a, cudaStream_t st) {
     if (low) {
-        if (!pair) launch_dots_v<__nv_bfloat16, K, false, false>(a, st);
-        else if (self) launch_dots_v<__nv_bfloat16, K, true, true>(a, st);
-        else launch_dots_v<__nv_bfloat16, K, true, false>(a, st);
+        if (!pair) launch_dots_v<__nv_bfloat16, float, K, false, false>(a, st);
+        else if (self) launch_dots_v<__nv_bfloat16, float, K, true, true>(a, st);
+        else launch_dots_v<__nv_bfloat16, float, K, true, false>(a, st);
     } else {
-        if (!pair) launch_dots_v<double, K, false, false>(a, st);
-        else if (self) launch_dots_v<double, K, true, true>(a, st);
-        else launch_dots_v<double, K, true, false>(a, st);
+        if (!pair) launch_dots_v<double, double, K, false, false>(a, st);
+        else if (self) launch_dots_v<double, double, K, true, true>(a, st);
+        else launch_dots_v<double, double, K, true, false>(a, st);
     }
 }
 
@@ -556,13 +561,12 @@ int history_dots_now(mdft_handle *h, LbfgsHist &H, const double *g) {
 
 template <int K, bool NP>
 void launch_direction_k(bool low, const DirArgs &a, cudaStream_t st) {
-    const bool v2 = a.n % 2 == 0;
     if (low) {
-        if (v2) k_direction<__nv_bfloat16, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<__nv_bfloat16, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        if (a.n % 4 == 0) k_direction<__nv_bfloat16, float, K, NP, 4><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<__nv_bfloat16, float, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     } else {
-        if (v2) k_direction<double, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        if (a.n % 2 == 0) k_direction<double, double, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<double, double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     }
 }
 template <int K>
@@ -584,7 +588,7 @@ struct PendingPair {
 // (R = upper triangle of S'Y, D its diagonal; no history: d = -g/theta).  The slope g.d and
 // d.d come from the Gram data (no synchronise); a pending pair is stored on the way.
 // With x non-null the last launch also writes the first trial point xt = x + stp_t d.
-int direction(mdft_handle *h, const LbfgsHist &H, const double *g, double *d, const PendingPair &pend, double *gd, double *dd,
+int direction(mdft_handle *h, const LbfgsHist &H, const void *g, void *d, const PendingPair &pend, double *gd, double *dd,
               const double *x = nullptr, double *xt = nullptr, double stp_t = 1.0) {
     LbfgsState &L = h->lb;
     const long long n = L.n;
@@ -715,14 +719,15 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     const int m = o->m;
     cudaStream_t st = h->stream;
     if (H.m != m) H.reset(m, H.low);
-    double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;
+    double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;  // gc, gt and L.d hold TV values
+    const bool v32 = H.low;  // mixed solves: FP32 gradient and direction vectors
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
     double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0;
     int iter = 0, nfgv = 0, status = 3;
     const bool fresh = H.col == 0;
     PendingPair pend;
-    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax))) return rc;
+    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32))) return rc;
     nfgv = 1;
     trace_iter(h, xc, 0, nfgv, f, gmax, 0.0);
     double sbgnrm = gmax;
@@ -759,11 +764,17 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 iback = ifun - 1;
                 if (iback >= 20) break;
                 if (ifun > 1) {  // the first trial point came with the direction
-                    if (n % 2 == 0) k_trial2<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n / 2);
-                    else k_trial<<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                    if (v32) {
+                        const float *d32 = reinterpret_cast<const float *>(L.d.p);
+                        if (n % 4 == 0) k_trial<float, 4><<<vec_grid(), 256, 0, st>>>(xt, xc, d32, stp, n);
+                        else k_trial<float, 1><<<vec_grid(), 256, 0, st>>>(xt, xc, d32, stp, n);
+                    } else {
+                        if (n % 2 == 0) k_trial<double, 2><<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                        else k_trial<double, 1><<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                    }
                     h->launches += 1;
                 }
-                if ((rc = eval_launch(h, xt, gt, L.d.p))) return rc;
+                if ((rc = eval_launch(h, xt, gt, L.d.p, v32))) return rc;
                 // the history's products with this trial gradient, queued before the one
                 // synchronise of the step (used if the trial is accepted)
                 if ((rc = launch_history_dots(h, H, gt, gc, L.d.p, stp, P))) return rc;
@@ -838,7 +849,7 @@ done:
         if ((rc = direction(h, H, gc, L.d.p, pend, &gd2, &dd2))) return rc;
     }
     if (xc != L.x.p) cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
-    if (gc != h->df.p) cudaMemcpyAsync(h->df.p, gc, n * 8, cudaMemcpyDeviceToDevice, st);
+    if (gc != h->df.p) cudaMemcpyAsync(h->df.p, gc, n * (v32 ? 4 : 8), cudaMemcpyDeviceToDevice, st);
     if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;
     res->f = f;
     res->pgnorm = sbgnrm;
@@ -861,7 +872,9 @@ int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_resu
     const int saved = h->eval_prec;
     int rc;
     LbfgsHist H;
-    H.reset(o->m, o->precision == MDFT_PREC_MIXED);
+    // BF16 history and FP32 vectors for mixed solves where the bulk-copy gathers (FP32 and, for
+    // the FP64 check and polish, FP64) can take FP32 vectors
+    H.reset(o->m, o->precision == MDFT_PREC_MIXED && h->gt_ncol32 > 0 && h->gt_ncol64 > 0);
     res->evaluations_mixed = 0;
     if (o->precision == MDFT_PREC_MIXED) {
         h->eval_prec = MDFT_PREC_MIXED;
