@@ -59,11 +59,12 @@ __device__ __forceinline__ void loadpw(const double2 *p, double2 (&v)[PW]) {
     for (int k = 0; k < PW; ++k) v[k] = p[k];
 }
 
-// TD: type of df and of the search direction (double, or float for the FP32 L-BFGS vectors)
-template <typename T, int NCOL, typename TD>
+// TD: type of df and of the search direction (double, or float for the FP32 L-BFGS vectors);
+// TX: type of xi and vext (double, or float in the FP32 phase of a mixed solve)
+template <typename T, int NCOL, typename TD, typename TX = double>
 __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_tma(const typename Cplx<T>::t *__restrict__ planes,
-                                                              const T *__restrict__ B, const double *__restrict__ xi,
-                                                              const double *__restrict__ vext, const double *__restrict__ w,
+                                                              const T *__restrict__ B, const TX *__restrict__ xi,
+                                                              const TX *__restrict__ vext, const double *__restrict__ w,
                                                               TD *__restrict__ df, double *__restrict__ partial,
                                                               int *__restrict__ err, GatherArgs a, int ntiles) {
     using C = typename Cplx<T>::t;
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
     unsigned char *stage0 = gt_smem + gt_b_bytes<T>(np, NCOL);
     const size_t sbytes = gt_stage_bytes<T>(np, no);
     const size_t plbytes = (size_t)np * BM * sizeof(C);
-    const size_t fbytes = (size_t)BM * no * sizeof(double);
+    const size_t fbytes = (size_t)BM * no * sizeof(TX);
     __shared__ uint64_t full[kGtStages];
     __shared__ int abort_flag;
     __shared__ double red[kGatherSums][kGtThreads / 32];
@@ -135,8 +136,8 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
         if (ok) {
             const unsigned char *st = stage0 + s * sbytes;
             const C *pl = reinterpret_cast<const C *>(st);
-            const double *xs = reinterpret_cast<const double *>(st + plbytes);
-            const double *vs = xs + (size_t)BM * no;
+            const TX *xs = reinterpret_cast<const TX *>(st + plbytes);
+            const TX *vs = xs + (size_t)BM * no;
             const TD *ds = reinterpret_cast<const TD *>(vs + (size_t)BM * no);
             T acc[PW][NCOL];
 #pragma unroll

@@ -13,7 +13,8 @@
 // (mixed solves: pairs are rounded to BF16 when stored and every product, in FP64, uses the
 // stored values, so the compact matrix stays the exact BFGS matrix of the stored pairs).
 // Gradient and direction vectors TV: double (FP64 solves) or float (mixed solves); the
-// point x is FP64 in both.  A thread takes V consecutive elements per step (16 bytes of TV).
+// point x (TXP): FP64, or FP32 in the FP32 phase of a mixed solve.  A thread takes V
+// consecutive elements per step (16 bytes of TV).
 // Every reduction is two-stage with the fixed grid kRedBlocks and a fixed summation order
 // for a given (grid, VEC), so results are reproducible run to run.
 #pragma once
@@ -169,8 +170,8 @@ struct DirArgs {
     void *d;
     int accumulate;
     long long n;
-    const double *x;  // non-null (last launch): also the first trial point xt = x + stp_t d (FP64)
-    double *xt;
+    const void *x;  // non-null (last launch): also the first trial point xt = x + stp_t d (type TXP)
+    void *xt;
     double stp_t;
 };
 
@@ -192,7 +193,7 @@ __device__ __forceinline__ double direction_elem(const DirArgs &a, double gi, do
     return di;
 }
 
-template <typename TS, typename TV, int K, bool NEWPAIR, int V>
+template <typename TS, typename TV, typename TXP, int K, bool NEWPAIR, int V>
 __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
     constexpr int KK = K > 0 ? K : 1;
     const TS *vv[KK];
@@ -229,11 +230,11 @@ __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
         }
         vstore<TV, V>(dp, j, r);
         if (a.x) {
-            double xv[V], xo[V];
-            vload<double, V>(a.x, j, xv);
+            TXP xv[V], xo[V];
+            vload<TXP, V>(static_cast<const TXP *>(a.x), j, xv);
 #pragma unroll
-            for (int e = 0; e < V; ++e) xo[e] = trial_elem(xv[e], (double)r[e], a.stp_t);
-            vstore<double, V>(a.xt, j, xo);
+            for (int e = 0; e < V; ++e) xo[e] = (TXP)trial_elem((double)xv[e], (double)r[e], a.stp_t);
+            vstore<TXP, V>(static_cast<TXP *>(a.xt), j, xo);
         }
         if constexpr (NEWPAIR) {
             vstore<TS, V>(snew, j, sn);
@@ -243,18 +244,25 @@ __global__ void __launch_bounds__(kRedThreads) k_direction(DirArgs a) {
 }
 
 // xt = x + stp d   (lnsrlb: x = z at stp = 1, else stp d + t); d of type TV, V per thread
-template <typename TV, int V>
-__global__ void k_trial(double *__restrict__ xt, const double *__restrict__ x, const TV *__restrict__ d, double stp, long long n) {
+template <typename TV, typename TXP, int V>
+__global__ void k_trial(TXP *__restrict__ xt, const TXP *__restrict__ x, const TV *__restrict__ d, double stp, long long n) {
     const long long nv = n / V;
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += (long long)gridDim.x * blockDim.x) {
-        double xv[V], xo[V];
+        TXP xv[V], xo[V];
         TV dv[V];
-        vload<double, V>(x, j, xv);
+        vload<TXP, V>(x, j, xv);
         vload<TV, V>(d, j, dv);
 #pragma unroll
-        for (int e = 0; e < V; ++e) xo[e] = trial_elem(xv[e], (double)dv[e], stp);
-        vstore<double, V>(xt, j, xo);
+        for (int e = 0; e < V; ++e) xo[e] = (TXP)trial_elem((double)xv[e], (double)dv[e], stp);
+        vstore<TXP, V>(xt, j, xo);
     }
+}
+
+// out = (TO) in, element-wise (precision changes of whole vectors at phase boundaries)
+template <typename TI, typename TO>
+__global__ void k_convert(TO *__restrict__ out, const TI *__restrict__ in, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (TO)in[i];
 }
 
 // out[r] = sum over blocks of part[r][.] (one block per row, fixed order)

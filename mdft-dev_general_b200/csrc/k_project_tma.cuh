@@ -50,8 +50,9 @@ template <> struct Vec8<double> {
     }
 };
 
-template <typename T>
-__global__ void __launch_bounds__(256, 1) k_project_tma(const double *__restrict__ xi, const T *__restrict__ A,
+// TX: type of xi (double, or float in the FP32 phase of a mixed solve)
+template <typename T, typename TX = double>
+__global__ void __launch_bounds__(256, 1) k_project_tma(const TX *__restrict__ xi, const T *__restrict__ A,
                                                         typename Cplx<T>::t *__restrict__ planes, int *__restrict__ err,
                                                         AngularArgs a, int ntiles) {
     using C = typename Cplx<T>::t;
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(256, 1) k_project_tma(const double *__restrict
     T *As = reinterpret_cast<T *>(pt_smem);  // [no][NC]
     T *dr = reinterpret_cast<T *>(pt_smem + ((size_t)no * NC * sizeof(T) + 15) / 16 * 16);  // [no][kPtLd]
     unsigned char *stage0 = reinterpret_cast<unsigned char *>(dr) + ((size_t)no * kPtLd * sizeof(T) + 15) / 16 * 16;
-    const size_t sbytes = (size_t)kPtBM * no * sizeof(double);
+    const size_t sbytes = (size_t)kPtBM * no * sizeof(TX);
     __shared__ uint64_t full[kPtStages];
     __shared__ int abort_flag;
     const int nmine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -90,10 +91,10 @@ __global__ void __launch_bounds__(256, 1) k_project_tma(const double *__restrict
         const bool ok = mbar_wait(&full[s], (uint32_t)((i / kPtStages) & 1));
         if (!ok) abort_flag = 1;
         if (ok) {
-            const double *xs = reinterpret_cast<const double *>(stage0 + s * sbytes);
+            const TX *xs = reinterpret_cast<const TX *>(stage0 + s * sbytes);
             for (int e = tid; e < kPtBM * no; e += blockDim.x) {
                 const int p = e / no, io = e % no;
-                const double x = xs[e];
+                const double x = (double)xs[e];
                 dr[io * kPtLd + p] = (T)(a.rho0 * (x * x - 1.0));
             }
         }

@@ -64,6 +64,7 @@ struct mdft_handle {
     bool have_vext = false;
     // device state
     DevBuf<double> xi, vext, df, w, A, B, partial, sums;
+    DevBuf<float> vext32;  // FP32 copy of vext for the FP32 phase of mixed solves (made per solve)
     DevBuf<double2> planes, ctab;
     DevBuf<double2> tw64[3];
     // mixed path: FP32 projections, c table, twiddles and angular matrices
@@ -343,8 +344,10 @@ void stage_mark(mdft_handle *h, int i) {
 // The excess-term pipeline plus (optionally) the ideal/external term on device
 // arrays, in precision T; leaves {F_id, F_ext, sum_exc, df.dvec, max|df|} in h->sums.
 template <typename T>
-int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const void *dvec, bool vec32) {
+int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, int df_mode, const void *dvec, bool vec32,
+                   bool x32) {
     using C = typename Cplx<T>::t;
+    const double *d_xi = static_cast<const double *>(xin);  // FP64 point unless x32
     const Grid &g = h->g;
     const bool dbl = sizeof(T) == 8;
     C *planes = dbl ? (C *)h->planes.p : (C *)h->planes32.p;
@@ -355,7 +358,15 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     for (int ax = 0; ax < 3; ++ax) tw[ax] = dbl ? (const void *)h->tw64[ax].p : (const void *)h->tw32[ax].p;
     stage_mark(h, 0);
     AngularArgs aa{g.N, g.no, g.np, g.rho0};
-    if ((dbl ? h->pt_ok64 : h->pt_ok32) && ((uintptr_t)d_xi & 15u) == 0) {
+    if (x32 && (dbl || !h->pt_ok32 || !h->vext32.p || ((uintptr_t)xin & 15u) != 0)) {
+        set_error("an FP32 point needs the FP32 bulk-copy kernels");
+        return MDFT_E_STATE;
+    }
+    if (x32) {
+        const int ntiles = (int)(g.N / kPtBM);
+        k_project_tma<float, float><<<std::min(ntiles, h->nsm), 256, project_tma_smem_bytes<float>(g.np, g.no), h->stream>>>(
+            static_cast<const float *>(xin), (const float *)A, (float2 *)planes, h->kerr.p, aa, ntiles);
+    } else if ((dbl ? h->pt_ok64 : h->pt_ok32) && ((uintptr_t)d_xi & 15u) == 0) {
         const int ntiles = (int)(g.N / kPtBM);
         k_project_tma<T><<<std::min(ntiles, h->nsm), 256, project_tma_smem_bytes<T>(g.np, g.no), h->stream>>>(d_xi, A, planes,
                                                                                                              h->kerr.p, aa, ntiles);
@@ -397,7 +408,7 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
     auto al16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
     long long red_blocks = h->nblk_gather;
     const bool tma_gather = gt_ncol > 0 && ga.df_mode != 2 && al16(d_xi) && al16(dvec);
-    if (vec32 && !tma_gather) {
+    if ((vec32 || x32) && !tma_gather) {
         set_error("FP32 gradient vectors need the bulk-copy gather");
         return MDFT_E_STATE;
     }
@@ -405,7 +416,19 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
         const int ntiles = (int)(g.N / gt_bm<T>());
         const int grid = std::min(ntiles, h->nsm * (dbl ? 1 : 2));
         const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
-        if (vec32) {
+        if (x32) {
+            // FP32 phase of a mixed solve: point, vext, gradient and direction in FP32
+            float *df32 = reinterpret_cast<float *>(d_df);
+            const float *x32p = static_cast<const float *>(xin);
+            const float2 *pl = (const float2 *)planes;
+            const float *B32 = (const float *)B;
+            if (gt_ncol == 1)
+                k_gather_tma<float, 1, float, float><<<grid, kGtThreads, smem, h->stream>>>(pl, B32, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
+            else if (gt_ncol == 2)
+                k_gather_tma<float, 2, float, float><<<grid, kGtThreads, smem, h->stream>>>(pl, B32, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
+            else
+                k_gather_tma<float, 3, float, float><<<grid, kGtThreads, smem, h->stream>>>(pl, B32, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
+        } else if (vec32) {
             float *df32 = reinterpret_cast<float *>(d_df);
             if (gt_ncol == 1)
                 k_gather_tma<T, 1, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
@@ -436,11 +459,12 @@ int run_pipeline_t(mdft_handle *h, const double *d_xi, double *d_df, int do_idea
 }
 
 // dvec (df_mode 1 only): h_sums[3] = df.dvec, h_sums[4] = max|df| after finish_sums.
-// vec32 (bulk-copy gather only): df and dvec are FP32 vectors (the minimiser's mixed solves).
-int run_pipeline(mdft_handle *h, const double *d_xi, double *d_df, int do_ideal, int df_mode, const void *dvec = nullptr,
-                 bool vec32 = false) {
-    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32);
-    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32);
+// vec32 (bulk-copy gather only): df and dvec are FP32 vectors (the minimiser's mixed solves);
+// x32 (FP32 evaluations, with vec32): the point is FP32 too and vext is read from h->vext32.
+int run_pipeline(mdft_handle *h, const void *d_xi, double *d_df, int do_ideal, int df_mode, const void *dvec = nullptr,
+                 bool vec32 = false, bool x32 = false) {
+    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32, x32);
+    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32, x32);
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
@@ -600,12 +624,15 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         h->pt_ok32 = pshape && project_tma_smem_bytes<float>(g.np, g.no) <= dyn_max;
         if ((rc = allow_smem((const void *)k_project_tma<double>, maxsmem))) return rc;
         if ((rc = allow_smem((const void *)k_project_tma<float>, maxsmem))) return rc;
+        if ((rc = allow_smem((const void *)k_project_tma<float, float>, maxsmem))) return rc;
         const void *fns[] = {(const void *)k_gather_tma<double, 1, double>, (const void *)k_gather_tma<double, 2, double>,
                              (const void *)k_gather_tma<double, 3, double>, (const void *)k_gather_tma<float, 1, double>,
                              (const void *)k_gather_tma<float, 2, double>,  (const void *)k_gather_tma<float, 3, double>,
                              (const void *)k_gather_tma<double, 1, float>,  (const void *)k_gather_tma<double, 2, float>,
                              (const void *)k_gather_tma<double, 3, float>,  (const void *)k_gather_tma<float, 1, float>,
-                             (const void *)k_gather_tma<float, 2, float>,   (const void *)k_gather_tma<float, 3, float>};
+                             (const void *)k_gather_tma<float, 2, float>,   (const void *)k_gather_tma<float, 3, float>,
+                             (const void *)k_gather_tma<float, 1, float, float>, (const void *)k_gather_tma<float, 2, float, float>,
+                             (const void *)k_gather_tma<float, 3, float, float>};
         for (const void *fn : fns)
             if ((rc = allow_smem(fn, maxsmem))) return rc;
     }
@@ -673,7 +700,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
 int mdft_destroy(mdft_handle *h) {
     if (!h) return MDFT_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    h->xi.free(); h->vext.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
+    h->xi.free(); h->vext.free(); h->vext32.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
     h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free(); h->oz_ints.free(); h->oz_dbls.free();
     for (int i = 0; i < 3; ++i) {
         h->tw64[i].free();

@@ -13,8 +13,8 @@ inline unsigned vec_grid() { return kRedBlocks; }
 // Evaluation in two halves so that more work can be queued before the synchronise:
 // eval_launch queues the pipeline at x (gradient into g; with dvec also g.dvec and max|g|
 // from the gather pass), eval_finish waits and reads f, g.dvec and max|g|.
-int eval_launch(mdft_handle *h, const double *x, double *g, const void *dvec, bool v32 = false) {
-    return run_pipeline(h, x, g, 1, 1, dvec, v32);
+int eval_launch(mdft_handle *h, const void *x, double *g, const void *dvec, bool v32 = false, bool x32 = false) {
+    return run_pipeline(h, x, g, 1, 1, dvec, v32, x32);
 }
 
 int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
@@ -34,9 +34,9 @@ int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
 
 // x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.  v32: g and dvec
 // are FP32 vectors (the minimiser's mixed solves).
-int eval_fg(mdft_handle *h, const double *x, double *g, const void *dvec, double *f, double *gd, double *gmax,
-            bool v32 = false) {
-    int rc = eval_launch(h, x, g, dvec, v32);
+int eval_fg(mdft_handle *h, const void *x, double *g, const void *dvec, double *f, double *gd, double *gmax,
+            bool v32 = false, bool x32 = false) {
+    int rc = eval_launch(h, x, g, dvec, v32, x32);
     if (rc) return rc;
     return eval_finish(h, f, gd, gmax);
 }
@@ -560,19 +560,22 @@ int history_dots_now(mdft_handle *h, LbfgsHist &H, const double *g) {
 }
 
 template <int K, bool NP>
-void launch_direction_k(bool low, const DirArgs &a, cudaStream_t st) {
-    if (low) {
-        if (a.n % 4 == 0) k_direction<__nv_bfloat16, float, K, NP, 4><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<__nv_bfloat16, float, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+void launch_direction_k(bool low, bool x32, const DirArgs &a, cudaStream_t st) {
+    if (low && x32) {
+        if (a.n % 4 == 0) k_direction<__nv_bfloat16, float, float, K, NP, 4><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<__nv_bfloat16, float, float, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+    } else if (low) {
+        if (a.n % 4 == 0) k_direction<__nv_bfloat16, float, double, K, NP, 4><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<__nv_bfloat16, float, double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     } else {
-        if (a.n % 2 == 0) k_direction<double, double, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
-        else k_direction<double, double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        if (a.n % 2 == 0) k_direction<double, double, double, K, NP, 2><<<vec_grid(), kRedThreads, 0, st>>>(a);
+        else k_direction<double, double, double, K, NP, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
     }
 }
 template <int K>
-void launch_direction(bool low, bool np, const DirArgs &a, cudaStream_t st) {
-    if (np) launch_direction_k<K, true>(low, a, st);
-    else launch_direction_k<K, false>(low, a, st);
+void launch_direction(bool low, bool x32, bool np, const DirArgs &a, cudaStream_t st) {
+    if (np) launch_direction_k<K, true>(low, x32, a, st);
+    else launch_direction_k<K, false>(low, x32, a, st);
 }
 
 // Pair accepted in the last step and not yet stored: k_direction forms it from the
@@ -588,8 +591,9 @@ struct PendingPair {
 // (R = upper triangle of S'Y, D its diagonal; no history: d = -g/theta).  The slope g.d and
 // d.d come from the Gram data (no synchronise); a pending pair is stored on the way.
 // With x non-null the last launch also writes the first trial point xt = x + stp_t d.
+// x, xt: FP32 when x32 (the FP32 phase of a mixed solve), else FP64.
 int direction(mdft_handle *h, const LbfgsHist &H, const void *g, void *d, const PendingPair &pend, double *gd, double *dd,
-              const double *x = nullptr, double *xt = nullptr, double stp_t = 1.0) {
+              const void *x = nullptr, void *xt = nullptr, double stp_t = 1.0, bool x32 = false) {
     LbfgsState &L = h->lb;
     const long long n = L.n;
     const int k = H.col, m = H.m;
@@ -668,15 +672,15 @@ int direction(mdft_handle *h, const LbfgsHist &H, const void *g, void *d, const 
             a.stp_t = stp_t;
         }
         switch (K) {
-            case 0: launch_direction<0>(H.low, np, a, st); break;
-            case 2: launch_direction<2>(H.low, np, a, st); break;
-            case 4: launch_direction<4>(H.low, np, a, st); break;
-            case 6: launch_direction<6>(H.low, np, a, st); break;
-            case 8: launch_direction<8>(H.low, np, a, st); break;
-            case 10: launch_direction<10>(H.low, np, a, st); break;
-            case 12: launch_direction<12>(H.low, np, a, st); break;
-            case 14: launch_direction<14>(H.low, np, a, st); break;
-            default: launch_direction<16>(H.low, np, a, st); break;
+            case 0: launch_direction<0>(H.low, x32, np, a, st); break;
+            case 2: launch_direction<2>(H.low, x32, np, a, st); break;
+            case 4: launch_direction<4>(H.low, x32, np, a, st); break;
+            case 6: launch_direction<6>(H.low, x32, np, a, st); break;
+            case 8: launch_direction<8>(H.low, x32, np, a, st); break;
+            case 10: launch_direction<10>(H.low, x32, np, a, st); break;
+            case 12: launch_direction<12>(H.low, x32, np, a, st); break;
+            case 14: launch_direction<14>(H.low, x32, np, a, st); break;
+            default: launch_direction<16>(H.low, x32, np, a, st); break;
         }
         h->launches += 1;
     }
@@ -694,6 +698,11 @@ int direction(mdft_handle *h, const LbfgsHist &H, const void *g, void *d, const 
 void trace_iter(mdft_handle *h, const double *x, int iter, int nfgv, double f, double gmax, double stp) {
     if (!h->trace) return;
     const Grid &g = h->g;
+    if (!x) {  // FP32 point: no dN
+        std::fprintf(stderr, "mdft-trace it %d nfg %d prec %s f %.15e gmax %.6e stp %.6e dN nan\n", iter, nfgv,
+                     h->eval_prec == MDFT_PREC_MIXED ? "mixed" : "fp64", f, gmax, stp);
+        return;
+    }
     k_density_sum<<<vec_grid(), 256, 0, h->stream>>>(x, h->w.p, g.no, (long long)h->lb.n, g.rho0, h->vpart.p);
     k_finish_dot_max<<<1, 256, 0, h->stream>>>(h->vpart.p, vec_grid(), h->vsc.p, 4);
     cudaMemcpyAsync(h->h_vsc + 4, h->vsc.p + 4, 8, cudaMemcpyDeviceToHost, h->stream);
@@ -721,15 +730,23 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     if (H.m != m) H.reset(m, H.low);
     double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;  // gc, gt and L.d hold TV values
     const bool v32 = H.low;  // mixed solves: FP32 gradient and direction vectors
+    // FP32 phase of a mixed solve: the point too is FP32 (xc, xt then hold floats); the FP64
+    // start point in L.x is converted into L.t first, and the result back into L.x at the end
+    const bool x32 = v32 && h->eval_prec == MDFT_PREC_MIXED && h->pt_ok32 && h->gt_ncol32 > 0 && h->vext32.p;
+    if (x32) {
+        k_convert<double, float><<<vec_grid(), 256, 0, st>>>(reinterpret_cast<float *>(L.t.p), L.x.p, n);
+        h->launches += 1;
+        std::swap(xc, xt);
+    }
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
     double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0;
     int iter = 0, nfgv = 0, status = 3;
     const bool fresh = H.col == 0;
     PendingPair pend;
-    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32))) return rc;
+    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32, x32))) return rc;
     nfgv = 1;
-    trace_iter(h, xc, 0, nfgv, f, gmax, 0.0);
+    trace_iter(h, x32 ? nullptr : xc, 0, nfgv, f, gmax, 0.0);
     double sbgnrm = gmax;
     if (sbgnrm <= o->pgtol) { status = 0; goto done; }
     if ((rc = history_dots_now(h, H, gc))) return rc;  // s_i.g, y_i.g, g.g at the start point
@@ -739,7 +756,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         // lnsrlb's first step: 1/|d| on the first iteration from an empty history, where
         // d = -g/theta and |d|^2 = g.g/theta^2, else 1
         stp = (iter == 0 && fresh) ? std::min(1.0 / std::sqrt(H.gg / (H.theta * H.theta)), stpmx) : 1.0;
-        if ((rc = direction(h, H, gc, L.d.p, pend, &gd, &dd, xc, xt, stp))) return rc;
+        if ((rc = direction(h, H, gc, L.d.p, pend, &gd, &dd, xc, xt, stp, x32))) return rc;
         pend = PendingPair();
         // ---- line search (lnsrlb) ----
         fold = f;
@@ -764,17 +781,23 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 iback = ifun - 1;
                 if (iback >= 20) break;
                 if (ifun > 1) {  // the first trial point came with the direction
-                    if (v32) {
+                    if (x32) {
                         const float *d32 = reinterpret_cast<const float *>(L.d.p);
-                        if (n % 4 == 0) k_trial<float, 4><<<vec_grid(), 256, 0, st>>>(xt, xc, d32, stp, n);
-                        else k_trial<float, 1><<<vec_grid(), 256, 0, st>>>(xt, xc, d32, stp, n);
+                        float *xt32 = reinterpret_cast<float *>(xt);
+                        const float *xc32 = reinterpret_cast<const float *>(xc);
+                        if (n % 4 == 0) k_trial<float, float, 4><<<vec_grid(), 256, 0, st>>>(xt32, xc32, d32, stp, n);
+                        else k_trial<float, float, 1><<<vec_grid(), 256, 0, st>>>(xt32, xc32, d32, stp, n);
+                    } else if (v32) {
+                        const float *d32 = reinterpret_cast<const float *>(L.d.p);
+                        if (n % 4 == 0) k_trial<float, double, 4><<<vec_grid(), 256, 0, st>>>(xt, xc, d32, stp, n);
+                        else k_trial<float, double, 1><<<vec_grid(), 256, 0, st>>>(xt, xc, d32, stp, n);
                     } else {
-                        if (n % 2 == 0) k_trial<double, 2><<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
-                        else k_trial<double, 1><<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                        if (n % 2 == 0) k_trial<double, double, 2><<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
+                        else k_trial<double, double, 1><<<vec_grid(), 256, 0, st>>>(xt, xc, L.d.p, stp, n);
                     }
                     h->launches += 1;
                 }
-                if ((rc = eval_launch(h, xt, gt, L.d.p, v32))) return rc;
+                if ((rc = eval_launch(h, xt, gt, L.d.p, v32, x32))) return rc;
                 // the history's products with this trial gradient, queued before the one
                 // synchronise of the step (used if the trial is accepted)
                 if ((rc = launch_history_dots(h, H, gt, gc, L.d.p, stp, P))) return rc;
@@ -812,7 +835,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         std::swap(gc, gt);
         gmax = gmax_t;
         sbgnrm = gmax;
-        trace_iter(h, xc, iter, nfgv, f, gmax, stp);
+        trace_iter(h, x32 ? nullptr : xc, iter, nfgv, f, gmax, stp);
         if (sbgnrm <= o->pgtol) { status = 0; goto done; }
         if ((fold - f) <= o->ftol_abs) { status = 1; goto done; }
         // ---- BFGS update (matupd) ----
@@ -848,7 +871,19 @@ done:
         double gd2, dd2;
         if ((rc = direction(h, H, gc, L.d.p, pend, &gd2, &dd2))) return rc;
     }
-    if (xc != L.x.p) cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
+    if (x32) {
+        // the FP32 point back to FP64 in L.x (through L.t when it sits in L.x's storage)
+        const float *x32p = reinterpret_cast<const float *>(xc);
+        if (xc == L.t.p) {
+            k_convert<float, double><<<vec_grid(), 256, 0, st>>>(L.x.p, x32p, n);
+        } else {
+            k_convert<float, double><<<vec_grid(), 256, 0, st>>>(L.t.p, x32p, n);
+            cudaMemcpyAsync(L.x.p, L.t.p, n * 8, cudaMemcpyDeviceToDevice, st);
+        }
+        h->launches += 1;
+    } else if (xc != L.x.p) {
+        cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
+    }
     if (gc != h->df.p) cudaMemcpyAsync(h->df.p, gc, n * (v32 ? 4 : 8), cudaMemcpyDeviceToDevice, st);
     if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;
     res->f = f;
@@ -877,6 +912,13 @@ int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_resu
     H.reset(o->m, o->precision == MDFT_PREC_MIXED && h->gt_ncol32 > 0 && h->gt_ncol64 > 0);
     res->evaluations_mixed = 0;
     if (o->precision == MDFT_PREC_MIXED) {
+        if (H.low && h->pt_ok32) {
+            // FP32 copy of vext for the FP32 phase (vext does not change during the solve)
+            const size_t nf = (size_t)h->g.N * h->g.no;
+            if (!h->vext32.p && (rc = alloc_check(h->vext32.alloc(nf), "FP32 vext", nf * 4))) return rc;
+            k_convert<double, float><<<vec_grid(), 256, 0, h->stream>>>(h->vext32.p, h->vext.p, (long long)nf);
+            h->launches += 1;
+        }
         h->eval_prec = MDFT_PREC_MIXED;
         mdft_minimize_opts o1 = *o;
         if (o->pgtol_mixed > 0) o1.pgtol = o->pgtol_mixed;
