@@ -24,11 +24,11 @@ constexpr int kPtStages = 2;
 constexpr int kPtLd = kPtBM + 1;  // padded row of the transposed tile
 
 inline int pt_warps(int np) { return (np + 3) / 4; }
-template <typename T>
+template <typename T, typename TX = double>
 inline size_t project_tma_smem_bytes(int np, int no) {
     const size_t a = (size_t)no * 8 * pt_warps(np) * sizeof(T);
     const size_t dr = ((size_t)no * kPtLd * sizeof(T) + 15) / 16 * 16;
-    const size_t st = (size_t)kPtBM * no * sizeof(double);
+    const size_t st = (size_t)kPtBM * no * sizeof(TX);
     return (a + 15) / 16 * 16 + dr + kPtStages * st;
 }
 
@@ -52,7 +52,7 @@ template <> struct Vec8<double> {
 
 // TX: type of xi (double, or float in the FP32 phase of a mixed solve)
 template <typename T, typename TX = double>
-__global__ void __launch_bounds__(256, 1) k_project_tma(const TX *__restrict__ xi, const T *__restrict__ A,
+__global__ void __launch_bounds__(256, sizeof(TX) == 4 ? 2 : 1) k_project_tma(const TX *__restrict__ xi, const T *__restrict__ A,
                                                         typename Cplx<T>::t *__restrict__ planes, int *__restrict__ err,
                                                         AngularArgs a, int ntiles) {
     using C = typename Cplx<T>::t;

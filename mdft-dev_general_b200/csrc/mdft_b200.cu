@@ -77,6 +77,7 @@ struct mdft_handle {
     int nsm = 148;
     int gt_ncol64 = 0, gt_ncol32 = 0;  // k_gather_tma columns of 32 per precision (0: not usable)
     bool pt_ok64 = false, pt_ok32 = false;  // k_project_tma usable per precision
+    int pt_grid_x32 = 0;                    // resident CTAs of k_project_tma<float, float>
     int xy_grid_cap64 = 0, xy_grid_cap32 = 0;  // CTAs of the persistent xy FFT (resident count)
     DevBuf<int> kerr;                  // set by a pipeline kernel whose bounded wait ran out
     int *h_kerr = nullptr;
@@ -364,7 +365,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     }
     if (x32) {
         const int ntiles = (int)(g.N / kPtBM);
-        k_project_tma<float, float><<<std::min(ntiles, h->nsm), 256, project_tma_smem_bytes<float>(g.np, g.no), h->stream>>>(
+        k_project_tma<float, float><<<std::min(ntiles, h->pt_grid_x32), 256, project_tma_smem_bytes<float, float>(g.np, g.no), h->stream>>>(
             static_cast<const float *>(xin), (const float *)A, (float2 *)planes, h->kerr.p, aa, ntiles);
     } else if ((dbl ? h->pt_ok64 : h->pt_ok32) && ((uintptr_t)d_xi & 15u) == 0) {
         const int ntiles = (int)(g.N / kPtBM);
@@ -625,6 +626,12 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         if ((rc = allow_smem((const void *)k_project_tma<double>, maxsmem))) return rc;
         if ((rc = allow_smem((const void *)k_project_tma<float>, maxsmem))) return rc;
         if ((rc = allow_smem((const void *)k_project_tma<float, float>, maxsmem))) return rc;
+        {
+            int b = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_project_tma<float, float>, 256,
+                                                          project_tma_smem_bytes<float, float>(g.np, g.no));
+            h->pt_grid_x32 = h->nsm * std::max(1, b);
+        }
         const void *fns[] = {(const void *)k_gather_tma<double, 1, double>, (const void *)k_gather_tma<double, 2, double>,
                              (const void *)k_gather_tma<double, 3, double>, (const void *)k_gather_tma<float, 1, double>,
                              (const void *)k_gather_tma<float, 2, double>,  (const void *)k_gather_tma<float, 3, double>,

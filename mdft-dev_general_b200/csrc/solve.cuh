@@ -427,7 +427,8 @@ inline void *hist_slot(const LbfgsHist &H, double *base, int j, long long n) {
 
 template <typename TS, typename TV, int K, bool PAIR, bool SELF>
 void launch_dots_v(const PairDotsArgs &a, cudaStream_t st) {
-    constexpr int V = 16 / (int)sizeof(TV);
+    // 16-byte accesses of the narrower of the vector and history types (8 FP32/BF16 elements)
+    constexpr int V = 16 / (int)(sizeof(TS) < sizeof(TV) ? sizeof(TS) : sizeof(TV));
     if (a.n % V == 0) k_pair_dots<TS, TV, K, PAIR, SELF, V><<<vec_grid(), kRedThreads, 0, st>>>(a);
     else k_pair_dots<TS, TV, K, PAIR, SELF, 1><<<vec_grid(), kRedThreads, 0, st>>>(a);
 }
