@@ -83,7 +83,7 @@ __device__ __forceinline__ void ozp_fmac(float2 &acc, float2 a, float2 b) {  // 
 
 template <int MM, int MR>
 __global__ void __launch_bounds__(kOzpThreads) k_ozp(float2 *__restrict__ planes, const float2 *__restrict__ ctab, Oz2Args a,
-                                                     OzpParams pp) {
+                                                     OzpParams pp, const float2 *__restrict__ cq) {
     using S = OzShape<MM, MR>;
     constexpr int NP = S::np();
     constexpr int NH = S::nhalf() > 0 ? S::nhalf() : 1;
@@ -204,12 +204,19 @@ __global__ void __launch_bounds__(kOzpThreads) k_ozp(float2 *__restrict__ planes
         }
 
     // ---- interpolated c (:534-539) and the OZ sums (:561-606), one chi block at a time ----
+    // cq (cubic grid in a cubic box): c already interpolated at every |q|^2 = (2 pi/L)^2 s2 of
+    // the grid, row s2; otherwise the two bracketing rows of the table and their weight
     const double nrm = sqrt(qx * qx + qy * qy + qz * qz);
     const double eff = nrm / a.dq + 1.0;
     const int iq = (int)eff;
     const float alpha = (float)(eff - iq);
     const float2 *c0 = ctab + (size_t)(iq - 1) * a.ncoef;
     const float2 *c1 = ctab + (size_t)iq * a.ncoef;
+    const float2 *crow = nullptr;
+    if (cq) {
+        const int sx = ix <= a.nx / 2 ? ix : ix - a.nx, sy = iy <= a.ny / 2 ? iy : iy - a.ny, sz = iz <= a.nz / 2 ? iz : iz - a.nz;
+        crow = cq + (size_t)(sx * sx + sy * sy + sz * sz) * a.ncoef;
+    }
 #pragma unroll
     for (int khi = -MM; khi <= MM; ++khi) {
         constexpr int BMAX = 2 * (MM / MR + 1) * (MM + 1);
@@ -227,10 +234,14 @@ __global__ void __launch_bounds__(kOzpThreads) k_ozp(float2 *__restrict__ planes
 #pragma unroll
                     for (int nu2 = -n / MR; nu2 <= n / MR; ++nu2, ++k) {
                         const int ia = pp.ia0[ip] + k;
-                        const float2 A0 = c0[ia], A1 = c1[ia];
                         float2 ce;
-                        ce.x = alpha * A1.x + (1.f - alpha) * A0.x;
-                        ce.y = alpha * A1.y + (1.f - alpha) * A0.y;
+                        if (crow) {
+                            ce = crow[ia];
+                        } else {
+                            const float2 A0 = c0[ia], A1 = c1[ia];
+                            ce.x = alpha * A1.x + (1.f - alpha) * A0.x;
+                            ce.y = alpha * A1.y + (1.f - alpha) * A0.y;
+                        }
                         const int jp = S::pidx(n, khi, nu2 < 0 ? -nu2 : nu2);
                         if (nu2 < 0) {
                             ozp_fma(s, ce, sq[jp * B]);
@@ -288,6 +299,28 @@ __global__ void __launch_bounds__(kOzpThreads) k_ozp(float2 *__restrict__ planes
 }
 
 inline size_t ozp_smem_bytes(int np) { return sizeof(float2) * 2 * (size_t)np * kOzpThreads; }
+
+// c(|q|) interpolated on the host at every |q|^2 of a cubic grid in a cubic box (s2 = 0 ..
+// 3 (n/2)^2, |q| = 2 pi/L sqrt(s2)), with the kernel's interpolation rule; empty otherwise.
+inline std::vector<float2> build_ozp_cq(const Grid &g, const CTable &ct, const std::vector<float2> &c32) {
+    std::vector<float2> t;
+    if (!(g.nx == g.ny && g.ny == g.nz && g.lx == g.ly && g.ly == g.lz)) return t;
+    const int h = g.nx / 2, rows = 3 * h * h + 1, nc = ct.ncoef;
+    const double tp = 2.0 * kPi / g.lx;
+    t.resize((size_t)rows * nc);
+    for (int s2 = 0; s2 < rows; ++s2) {
+        const double nrm = std::sqrt((double)s2) * tp;
+        const double eff = nrm / ct.dq + 1.0;
+        const int iq = (int)eff;
+        if (iq < 1 || iq >= ct.nq) return std::vector<float2>();
+        const float alpha = (float)(eff - iq);
+        for (int i = 0; i < nc; ++i) {
+            const float2 A = c32[(size_t)(iq - 1) * nc + i], B = c32[(size_t)iq * nc + i];
+            t[(size_t)s2 * nc + i] = make_float2(alpha * B.x + (1.f - alpha) * A.x, alpha * B.y + (1.f - alpha) * A.y);
+        }
+    }
+    return t;
+}
 
 // Host: parameters of k_ozp for this grid and c table; false when the shape is not covered
 // (then k_oz2<float> runs).  The coefficients and term order mirror build_oz_tables.

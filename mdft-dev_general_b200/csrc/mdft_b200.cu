@@ -88,6 +88,7 @@ struct mdft_handle {
     int oz_grid = 0, oz_warps = 8, oz_grid32 = 0, oz_warps32 = 8;
     bool ozp_ok = false;  // FP32 evaluations use the thread-per-pair k_ozp
     OzpParams ozp{};
+    DevBuf<float2> ozp_cq;  // c interpolated at every |q|^2 of a cubic grid (empty: interpolate per pair)
     size_t oz_smem = 0, oz_smem32 = 0;
     // timing
     bool timing = false;
@@ -334,7 +335,8 @@ void launch_ozp(mdft_handle *h, float2 *planes, const float2 *ctab, const Oz2Arg
     const Grid &g = h->g;
     const unsigned grid = (unsigned)((oz.nk + kOzpThreads - 1) / kOzpThreads);
     const size_t smem = ozp_smem_bytes(g.np);
-    void *args[] = {(void *)&planes, (void *)&ctab, (void *)&oz, (void *)&h->ozp};
+    const float2 *cq = h->ozp_cq.p;
+    void *args[] = {(void *)&planes, (void *)&ctab, (void *)&oz, (void *)&h->ozp, (void *)&cq};
     cudaLaunchKernel(ozp_kernel(g.mmax, g.mrso), dim3(grid), dim3(kOzpThreads), args, smem, h->stream);
 }
 
@@ -696,6 +698,13 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         if (fn && build_ozp_params(g, h->ct, h->ozp) && ozp_smem_bytes(g.np) <= dyn_max) {
             if ((rc = allow_smem(fn, maxsmem))) return rc;
             h->ozp_ok = true;
+            std::vector<float2> c32(h->ct.c.size() / 2);  // the FP32 table as the kernels read it
+            for (size_t i = 0; i < c32.size(); ++i) c32[i] = make_float2((float)h->ct.c[2 * i], (float)h->ct.c[2 * i + 1]);
+            std::vector<float2> cq = build_ozp_cq(g, h->ct, c32);
+            if (!cq.empty()) {
+                if ((rc = alloc_check(h->ozp_cq.alloc(cq.size()), "OZ c rows", cq.size() * 8))) return rc;
+                cudaMemcpy(h->ozp_cq.p, cq.data(), cq.size() * 8, cudaMemcpyHostToDevice);
+            }
         }
     }
     h->eval_prec = h->precision;
@@ -707,6 +716,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
 int mdft_destroy(mdft_handle *h) {
     if (!h) return MDFT_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    h->ozp_cq.free();
     h->xi.free(); h->vext.free(); h->vext32.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
     h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free(); h->oz_ints.free(); h->oz_dbls.free();
     for (int i = 0; i < 3; ++i) {
