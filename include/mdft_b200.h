@@ -226,6 +226,65 @@ int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const 
 /* Number of kernels this handle has launched since creation. */
 int mdft_get_launch_count(const mdft_handle *h, long long *count);
 
+/* ---- Learned warm start (no counterpart in the reference, whose solves always start
+ * from guess_density, src/module_density.f90:267-284) ----
+ *
+ * A periodic 3-D convolutional encoder-decoder (4 levels, 16-128 channels, GELU,
+ * 906,772 parameters; BF16 weights, FP32 activations and accumulation) maps 3 input
+ * channels of a solute on the solver's grid -- Lennard-Jones energy, electrostatic
+ * potential, Gaussian site density -- to the 4 m <= 1 projections of the converged
+ * log-density ln(rho/rho0) in the real basis {1, u_x, u_y, u_z} (u: molecular z axis).
+ * Device arrays are [channel][point], points in xi's order without io.  Grid
+ * dimensions must be multiples of 8.  One network object serves one handle (it holds
+ * the activation buffers and runs on one stream). */
+typedef struct mdft_warm_net mdft_warm_net;
+
+int mdft_warm_net_create(int nx, int ny, int nz, int device, mdft_warm_net **out);
+int mdft_warm_net_destroy(mdft_warm_net *net);
+int mdft_warm_net_num_params(const mdft_warm_net *net, long long *n);
+/* He-normal weights from a seed (splitmix64 + Box-Muller), zero biases, head scaled 0.1. */
+int mdft_warm_net_init(mdft_warm_net *net, unsigned long long seed);
+/* FP32 master parameters (host arrays of num_params values); set resets Adam's moments. */
+int mdft_warm_net_set_params(mdft_warm_net *net, const float *params, long long n);
+int mdft_warm_net_get_params(const mdft_warm_net *net, float *params, long long n);
+/* Run on this CUDA stream (NULL: the network's own stream). */
+int mdft_warm_net_set_stream(mdft_warm_net *net, void *stream);
+/* d_in: 3 x N channels; d_out (may be NULL): 4 x N projections; queued, not synchronised. */
+int mdft_warm_net_forward(mdft_warm_net *net, const float *d_in, float *d_out);
+/* Device address of the last forward's output (4 x N), valid until the next call. */
+int mdft_warm_net_output(mdft_warm_net *net, const float **d_out);
+/* Masked squared-error loss sum_v mask_v sum_c (y - t)^2 / (4 N) of one sample and its
+ * gradient with respect to every parameter (host array of num_params FP32 values). */
+int mdft_warm_net_gradients(mdft_warm_net *net, const float *d_in, const float *d_target, const float *d_mask, float *grad,
+                            double *loss);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on the mean gradient of nbatch samples
+ * (device pointer arrays; d_mask may be NULL).  Queued, not synchronised. */
+int mdft_warm_net_train_step(mdft_warm_net *net, const float *const *d_in, const float *const *d_target,
+                             const float *const *d_mask, int nbatch, float lr);
+/* Mean loss per sample of the training steps since the last call (synchronises). */
+int mdft_warm_net_take_loss(mdft_warm_net *net, double *mean_loss);
+int mdft_warm_net_launch_count(const mdft_warm_net *net, long long *count);
+int mdft_warm_net_grid(const mdft_warm_net *net, int *nxyz);
+
+/* The network's 3 input channels for a solute on h's grid (sites as in mdft_solve). */
+int mdft_warm_features(mdft_handle *h, int nsite, const double *q, const double *sig, const double *eps, const double *xyz,
+                       int nsolvsite, const double *sq, const double *ssig, const double *seps, const double *sxyz,
+                       double rvdw, float *d_feat);
+/* Training target (4 x N) and loss mask (N, may be NULL) from a converged density d_xi
+ * (device; NULL: the handle's last solve) with the handle's vext. */
+int mdft_warm_target(mdft_handle *h, const double *d_xi, float *d_target, float *d_mask);
+/* Starting density from 4 x N projections (d_xi device; NULL: the handle's solver point). */
+int mdft_warm_expand(mdft_handle *h, const float *d_pred, double *d_xi);
+/* Make mdft_solve (and mdft_solve_batch on this handle) start from the network's
+ * prediction instead of guess_density; NULL restores the bulk guess.  A warm-started
+ * solve that ends in a line-search failure or at the iteration limit is redone from the
+ * bulk guess.  The network must be built for the handle's grid; while attached it runs on
+ * the handle's stream (detaching, or mdft_destroy of the handle, returns it to its own).
+ * Detach a network before destroying it. */
+int mdft_set_warm_net(mdft_handle *h, mdft_warm_net *net);
+/* stats[0]: warm-started solves, stats[1]: of which redone from the bulk guess. */
+int mdft_get_warm_stats(const mdft_handle *h, long long *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,13 @@ struct mdft_handle {
     double *h_vsc = nullptr;
     // minimiser work (allocated on first use)
     LbfgsState lb;
+    // learned warm start (mdft_set_warm_net): the network, its input channels, the
+    // orientation table {u_x, u_y, u_z, w} and the solute sites, allocated on first use
+    mdft_warm_net *warm = nullptr;
+    DevBuf<float> wfeat;
+    DevBuf<double4> wdir;
+    DevBuf<double> wsite;
+    long long warm_starts = 0, warm_fallbacks = 0;
 };
 
 namespace {
@@ -716,6 +723,9 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
 int mdft_destroy(mdft_handle *h) {
     if (!h) return MDFT_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    // an attached warm-start network goes back to its own stream before this one is destroyed
+    if (h->warm) mdft_warm_net_set_stream(h->warm, nullptr);
+    h->warm = nullptr;
     h->ozp_cq.free();
     h->xi.free(); h->vext.free(); h->vext32.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
     h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free(); h->oz_ints.free(); h->oz_dbls.free();

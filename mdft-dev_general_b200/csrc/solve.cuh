@@ -984,6 +984,8 @@ int mdft_guess_density_device(mdft_handle *h, double *d_xi) {
 
 }  // extern "C"
 
+#include "warmstart.cuh"
+
 namespace {
 
 // d_xi device; h->xi is overwritten (it holds the empty box afterwards)
@@ -1072,10 +1074,28 @@ int mdft_solve(mdft_handle *h, int nsite, const double *q, const double *sig, co
     if ((rc = lbfgs_alloc(h, o->m))) return rc;
     LbfgsState &L = h->lb;
     const double vmax = (-std::log(kEpsDp) - (double)0.05f) * h->g.kT;
-    k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, L.x.p, vmax, L.n);
-    h->launches += 1;
-    lap("guess");
+    const bool warm = h->warm != nullptr;
+    if (warm) {
+        if ((rc = warm_start_impl(h, nsite, q, sig, eps, xyz, nsv, ssig, seps, rvdw, L.x.p))) return rc;
+        h->warm_starts += 1;
+    } else {
+        k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, L.x.p, vmax, L.n);
+        h->launches += 1;
+    }
+    lap(warm ? "warm start" : "guess");
     if ((rc = solve_phases(h, o, res))) return rc;
+    // a warm-started solve that stops without meeting its tests (line-search failure or the
+    // iteration limit) is redone from the bulk guess; the result counts both solves' work
+    if (warm && res->status != 0 && res->status != 1) {
+        mdft_minimize_result r0 = *res;
+        k_guess<<<vec_grid(), 256, 0, h->stream>>>(h->vext.p, L.x.p, vmax, L.n);
+        h->launches += 1;
+        if ((rc = solve_phases(h, o, res))) return rc;
+        res->iterations += r0.iterations;
+        res->evaluations += r0.evaluations;
+        res->evaluations_mixed += r0.evaluations_mixed;
+        h->warm_fallbacks += 1;
+    }
     lap("minimise");
     double pc[4];
     if ((rc = pressure_impl(h, L.x.p, res->f, lj, pc))) return rc;

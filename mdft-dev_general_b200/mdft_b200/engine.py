@@ -59,6 +59,7 @@ class _MinRes(C.Structure):
 
 
 _DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
 
 
 class _Solute(C.Structure):
@@ -96,6 +97,28 @@ SIGNATURES = {
                                    C.c_double, C.c_double, C.POINTER(_MinOpts), _DP, C.c_void_p, C.POINTER(C.c_int)]),
     "mdft_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "mdft_get_stage_times": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int)]),
+    # learned warm start
+    "mdft_warm_net_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "mdft_warm_net_destroy": (C.c_int, [C.c_void_p]),
+    "mdft_warm_net_num_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "mdft_warm_net_init": (C.c_int, [C.c_void_p, C.c_ulonglong]),
+    "mdft_warm_net_set_params": (C.c_int, [C.c_void_p, _FP, C.c_longlong]),
+    "mdft_warm_net_get_params": (C.c_int, [C.c_void_p, _FP, C.c_longlong]),
+    "mdft_warm_net_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mdft_warm_net_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mdft_warm_net_output": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mdft_warm_net_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _FP, _DP]),
+    "mdft_warm_net_train_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                           C.POINTER(C.c_void_p), C.c_int, C.c_float]),
+    "mdft_warm_net_take_loss": (C.c_int, [C.c_void_p, _DP]),
+    "mdft_warm_net_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "mdft_warm_net_grid": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "mdft_warm_features": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP,
+                                     C.c_double, C.c_void_p]),
+    "mdft_warm_target": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mdft_warm_expand": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mdft_set_warm_net": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mdft_get_warm_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
 }
 
 
@@ -143,6 +166,7 @@ class Engine:
         self.box = (lx, ly, lz)
         self.shape = (nz, ny, nx, s.no)
         self.dv, self.rho0, self.kT = s.dv, s.rho0, s.kT
+        self.device = device
         self.lj_tail = 0.0
 
     def close(self):
@@ -290,6 +314,33 @@ class Engine:
         return dict(dG=out[0], f=out[1], pmv=out[2], lj_tail=out[3], pbulk=out[4], deltaN=out[5], pgnorm=r.pgnorm,
                     iterations=r.iterations, evaluations=r.evaluations, status=r.status,
                     evaluations_mixed=r.evaluations_mixed)
+
+    # -- learned warm start ---------------------------------------------------
+    def warm_features(self, solute, solvent, d_feat: int, rvdw=10.0):
+        """The warm-start network's 3 x N input channels for `solute` into device memory."""
+        q, sg, ep, xyz = (np.ascontiguousarray(v, dtype=np.float64) for v in (solute.q, solute.sig, solute.eps, solute.xyz))
+        vq, vs, ve, vx = (np.array(v, dtype=np.float64) for v in (solvent.q, solvent.sig, solvent.eps, solvent.xyz))
+        _check(lib().mdft_warm_features(self.h, len(q), _p(q), _p(sg), _p(ep), _p(xyz), len(vq), _p(vq), _p(vs), _p(ve),
+                                        _p(vx), float(rvdw), C.c_void_p(d_feat)))
+
+    def warm_target(self, d_target: int, d_mask: int | None = None, d_xi: int | None = None):
+        """4 x N log-density projections (and the N-point loss mask) of the density d_xi
+        (device; None: the last solve's result)."""
+        _check(lib().mdft_warm_target(self.h, None if d_xi is None else C.c_void_p(d_xi), C.c_void_p(d_target),
+                                      None if d_mask is None else C.c_void_p(d_mask)))
+
+    def warm_expand(self, d_pred: int, d_xi: int):
+        _check(lib().mdft_warm_expand(self.h, C.c_void_p(d_pred), C.c_void_p(d_xi)))
+
+    def set_warm_net(self, net):
+        """Start solves on this engine from `net`'s prediction (None: from the bulk guess)."""
+        _check(lib().mdft_set_warm_net(self.h, None if net is None else net.h))
+        self._warm = net
+
+    def warm_stats(self):
+        s = (C.c_longlong * 2)()
+        _check(lib().mdft_get_warm_stats(self.h, s))
+        return dict(warm_starts=s[0], fallbacks=s[1])
 
     def set_timing(self, on=True):
         _check(lib().mdft_set_timing(self.h, 1 if on else 0))

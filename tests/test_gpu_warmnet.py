@@ -1,0 +1,196 @@
+"""Learned warm start on the GPU against the CPU oracle (oracle/warmnet_ref.py).
+
+* the network's forward and every parameter gradient (library kernels: BF16 weights, FP32
+  activations and accumulation) against torch float64 autograd of the same network with
+  the same BF16-rounded weights, on a 16^3 grid;
+* training steps lower the loss;
+* the solver-side kernels (input channels, log-density projections and mask, starting
+  density) against their numpy restatements;
+* warm-started solves converge to the cold solve's result, and with the committed trained
+  parameters they are compared with cold solves on held-out solutes at 64^3."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import cases
+from mdft_b200 import Engine, PREC_MIXED, synth, warmstart
+from oracle import oracle as O
+from oracle import warmnet_ref as W
+
+pytestmark = pytest.mark.gpu
+SV = cases.SOLVENT
+N16 = 16
+
+
+def _dev(a, dtype=torch.float32):
+    t = torch.tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+    torch.cuda.synchronize()
+    return t
+
+
+@pytest.fixture(scope="module")
+def net16():
+    net = warmstart.WarmNet(N16, seed=5)
+    yield net
+    net.close()
+
+
+def _sample(seed):
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((3, N16, N16, N16)).astype(np.float32)
+    t = rng.standard_normal((4, N16, N16, N16)).astype(np.float32)
+    m = (rng.random((N16, N16, N16)) > 0.25).astype(np.float32)
+    return x, t, m
+
+
+def test_forward_matches_oracle(net16):
+    x, _, _ = _sample(11)
+    dx = _dev(x)
+    out = torch.empty((4, N16, N16, N16), device="cuda")
+    net16.forward(dx.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    p = W.bf16_weights(net16.get_params()).astype(np.float64)
+    ref = W.forward(torch.tensor(p), torch.tensor(x, dtype=torch.float64), torch).numpy()
+    got = out.cpu().numpy()
+    assert np.isfinite(got).all()
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err < 1e-5, err
+
+
+def test_gradients_match_oracle(net16):
+    x, t, m = _sample(12)
+    dx, dt, dm = _dev(x), _dev(t), _dev(m)
+    g, loss = net16.gradients(dx.data_ptr(), dt.data_ptr(), dm.data_ptr())
+    p = W.bf16_weights(net16.get_params()).astype(np.float64)
+    pt = torch.tensor(p, requires_grad=True)
+    y = W.forward(pt, torch.tensor(x, dtype=torch.float64), torch)
+    L = W.loss(y, torch.tensor(t, dtype=torch.float64), torch.tensor(m, dtype=torch.float64))
+    L.backward()
+    assert abs(loss - L.item()) <= 1e-5 * abs(L.item())
+    ref = pt.grad.numpy()
+    off = 0
+    for li, (k, _, _, ci, co, _, _) in enumerate(W.LAYERS):
+        n = int(np.prod(W.weight_shape(k, ci, co)))
+        for a, b, what in ((off, off + n, "W"), (off + n, off + n + co, "b")):
+            e = np.abs(g[a:b] - ref[a:b]).max() / np.abs(ref[a:b]).max()
+            assert e < 2e-4, (li, what, e)
+        off += n + co
+
+
+def test_training_lowers_the_loss():
+    net = warmstart.WarmNet(N16, seed=6)
+    rng = np.random.default_rng(13)
+    data = []
+    for _ in range(2):
+        x = rng.standard_normal((3, N16, N16, N16)).astype(np.float32)
+        t = np.stack([np.tanh(x[0] - 0.5 * x[1]), 0.3 * x[2], np.roll(x[0], 1, axis=2), x[1] * 0.5]).astype(np.float32)
+        data.append((_dev(x), _dev(t), _dev(np.ones((N16,) * 3, np.float32))))
+    before = warmstart.evaluate_loss(net, data)
+    for _ in range(80):
+        net.train_step([d[0].data_ptr() for d in data], [d[1].data_ptr() for d in data], [d[2].data_ptr() for d in data],
+                       2e-3)
+    assert np.isfinite(net.take_loss())
+    after = warmstart.evaluate_loss(net, data)
+    assert after < 0.3 * before, (before, after)
+    net.close()
+
+
+@pytest.fixture(scope="module")
+def sys16(tmp_path_factory):
+    c = cases.CASES["mol16_m2"]
+    ck = cases.ck_path(tmp_path_factory.mktemp("ck"), c["mmax"])
+    e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    sol = cases.solute_of(c)
+    e.compute_vext(sol, SV, rvdw=c["rvdw"])
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    tab = W.orientation_table(o.rotm, o.weights)
+    yield c, ck, e, sol, tab
+    e.close()
+
+
+def _vmax(kT):
+    return (-np.log(np.finfo(np.float64).eps) - float(np.float32(0.05))) * kT
+
+
+def test_channels_match_oracle(sys16):
+    c, _, e, sol, _ = sys16
+    n = c["n"]
+    feat = torch.empty((3, n ** 3), device="cuda")
+    e.warm_features(sol, SV, feat.data_ptr(), rvdw=c["rvdw"])
+    torch.cuda.synchronize()
+    ref = W.features((n, n, n), (c["L"],) * 3, sol, SV, e.kT, c["rvdw"]).reshape(3, -1)
+    got = feat.cpu().numpy()
+    for ch in range(3):
+        assert np.abs(got[ch] - ref[ch]).max() <= 1e-6 * max(1.0, np.abs(ref[ch]).max()), ch
+
+
+def test_target_and_expand_match_oracle(sys16):
+    c, _, e, _, tab = sys16
+    n = c["n"]
+    vext = e.get_vext()
+    rng = np.random.default_rng(14)
+    xi = rng.uniform(0.2, 2.5, e.shape)
+    xi[vext >= _vmax(e.kT)] = 0.0
+    dxi = _dev(xi, torch.float64)
+    tgt = torch.empty((4, n ** 3), device="cuda")
+    mask = torch.empty((n ** 3,), device="cuda")
+    e.warm_target(tgt.data_ptr(), mask.data_ptr(), d_xi=dxi.data_ptr())
+    torch.cuda.synchronize()
+    rt, rm = W.target(xi, vext, tab, _vmax(e.kT))
+    assert np.abs(tgt.cpu().numpy() - rt.reshape(4, -1)).max() < 1e-5
+    assert np.array_equal(mask.cpu().numpy(), rm.reshape(-1).astype(np.float32))
+    pred = rng.uniform(-2, 2, (4, n ** 3)).astype(np.float32)
+    dp = _dev(pred)
+    out = torch.empty(e.shape, dtype=torch.float64, device="cuda")
+    e.warm_expand(dp.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    rx = W.expand(pred.astype(np.float64).reshape(4, n, n, n), vext, tab, _vmax(e.kT))
+    assert np.abs(out.cpu().numpy() - rx).max() <= 1e-12 * rx.max()
+
+
+@pytest.mark.parametrize("precision", [0, PREC_MIXED])
+def test_warm_started_solve_reaches_the_cold_result(sys16, precision):
+    c, ck, _, sol, _ = sys16
+    opts = dict(m=5, pgtol=1e-5, ftol_abs=-1.0, itermax=2000, precision=precision)
+    cold = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=precision)
+    rc = cold.solve(sol, SV, rvdw=c["rvdw"], **opts)
+    warm = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=precision)
+    net = warmstart.WarmNet(c["n"], seed=9)
+    warm.set_warm_net(net)
+    rw = warm.solve(sol, SV, rvdw=c["rvdw"], **opts)
+    st = warm.warm_stats()
+    assert st["warm_starts"] == 1 and st["fallbacks"] == 0
+    assert rw["status"] == 0 and rw["pgnorm"] <= 1e-5
+    assert abs(rw["dG"] - rc["dG"]) < 2e-3, (rw["dG"], rc["dG"])
+    warm.set_warm_net(None)
+    rb = warm.solve(sol, SV, rvdw=c["rvdw"], **opts)
+    assert rb["evaluations"] == rc["evaluations"] and abs(rb["dG"] - rc["dG"]) < 1e-9 * abs(rc["dG"])
+    for x in (warm, cold):
+        x.close()
+    net.close()
+
+
+@pytest.mark.skipif(not os.path.exists(warmstart.WEIGHTS), reason="no trained parameters in the package")
+def test_trained_network_against_cold_solves(tmp_path):
+    """Held-out 1-30-site solutes at 64^3, mixed precision to max|df| <= 1e-4: the warm-started
+    solve reaches the cold solve's dG within 0.1 kJ/mol; the evaluation counts are reported."""
+    params, meta = warmstart.load_params()
+    ck = str(tmp_path / "ck.dat")
+    synth.make_ck_file(ck, 3, seed=warmstart.CK_SEED, kmax=12.0)
+    opts = dict(m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=3000, precision=PREC_MIXED)
+    e = Engine(64, 32.0, 3, ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    net = warmstart.WarmNet(64, params=params)
+    evals = []
+    for sd in (50000000, 50000001, 50000002):
+        sol = warmstart.centred(warmstart.config4_solute(sd), e.box)
+        e.set_warm_net(None)
+        rc = e.solve(sol, SV, **opts)
+        e.set_warm_net(net)
+        rw = e.solve(sol, SV, **opts)
+        assert abs(rw["dG"] - rc["dG"]) <= 0.1, (sd, rw["dG"], rc["dG"])
+        evals.append((rc["evaluations"] + rc["evaluations_mixed"], rw["evaluations"] + rw["evaluations_mixed"]))
+    print("evaluations cold/warm:", evals, "trained:", meta)
+    e.close()
+    net.close()
