@@ -58,8 +58,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="small grid smoke run (not a bench number)")
-    ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
-                    help="mixed: FP32 excess pipeline then an FP64 polish; fp64: plain FP64 solve")
+    ap.add_argument("--form", default="mixed", choices=["learned", "mixed", "fp64"],
+                    help="learned: mixed solves started from the trained warm-start network; mixed: FP32 excess "
+                         "pipeline then an FP64 polish, from the bulk guess; fp64: plain FP64 solve")
     ap.add_argument("--pgtol", type=float, default=PGTOL, help="stop at max|df| <= pgtol (FP64 gradient)")
     ap.add_argument("--workers", type=int, default=3,
                     help="concurrent solves per GPU (engine handles, each with its own buffers and stream)")
@@ -224,7 +225,24 @@ def main():
     ck = ck_file(MMAX)
     sv = synth.Solvent()
     prec = PREC_FP64 if args.form == "fp64" else PREC_MIXED
-    eng = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec)
+    warm_params, warm_meta, warm_note = None, None, None
+    if args.form == "learned":
+        from mdft_b200 import warmstart
+        if os.path.exists(warmstart.WEIGHTS):
+            warm_params, warm_meta = warmstart.load_params()
+        else:
+            warm_note = "no trained parameters in the package: solves start from the bulk guess"
+    nets = []
+
+    def attach(e):
+        if warm_params is not None:
+            from mdft_b200 import warmstart
+            net = warmstart.WarmNet(n, device=local, params=warm_params)
+            e.set_warm_net(net)
+            nets.append(net)
+        return e
+
+    eng = attach(Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec))
     stream = torch.cuda.ExternalStream(eng.stream)
     sols = [solute(10_000 * rank + i, box) for i in range(args.warmup + args.steps)]
     if args.evals:
@@ -245,6 +263,8 @@ def main():
         print(json.dumps({"solves": args.solves, "dG": r["dG"], "evaluations": r["evaluations"],
                           "evaluations_mixed": r["evaluations_mixed"]}))
         eng.close()
+        for net in nets:
+            net.close()
         return
 
     def barrier():
@@ -254,7 +274,7 @@ def main():
 
     # ---- W engine handles solve the steps' solutes concurrently (mdft_solve_batch) ----
     W = max(1, args.workers)
-    engines = [eng] + [Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec)
+    engines = [eng] + [attach(Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec))
                        for _ in range(W - 1)]
     streams = [torch.cuda.ExternalStream(e.stream) for e in engines]
 
@@ -324,7 +344,7 @@ def main():
     dom = max(per, key=per.get)
     peak, peak_kind = measured_peak_hbm()
     achieved = sb[dom] / (per[dom] * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC_BYTES.get((args.form, dom)) if n == N_GRID else None
+    traffic = NCU_TRAFFIC_BYTES.get(("fp64" if prec == PREC_FP64 else "mixed", dom)) if n == N_GRID else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind, "stage_ms": per,
             "algorithmic_bytes": sb[dom]}
@@ -345,9 +365,16 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": "%d^3 grid, %g A box, mmax %d, %d-site random-walk solute per step, synthetic c(k)"
                                        % (n, box, MMAX, NSITE),
-                           "form": ("plain FP64" if prec == PREC_FP64 else
+                           "form": ("plain FP64 from the bulk guess" if prec == PREC_FP64 else
+                                    ("learned warm start + " if warm_params is not None else "") +
                                     "mixed: FP32 projections/FFT/OZ with FP64 ideal term, reductions and L-BFGS, "
-                                    "then an FP64 polish") + " (vext + guess + L-BFGS m=5 + pressure correction)",
+                                    "then an FP64 polish") + " (vext + start + L-BFGS m=5 + pressure correction)",
+                           "warm_start": None if args.form != "learned" else (
+                               {"note": warm_note} if warm_params is None else
+                               {"network": "periodic 3-D conv encoder-decoder, 906772 parameters, BF16 weights",
+                                "trained": {k: warm_meta.get(k) for k in ("train", "epochs", "final_val_loss")},
+                                "starts": sum(e.warm_stats()["warm_starts"] for e in engines),
+                                "fallbacks_to_bulk_guess": sum(e.warm_stats()["fallbacks"] for e in engines)}),
                            "stop": "max|df|<=%g in FP64 (line-search stall accepted); dG checked against FP64 "
                                    "solves to max|df|<=%g" % (args.pgtol, PGTOL_REF),
                            "l2": "inputs larger than L2 (176 MB per field)",
@@ -362,6 +389,8 @@ def main():
         print(json.dumps(line))
     for e in engines:
         e.close()
+    for net in nets:
+        net.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -17,8 +17,11 @@
 // complex projections p(m <= 1, mu', mu = 0) of the reference's angl2proj
 // (src/module_orientation_projection_transform.f90:159-199) span the same functions.
 // Mask (FP32, [N]): 1 where some orientation is outside the hard core (vext < vmax).
-// Start: f = a_0 + a . u clamped to [-8, 4], xi = exp(f/2), and xi = 0 wherever
-// guess_density puts 0 (vext >= vmax, src/module_density.f90:267-284).
+// Start: f = a_0 + a . u clamped to [-2, 4], xi = exp(f/2), and xi = 0 wherever
+// guess_density puts 0 (vext >= vmax, src/module_density.f90:267-284).  The start's floor
+// is above the target's: dF/dxi is proportional to xi, so a region started near xi = 0
+// passes a max|df| test at the wrong density (a start floor of -8, xi = 0.018, left 28 of
+// 200 held-out solves at a different stationary point, up to 25 kJ/mol away).
 #pragma once
 
 namespace {
@@ -35,7 +38,8 @@ struct WarmFeatArgs {
 };
 
 constexpr double kWarmSmear = 0.5;  // A, width of the charge and site Gaussians
-constexpr double kWarmFloor = -8.0, kWarmCeil = 4.0;
+constexpr double kWarmFloor = -8.0, kWarmCeil = 4.0;  // target clamp of ln(rho/rho0)
+constexpr double kWarmStartFloor = -2.0;               // start clamp (xi >= exp(-1))
 
 __global__ void k_warm_features(float *__restrict__ feat, const WarmSite *__restrict__ s, WarmFeatArgs a) {
     const long long N = (long long)a.nx * a.ny * a.nz;
@@ -108,7 +112,7 @@ __global__ void k_warm_expand(const float *__restrict__ pred, const double *__re
         const int io = (int)(i - p * no);
         const double4 d = dir[io];
         double f = (double)pred[p] + (double)pred[N + p] * d.x + (double)pred[2 * N + p] * d.y + (double)pred[3 * N + p] * d.z;
-        f = fmin(fmax(f, kWarmFloor), kWarmCeil);
+        f = fmin(fmax(f, kWarmStartFloor), kWarmCeil);
         xi[i] = vext[i] >= vmax ? 0.0 : exp(0.5 * f);
     }
 }

@@ -249,9 +249,13 @@ def evaluate_heldout(params, seeds, solvent, ck, workers=3, pgtol=1e-4, pgtol_re
     rows = []
     for i, sd in enumerate(seeds):
         c, w = out["mixed_cold"][0][i], out["mixed_warm"][0][i]
-        rows.append(dict(seed=sd, nsite=len(sols[i].q), dG_fp64=ref[i],
+        f = out["fp64_ref"][0][i]
+        rows.append(dict(seed=sd, nsite=len(sols[i].q), dG_fp64=ref[i], fp64_evals=f["evaluations"],
+                         fp64_status=f["status"], fp64_pgnorm=f["pgnorm"],
                          cold_evals=c["evaluations"] + c["evaluations_mixed"], cold_iters=c["iterations"],
+                         cold_status=c["status"], cold_pgnorm=c["pgnorm"],
                          warm_evals=w["evaluations"] + w["evaluations_mixed"], warm_iters=w["iterations"],
+                         warm_status=w["status"], warm_pgnorm=w["pgnorm"],
                          cold_err=c["dG"] - ref[i], warm_err=w["dG"] - ref[i]))
     n = len(seeds)
     summ = dict(heldout=n, fallbacks=fallbacks,
@@ -263,6 +267,8 @@ def evaluate_heldout(params, seeds, solvent, ck, workers=3, pgtol=1e-4, pgtol_re
                 warm_mean_iters=float(np.mean([r["warm_iters"] for r in rows])),
                 cold_max_dG_err=float(np.max(np.abs([r["cold_err"] for r in rows]))),
                 warm_max_dG_err=float(np.max(np.abs([r["warm_err"] for r in rows]))),
+                cold_over_0p1=int(np.sum(np.abs([r["cold_err"] for r in rows]) > 0.1)),
+                warm_over_0p1=int(np.sum(np.abs([r["warm_err"] for r in rows]) > 0.1)),
                 fp64_mean_evals=float(np.mean([r["evaluations"] for r in out["fp64_ref"][0]])))
     return rows, summ
 
@@ -282,6 +288,7 @@ def main(argv=None):
     ap.add_argument("--ck", default=None, help="c(k) file (default: the synthetic mmax-3 table)")
     ap.add_argument("--eval", type=int, default=0, help="held-out 64^3 solutes to compare cold and warm solves on")
     ap.add_argument("--eval-seed0", type=int, default=50000000)
+    ap.add_argument("--eval-only", default=None, help="parameter file: skip training, only the held-out comparison")
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
@@ -296,6 +303,15 @@ def main(argv=None):
     if not a.ck:
         synth.make_ck_file(ck, MMAX, seed=CK_SEED, kmax=12.0)
     solvent = synth.Solvent()
+    if a.eval_only:
+        params, meta = load_params(a.eval_only)
+        rows, summ = evaluate_heldout(params, [a.eval_seed0 + i for i in range(a.eval)], solvent, ck,
+                                      workers=a.workers, pgtol=a.pgtol, log=log)
+        log("held-out: %s" % json.dumps(summ))
+        if a.report:
+            with open(a.report, "w") as f:
+                json.dump(dict(meta=meta, summary=summ, heldout=rows), f)
+        return
     engines = [E.Engine(TRAIN_N, TRAIN_BOX, MMAX, ck, temperature=solvent.temperature, n0=solvent.n0)
                for _ in range(a.workers)]
     seeds = [a.seed0 + i for i in range(a.train + a.val)]

@@ -103,7 +103,8 @@ def bf16_weights(flat: np.ndarray) -> np.ndarray:
 # solver-side kernels
 QFACT = (1.602176565e-19 ** 2 * 1.0e-3 * 6.02214129e23 / (4.0 * math.pi * 8.854187817e-12 * 1.0e-10))
 SMEAR = 0.5
-FLOOR, CEIL = -8.0, 4.0
+FLOOR, CEIL = -8.0, 4.0   # clamp of the target's ln(rho/rho0)
+START_FLOOR = -2.0        # clamp of the start's ln(rho/rho0)
 
 
 def features(dims, box, solute, solvent, kT, rvdw):
@@ -166,5 +167,5 @@ def expand(pred, vext, table, vmax):
     """pred: 4 x (nz, ny, nx) -> xi (nz, ny, nx, no)."""
     u = table[:, :3]
     f = pred[0][..., None] + sum(pred[k + 1][..., None] * u[:, k] for k in range(3))
-    f = np.clip(f, FLOOR, CEIL)
+    f = np.clip(f, START_FLOOR, CEIL)
     return np.where(vext >= vmax, 0.0, np.exp(0.5 * f))

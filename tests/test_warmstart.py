@@ -60,7 +60,7 @@ def test_projections_are_exact_on_the_quadrature(grid16):
     assert np.allclose(np.linalg.norm(tab[:, :3], axis=1), 1.0)
     rng = np.random.default_rng(3)
     n = c["n"]
-    a = rng.uniform(-1.5, 1.5, (4, n, n, n))
+    a = rng.uniform(-0.45, 0.45, (4, n, n, n))  # f = a0 + a.u stays above the start floor
     f = a[0][..., None] + sum(a[k + 1][..., None] * tab[:, k] for k in range(3))
     xi = np.exp(0.5 * f)
     vext = np.zeros_like(xi)
