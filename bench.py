@@ -310,7 +310,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     t_ms = float(t.item())
     value = world * args.steps / (t_ms / 1e3)
-    evals = [r["evaluations"] for r in timed]
+    # evaluations per solve: FP64 ones (the whole FP64 solve; the check/polish of a mixed one)
+    # plus the FP32 evaluations of a mixed solve
+    evals = [r["evaluations"] + r.get("evaluations_mixed", 0) for r in timed]
 
     # ---- e2e: the same call with each converged density returned to pinned host memory ----
     xi_pinned = [torch.empty(int(np.prod(eng.shape)), dtype=torch.float64, pin_memory=True) for _ in steps_idx]
@@ -354,10 +356,12 @@ def main():
         if not args.no_cpu_baseline and not args.quick:
             threads = os.cpu_count() or 1
             te_cpu = cpu_oracle_eval_seconds(n, box, MMAX, ck, 2, threads)
-            epsolve = float(np.mean(evals))
+            # the CPU solve is an FP64 solve: scale by the FP64 solve's evaluation count (this
+            # run's when it timed FP64 solves, else the FP64 GPU solves' count on this workload)
+            epsolve = float(np.mean(evals)) if prec == PREC_FP64 else float(EVALS_PER_SOLVE_FP64)
             cpu = {"value": 1.0 / (te_cpu * epsolve), "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": "2 FP64 evaluations of the workload on the host (oracle, %d OpenMP threads) x %.1f "
-                             "evaluations per solve (the GPU FP64 solves' mean)" % (threads, epsolve)}
+                             "evaluations per FP64 solve" % (threads, epsolve)}
         clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
@@ -382,6 +386,7 @@ def main():
                            "workers": W,
                            "evaluations_per_solve": evals,
                            "fp32_evaluations_per_solve": [r.get("evaluations_mixed", 0) for r in timed],
+                           "fp64_evaluations_per_solve": [r["evaluations"] for r in timed],
                            "dG": [r["dG"] for r in timed], "dG_fp64": dg_ref,
                            "dG_error_vs_fp64_max": max(dg_err), "all_within_0.1": bool(max(dg_err) <= 0.1)},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
