@@ -226,6 +226,40 @@ int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const 
 /* Number of kernels this handle has launched since creation. */
 int mdft_get_launch_count(const mdft_handle *h, long long *count);
 
+/* ---- Input files of the reference (host only; no GPU needed) ----
+ *
+ * dft.in (src/module_input.f90): lines are 100-character records, cut at '#', blank lines
+ * dropped (:654-732); a tag's value is list-directed-read from columns len(tag)+4 ..
+ * len(tag)+50 of the first line that starts with the tag followed by a blank, i.e. after
+ * "tag = " (:73-79); logicals take the first character of the first item, T/t or F/f
+ * (:386-427).  The getters leave *out untouched and set *found = 0 when the tag is absent
+ * (the caller's defaults stand); a value that does not read returns MDFT_E_IO. */
+typedef struct mdft_input mdft_input;
+int mdft_input_read(const char *path, mdft_input **out);
+int mdft_input_free(mdft_input *in);
+int mdft_input_nlines(const mdft_input *in, int *n);
+int mdft_input_line(const mdft_input *in, int i, char *buf, int buflen);
+/* n = 1..3 values (getinput%dp/dp2/dp3, getinput%int/int2/int3) */
+int mdft_input_get_dp(const mdft_input *in, const char *tag, int n, double *out, int *found);
+int mdft_input_get_int(const mdft_input *in, const char *tag, int n, int *out, int *found);
+int mdft_input_get_log(const mdft_input *in, const char *tag, int *out, int *found);
+/* character(50) value: the first list-directed item, NUL-terminated in out */
+int mdft_input_get_char(const mdft_input *in, const char *tag, char *out, int outlen, int *found);
+/* Grid and thermo of init_grid / init_thermo (src/module_grid.f90:62-95,
+ * src/module_thermo.f90:25): molrotsymorder (default 2), boxlen (default 128 128 128),
+ * boxnod (default nint(boxlen/0.3)), mmax (default 0), temperature (default 300); n0,
+ * the c(k) path, precision and device come from the caller. */
+int mdft_desc_from_input(const mdft_input *in, const char *ck_path, double n0, int precision, int device, mdft_desc *out);
+/* solute.in (src/module_solute.f90:36-52): a comment line, the site count, a comment line,
+ * then per site: index, q, sigma, epsilon, x, y, z, Z.  Charges are multiplied by
+ * charge_scale (solute_charges_scale_factor).  With q == NULL only *nsite is returned;
+ * otherwise the arrays hold cap sites (xyz 3 per site; Z may be NULL). */
+int mdft_read_solute(const char *path, double charge_scale, int cap, int *nsite, double *q, double *sig, double *eps,
+                     double *xyz, int *Z);
+/* mv_solute_to_center (src/module_solute.f90:146-187): with translate, move the mean site
+ * position to the box centre; then wrap every coordinate into [0, box) (Fortran MODULO). */
+int mdft_center_solute(int nsite, double *xyz, const double *box, int translate);
+
 /* ---- Learned warm start (no counterpart in the reference, whose solves always start
  * from guess_density, src/module_density.f90:267-284) ----
  *

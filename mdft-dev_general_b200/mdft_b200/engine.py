@@ -97,6 +97,19 @@ SIGNATURES = {
                                    C.c_double, C.c_double, C.POINTER(_MinOpts), _DP, C.c_void_p, C.POINTER(C.c_int)]),
     "mdft_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "mdft_get_stage_times": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int)]),
+    # input files
+    "mdft_input_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "mdft_input_free": (C.c_int, [C.c_void_p]),
+    "mdft_input_nlines": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "mdft_input_line": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int]),
+    "mdft_input_get_dp": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, _DP, C.POINTER(C.c_int)]),
+    "mdft_input_get_int": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mdft_input_get_log": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mdft_input_get_char": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_int)]),
+    "mdft_desc_from_input": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_int, C.c_int, C.POINTER(_Desc)]),
+    "mdft_read_solute": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.POINTER(C.c_int), _DP, _DP, _DP, _DP,
+                                   C.POINTER(C.c_int)]),
+    "mdft_center_solute": (C.c_int, [C.c_int, _DP, _DP, C.c_int]),
     # learned warm start
     "mdft_warm_net_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "mdft_warm_net_destroy": (C.c_int, [C.c_void_p]),
