@@ -25,7 +25,9 @@ def test_solve_from_input_files(tmp_path):
     opts = dict(m=5, pgtol=1e-5, ftol_abs=-1.0, itermax=2000)
     r1 = e.solve(sol, SV, rvdw=d.dp("rvdw", 10.0), **opts)
     ref = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
-    direct = synth.Solute(q=raw.q, sig=raw.sig, eps=raw.eps, xyz=inputs.center_solute(raw.xyz, ref.box))
+    # the same sites (as read from solute.in) given directly to an engine built without dft.in
+    direct = synth.Solute(q=sol.q.copy(), sig=sol.sig.copy(), eps=sol.eps.copy(), xyz=sol.xyz.copy())
+    assert np.allclose(sol.q, raw.q, atol=1e-10)
     r2 = ref.solve(direct, SV, rvdw=c["rvdw"], **opts)
     assert r1["evaluations"] == r2["evaluations"]
     assert abs(r1["dG"] - r2["dG"]) <= 1e-8 * max(1.0, abs(r2["dG"]))
