@@ -226,6 +226,26 @@ int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const 
 /* Number of kernels this handle has launched since creation. */
 int mdft_get_launch_count(const mdft_handle *h, long long *count);
 
+/* ---- The reference's density file (output/density.bin, input/density.bin) ----
+ *
+ * Write (src/module_postprocessing.f90:45-95): Fortran unformatted sequential records with
+ * 4-byte length markers -- ns (1; -1 when full), mmax, no, np, (nx, ny, nz), (dx, dy, dz),
+ * nsite, one 176-byte site_type record per solute site (name blank, type and n_sites 0,
+ * r, q, sig, eps, lambda1 = lambda2 = 0, Z), then per grid point (x fastest) one record of
+ * np complex angl2proj(xi(:, point)), or with full != 0 no records of one real each.
+ * xi: host array of no*nx*ny*nz doubles, or NULL for the handle's last solve; Z may be NULL. */
+int mdft_write_density_bin(mdft_handle *h, const double *xi, int nsite, const double *q, const double *sig, const double *eps,
+                           const double *xyz, const int *Z, int full, const char *path);
+/* Restart (read_restart_file, src/module_density.f90:61-261): the file's projections become xi
+ * on the file's grid (proj2angl with this handle's orientations; the file's mmax may be
+ * lower), interpolated trilinearly onto this grid with the file's box centred in this one
+ * (the reference's loop order: a point on a cell face takes the last cell's value; points
+ * outside every cell keep xi's input value).  A full-density file needs this grid and
+ * orientations.  The solute sites must match the file's (count no larger, positions equal
+ * to the file's plus the centring offset, same sigma and epsilon).  xi (host, in/out). */
+int mdft_read_density_bin(mdft_handle *h, const char *path, int nsite, const double *sig, const double *eps, const double *xyz,
+                          double *xi);
+
 /* ---- Input files of the reference (host only; no GPU needed) ----
  *
  * dft.in (src/module_input.f90): lines are 100-character records, cut at '#', blank lines

@@ -985,6 +985,7 @@ int mdft_guess_density_device(mdft_handle *h, double *d_xi) {
 }  // extern "C"
 
 #include "warmstart.cuh"
+#include "restart.cuh"
 
 namespace {
 

@@ -97,6 +97,10 @@ SIGNATURES = {
                                    C.c_double, C.c_double, C.POINTER(_MinOpts), _DP, C.c_void_p, C.POINTER(C.c_int)]),
     "mdft_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "mdft_get_stage_times": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int)]),
+    # density file
+    "mdft_write_density_bin": (C.c_int, [C.c_void_p, _DP, C.c_int, _DP, _DP, _DP, _DP, C.POINTER(C.c_int), C.c_int,
+                                         C.c_char_p]),
+    "mdft_read_density_bin": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, _DP, _DP, _DP, _DP]),
     # input files
     "mdft_input_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "mdft_input_free": (C.c_int, [C.c_void_p]),
@@ -327,6 +331,25 @@ class Engine:
         return dict(dG=out[0], f=out[1], pmv=out[2], lj_tail=out[3], pbulk=out[4], deltaN=out[5], pgnorm=r.pgnorm,
                     iterations=r.iterations, evaluations=r.evaluations, status=r.status,
                     evaluations_mixed=r.evaluations_mixed)
+
+    # -- the reference's density file -------------------------------------------
+    def write_density_bin(self, path, solute, xi=None, full=False):
+        """output/density.bin of the reference for `xi` (None: the last solve's density)."""
+        q, sg, ep, xyz = (np.ascontiguousarray(v, dtype=np.float64) for v in (solute.q, solute.sig, solute.eps, solute.xyz))
+        Z = None
+        if getattr(solute, "Z", None) is not None:
+            Z = (C.c_int * len(q))(*[int(z) for z in solute.Z])
+        x = None if xi is None else np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        _check(lib().mdft_write_density_bin(self.h, _p(x), len(q), _p(q), _p(sg), _p(ep), _p(xyz), Z, 1 if full else 0,
+                                            str(path).encode()))
+
+    def read_density_bin(self, path, solute, xi_start=None):
+        """Restart density from a density.bin onto this grid; points the file does not cover
+        keep xi_start's values (default: the bulk guess of the current vext)."""
+        sg, ep, xyz = (np.ascontiguousarray(v, dtype=np.float64) for v in (solute.sig, solute.eps, solute.xyz))
+        x = np.array(self.guess_density() if xi_start is None else xi_start, dtype=np.float64, copy=True).reshape(self.shape)
+        _check(lib().mdft_read_density_bin(self.h, str(path).encode(), len(sg), _p(sg), _p(ep), _p(xyz), _p(x)))
+        return x
 
     # -- learned warm start ---------------------------------------------------
     def warm_features(self, solute, solvent, d_feat: int, rvdw=10.0):
