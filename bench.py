@@ -46,8 +46,9 @@ PGTOL = 1e-4
 PGTOL_REF = 1e-6
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from the ncu
-# capture summarised in profiles/ncu_oz_gather_project_fp32_64cubed_mmax3.md (absent: null)
-NCU_TRAFFIC_BYTES = {("mixed", "oz"): 67.3e6, ("mixed", "gather"): 562.0e6, ("mixed", "project"): 213.9e6}
+# captures summarised in profiles/ncu_gather_traffic_api_64cubed_mmax3.md (gather) and
+# profiles/ncu_ozp_project_fft_fp32_64cubed_mmax3.md (oz, project); absent: null
+NCU_TRAFFIC_BYTES = {("mixed", "oz"): 65.1e6, ("mixed", "gather"): 559.2e6, ("mixed", "project"): 213.6e6}
 
 
 def parse():

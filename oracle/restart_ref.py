@@ -68,7 +68,7 @@ def restart(orc, d: dict, grid_n3, grid_d3, grid_L, xi_start):
     for k in range(nzp):
         for j in range(nyp):
             for i in range(nxp):
-                xp[k, j, i] = orc.proj2angl(np.ascontiguousarray(pad[k, j, i]).view(np.float64))
+                xp[k, j, i] = orc.proj2angl(pad[k, j, i])
     xi = np.array(xi_start, dtype=np.float64, copy=True)
     for io in range(no):
         for izp in range(1, nzp):
