@@ -176,6 +176,26 @@ def cpu_oracle_eval_seconds(n, box, mmax, ck, nevals, threads):
     return (time.perf_counter() - t0) / nevals
 
 
+def replica_seeds(rank, count):
+    """Seeds of the solutes one rank solves: replicas work on disjoint solutes."""
+    return [10_000 * rank + i for i in range(count)]
+
+
+def max_over_ranks(t_ms, world, device):
+    """The slowest rank's time (every rank calls this once per timed region)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([t_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, t_ms):
+    """Solutes/s of the whole job: every rank solves `steps` solutes within t_ms."""
+    return world * steps / (t_ms / 1e3)
+
+
 def reference_arm(args, rank, world):
     """CPU implementation of the path on the host cores (the C restatement; the
     Fortran reference cannot be compiled here)."""
@@ -220,7 +240,7 @@ def main():
 
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=180))
     n, box = (N_GRID, BOX) if not args.quick else (32, 16.0)
     rvdw = RVDW if not args.quick else 7.9
     ck = ck_file(MMAX)
@@ -245,7 +265,7 @@ def main():
 
     eng = attach(Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec))
     stream = torch.cuda.ExternalStream(eng.stream)
-    sols = [solute(10_000 * rank + i, box) for i in range(args.warmup + args.steps)]
+    sols = [solute(sd, box) for sd in replica_seeds(rank, args.warmup + args.steps)]
     if args.evals:
         # profiling mode: the same workload's evaluations at the guess density of the first solute
         eng.compute_vext(sols[0], sv, rvdw=rvdw)
@@ -306,11 +326,8 @@ def main():
     with Clocks(local) as clk:
         timed, t_ms = timed_batch(steps_idx)
     launches = sum(e.launch_count for e in engines) - l0
-    t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_ms = float(t.item())
-    value = world * args.steps / (t_ms / 1e3)
+    t_ms = max_over_ranks(t_ms, world, "cuda")
+    value = whole_job_rate(world, args.steps, t_ms)
     # evaluations per solve: FP64 ones (the whole FP64 solve; the check/polish of a mixed one)
     # plus the FP32 evaluations of a mixed solve
     evals = [r["evaluations"] + r.get("evaluations_mixed", 0) for r in timed]
@@ -320,10 +337,7 @@ def main():
     xi_host = [b.numpy().reshape(eng.shape) for b in xi_pinned]
     barrier()
     _, te_ms = timed_batch(steps_idx, xi_bufs=xi_host)
-    te = torch.tensor([te_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / (float(te.item()) / 1e3)
+    e2e_value = whole_job_rate(world, args.steps, max_over_ranks(te_ms, world, "cuda"))
     s0 = sols[0]
     h2d = 8 * (4 * s0.nsite + 4 * 3 * 2)  # solute q, sig, eps, xyz + solvent sites
     d2h = xi_host[0].nbytes + 8 * 6
