@@ -1,0 +1,112 @@
+"""Uneven batch: many solutes on different grids and angular orders solved concurrently.
+
+64 seeded solutes of 1-40 sites (random walk as the 24-site workload), each on a grid drawn
+from {32, 48, 64, 96}^3 with a box of 0.5 A x nodes and an mmax drawn from {1, 3}.  One
+engine handle per (grid, mmax); each solute is pinned to its handle and mdft_solve_batch runs
+the handles' solves concurrently.  Reported: aggregate solutes/s (wall clock around the
+batch call) and each solute's |dG - dG_FP64|, the FP64 solve to max|df| <= 1e-6 from the
+bulk guess being the reference.  rvdw is 7.9 A for every solute: the 16 A box of the 32^3
+grid allows at most 8 A (src/module_lennardjones.f90:55-59).
+
+    python -m mdft_b200.uneven_batch [--solutes 64] [--report out.json]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+from . import engine as E
+from . import synth
+
+GRIDS = (32, 48, 64, 96)
+MMAXES = (1, 3)
+RVDW = 7.9
+CK_SEED = 20260001
+
+
+def draw(nsolutes: int, seed0: int = 60000000):
+    """(seed, nsite, n, mmax) per solute, all from numpy's PCG64 seeded per solute."""
+    out = []
+    for i in range(nsolutes):
+        rng = np.random.default_rng(seed0 + i)
+        out.append((seed0 + i, int(rng.integers(1, 41)), int(rng.choice(GRIDS)), int(rng.choice(MMAXES))))
+    return out
+
+
+def solutes_of(plan):
+    sols = []
+    for seed, nsite, n, _ in plan:
+        s = synth.random_walk_solute(nsite, seed)
+        s.xyz = synth.center_solute(s.xyz, (0.5 * n,) * 3)
+        sols.append(s)
+    return sols
+
+
+def run(plan, ck_dir, precision, pgtol, solvent, workers_per_combo=1):
+    combos = sorted({(n, m) for _, _, n, m in plan})
+    ck = {}
+    for m in MMAXES:
+        ck[m] = os.path.join(ck_dir, "ck_m%d.txt" % m)
+        if not os.path.exists(ck[m]):
+            synth.make_ck_file(ck[m], m, seed=CK_SEED, kmax=12.0)
+    engines, index = [], {}
+    for n, m in combos:
+        index[(n, m)] = []
+        for _ in range(workers_per_combo):
+            index[(n, m)].append(len(engines))
+            engines.append(E.Engine(n, 0.5 * n, m, ck[m], temperature=solvent.temperature, n0=solvent.n0,
+                                    precision=precision))
+    sols = solutes_of(plan)
+    count = {}
+    handles = []
+    for _, _, n, m in plan:
+        k = count.get((n, m), 0)
+        handles.append(index[(n, m)][k % workers_per_combo])
+        count[(n, m)] = k + 1
+    t0 = time.perf_counter()
+    res = E.solve_batch(engines, sols, solvent, rvdw=RVDW, m=5, pgtol=pgtol, ftol_abs=-1.0, itermax=5000,
+                        precision=precision, handles=handles)
+    wall = time.perf_counter() - t0
+    for e in engines:
+        e.close()
+    return res, wall
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--solutes", type=int, default=64)
+    ap.add_argument("--pgtol", type=float, default=1e-4)
+    ap.add_argument("--workers-per-grid", type=int, default=1)
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+    solvent = synth.Solvent()
+    plan = draw(a.solutes)
+    d = tempfile.mkdtemp()
+    mixed, t_mixed = run(plan, d, E.PREC_MIXED, a.pgtol, solvent, a.workers_per_grid)
+    fp64, t_fp64 = run(plan, d, E.PREC_FP64, a.pgtol, solvent, a.workers_per_grid)
+    ref, t_ref = run(plan, d, E.PREC_FP64, 1e-6, solvent, a.workers_per_grid)
+    rows = []
+    for (seed, nsite, n, m), x, y, r in zip(plan, mixed, fp64, ref):
+        rows.append(dict(seed=seed, nsite=nsite, n=n, mmax=m, dG_fp64=r["dG"], mixed_err=x["dG"] - r["dG"],
+                         fp64_err=y["dG"] - r["dG"], mixed_evals=x["evaluations"] + x["evaluations_mixed"],
+                         fp64_evals=y["evaluations"], mixed_status=x["status"], fp64_status=y["status"]))
+    summ = dict(solutes=len(plan), handles=len({(n, m) for _, _, n, m in plan}) * a.workers_per_grid,
+                mixed_solutes_per_s=len(plan) / t_mixed, fp64_solutes_per_s=len(plan) / t_fp64,
+                mixed_max_abs_err=float(max(abs(r["mixed_err"]) for r in rows)),
+                fp64_max_abs_err=float(max(abs(r["fp64_err"]) for r in rows)),
+                mixed_over_0p1=int(sum(abs(r["mixed_err"]) > 0.1 for r in rows)),
+                fp64_over_0p1=int(sum(abs(r["fp64_err"]) > 0.1 for r in rows)),
+                wall_s=dict(mixed=t_mixed, fp64=t_fp64, fp64_ref_1e6=t_ref), pgtol=a.pgtol, rvdw=RVDW)
+    print(json.dumps(summ))
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump(dict(summary=summ, solutes=rows), f)
+
+
+if __name__ == "__main__":
+    main()

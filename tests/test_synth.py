@@ -50,3 +50,14 @@ def test_solute_generators():
     assert d.min() >= 3.0 and abs(c.q.sum()) < 1e-12
     x = synth.center_solute(s.xyz, (32.0,) * 3)
     assert np.all((x >= 0) & (x < 32.0))
+
+
+def test_uneven_batch_plan():
+    from mdft_b200 import uneven_batch as U
+    plan = U.draw(64)
+    assert plan == U.draw(64)
+    assert {n for _, _, n, _ in plan} == set(U.GRIDS) and {m for _, _, _, m in plan} == set(U.MMAXES)
+    assert all(1 <= k <= 40 for _, k, _, _ in plan)
+    for s, (_, k, n, _) in zip(U.solutes_of(plan), plan):
+        assert s.nsite == k and (s.xyz >= 0).all() and (s.xyz < 0.5 * n).all()
+        assert 0.5 * n / 2 >= U.RVDW  # the reference's cut-off check holds on every grid
