@@ -132,7 +132,7 @@ def centred(sol, box):
     return synth.Solute(q=sol.q, sig=sol.sig, eps=sol.eps, xyz=synth.center_solute(sol.xyz, box))
 
 
-def make_training_set(engines, seeds, solvent, torch, rvdw=10.0, pgtol=1e-4, precision=E.PREC_FP64, log=None):
+def make_training_set(engines, seeds, solvent, rvdw=10.0, pgtol=1e-4, precision=E.PREC_FP64, log=None):
     """Solve every seeded solute with the plain solver (from the bulk guess) on the given
     engines, one host thread per engine, and keep each one's channels, target and mask on
     the device.  Returns (samples, per-solute results)."""
@@ -315,7 +315,7 @@ def main(argv=None):
     engines = [E.Engine(TRAIN_N, TRAIN_BOX, MMAX, ck, temperature=solvent.temperature, n0=solvent.n0)
                for _ in range(a.workers)]
     seeds = [a.seed0 + i for i in range(a.train + a.val)]
-    samples, res = make_training_set(engines, seeds, solvent, torch, pgtol=a.pgtol, log=log)
+    samples, res = make_training_set(engines, seeds, solvent, pgtol=a.pgtol, log=log)
     tgen = time.time() - t0
     log("training set: %d solutes in %.1f s (%.1f evaluations per solve)" %
         (len(samples), tgen, np.mean([r["evaluations"] for r in res])))
