@@ -82,26 +82,32 @@ def main(argv=None):
     ap.add_argument("--solutes", type=int, default=64)
     ap.add_argument("--pgtol", type=float, default=1e-4)
     ap.add_argument("--workers-per-grid", type=int, default=1)
+    ap.add_argument("--forms", default="mixed,fp64", help="forms to time, comma-separated: mixed, fp64")
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
     solvent = synth.Solvent()
     plan = draw(a.solutes)
     d = tempfile.mkdtemp()
-    mixed, t_mixed = run(plan, d, E.PREC_MIXED, a.pgtol, solvent, a.workers_per_grid)
-    fp64, t_fp64 = run(plan, d, E.PREC_FP64, a.pgtol, solvent, a.workers_per_grid)
+    forms = [f for f in a.forms.split(",") if f]
+    out = {}
+    for f in forms:
+        prec = E.PREC_MIXED if f == "mixed" else E.PREC_FP64
+        out[f] = run(plan, d, prec, a.pgtol, solvent, a.workers_per_grid)
     ref, t_ref = run(plan, d, E.PREC_FP64, 1e-6, solvent, a.workers_per_grid)
     rows = []
-    for (seed, nsite, n, m), x, y, r in zip(plan, mixed, fp64, ref):
-        rows.append(dict(seed=seed, nsite=nsite, n=n, mmax=m, dG_fp64=r["dG"], mixed_err=x["dG"] - r["dG"],
-                         fp64_err=y["dG"] - r["dG"], mixed_evals=x["evaluations"] + x["evaluations_mixed"],
-                         fp64_evals=y["evaluations"], mixed_status=x["status"], fp64_status=y["status"]))
-    summ = dict(solutes=len(plan), handles=len({(n, m) for _, _, n, m in plan}) * a.workers_per_grid,
-                mixed_solutes_per_s=len(plan) / t_mixed, fp64_solutes_per_s=len(plan) / t_fp64,
-                mixed_max_abs_err=float(max(abs(r["mixed_err"]) for r in rows)),
-                fp64_max_abs_err=float(max(abs(r["fp64_err"]) for r in rows)),
-                mixed_over_0p1=int(sum(abs(r["mixed_err"]) > 0.1 for r in rows)),
-                fp64_over_0p1=int(sum(abs(r["fp64_err"]) > 0.1 for r in rows)),
-                wall_s=dict(mixed=t_mixed, fp64=t_fp64, fp64_ref_1e6=t_ref), pgtol=a.pgtol, rvdw=RVDW)
+    for i, (seed, nsite, n, m) in enumerate(plan):
+        row = dict(seed=seed, nsite=nsite, n=n, mmax=m, dG_fp64=ref[i]["dG"])
+        for f in forms:
+            x = out[f][0][i]
+            row.update({f + "_err": x["dG"] - ref[i]["dG"], f + "_evals": x["evaluations"] + x["evaluations_mixed"],
+                        f + "_status": x["status"]})
+        rows.append(row)
+    summ = dict(solutes=len(plan), handles=len({(n, m) for _, _, n, m in plan}) * a.workers_per_grid, pgtol=a.pgtol,
+                rvdw=RVDW, wall_s=dict({f: out[f][1] for f in forms}, fp64_ref_1e6=t_ref))
+    for f in forms:
+        errs = [abs(r[f + "_err"]) for r in rows]
+        summ.update({f + "_solutes_per_s": len(plan) / out[f][1], f + "_max_abs_err": float(max(errs)),
+                     f + "_over_0p1": int(sum(e > 0.1 for e in errs))})
     print(json.dumps(summ))
     if a.report:
         with open(a.report, "w") as f:
