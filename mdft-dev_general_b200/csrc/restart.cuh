@@ -22,6 +22,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <new>
 
 namespace {
 
@@ -124,6 +125,7 @@ struct FRecReader {
     bool rec(std::vector<unsigned char> &buf) {
         uint32_t n = 0, m = 0;
         if (std::fread(&n, 4, 1, f) != 1) { err = "unexpected end of file"; return false; }
+        if (n > (1u << 20)) { err = "record longer than any of this format"; return false; }  // <= 16 np bytes
         buf.resize(n);
         if (n && std::fread(buf.data(), n, 1, f) != 1) { err = "truncated record"; return false; }
         if (std::fread(&m, 4, 1, f) != 1 || m != n) { err = "record markers do not match"; return false; }
@@ -232,7 +234,11 @@ int mdft_read_density_bin(mdft_handle *h, const char *path, int nsite, const dou
     if (!ok) { set_error("%s: %s", path, r.err.c_str()); return MDFT_E_IO; }
     const bool full = ns < 0;
     if ((full ? -ns : ns) != 1) { set_error("%s: %d solvent species (one is supported)", path, full ? -ns : ns); return MDFT_E_ARG; }
-    if (n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || no_p < 1 || np_p < 1) { set_error("%s: bad grid in header", path); return MDFT_E_IO; }
+    if (n3[0] < 1 || n3[1] < 1 || n3[2] < 1 || n3[0] > 65536 || n3[1] > 65536 || n3[2] > 65536 || no_p < 1 || np_p < 1 ||
+        (long long)n3[0] * n3[1] * n3[2] > (1LL << 33)) {
+        set_error("%s: bad grid in header", path);
+        return MDFT_E_IO;
+    }
     // the file's box centred in this one (src/module_density.f90:129-131)
     const double off[3] = {(g.lx - d3[0] * n3[0]) / 2, (g.ly - d3[1] * n3[1]) / 2, (g.lz - d3[2] * n3[2]) / 2};
     if (nsite_p > nsite) { set_error("%s: %d solute sites in the file, %d given", path, nsite_p, nsite); return MDFT_E_ARG; }
@@ -262,7 +268,13 @@ int mdft_read_density_bin(mdft_handle *h, const char *path, int nsite, const dou
     }
     if (np_p > g.np) { set_error("%s: %d projections, this grid has %d (mmax %d < %d)", path, np_p, g.np, g.mmax, mmax_p); return MDFT_E_ARG; }
     const long long Np = (long long)n3[0] * n3[1] * n3[2];
-    std::vector<double2> hp((size_t)Np * g.np, make_double2(0.0, 0.0));
+    std::vector<double2> hp;
+    try {
+        hp.assign((size_t)Np * g.np, make_double2(0.0, 0.0));
+    } catch (const std::bad_alloc &) {
+        set_error("%s: no host memory for %lld points x %d projections", path, Np, g.np);
+        return MDFT_E_NOMEM;
+    }
     for (long long pt = 0; pt < Np; ++pt) {
         if (!r.rec(b) || b.size() != 16u * np_p) { set_error("%s: projection record %lld: %s", path, pt, r.err.empty() ? "bad length" : r.err.c_str()); return MDFT_E_IO; }
         std::memcpy(&hp[(size_t)pt * g.np], b.data(), 16u * np_p);
