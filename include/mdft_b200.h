@@ -44,7 +44,7 @@ extern "C" {
 
 /* Arithmetic of the excess-term pipeline. */
 #define MDFT_PREC_FP64 0  /* every stage in FP64 (parity path)                          */
-#define MDFT_PREC_MIXED 1 /* FP32 FFT + OZ, split-BF16 angular transforms, FP64 sums   */
+#define MDFT_PREC_MIXED 1 /* FP32 projections, FFTs, OZ and angular transforms, FP64 sums */
 
 typedef struct mdft_handle mdft_handle;
 
