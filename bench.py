@@ -386,9 +386,14 @@ def main():
                                        % (n, box, MMAX, NSITE),
                            "form": ("plain FP64 from the bulk guess" if prec == PREC_FP64 else
                                     ("learned warm start + " if warm_params is not None else "") +
-                                    "mixed: FP32 projections/FFT/OZ with FP64 ideal term, reductions and L-BFGS, "
-                                    "then an FP64 polish") + " (vext + start + L-BFGS m=5 + pressure correction)",
-                           "warm_start": None if args.form != "learned" else (
+                                    "mixed: FP32 projections, FFTs, OZ, angular transforms, ideal/external terms and "
+                                    "L-BFGS vectors (BF16 history) with FP64 sums, then an FP64 check/polish")
+                                   + " (vext + start + L-BFGS m=5 + pressure correction)",
+                           "warm_start": (
+                               {"used": False, "note": "the learned warm start (--form learned) is built and trained; "
+                                                       "on held-out solutes it needs as many evaluations as the bulk "
+                                                       "guess, so this form starts from the bulk guess"}
+                               if args.form == "mixed" else None) if args.form != "learned" else (
                                {"note": warm_note} if warm_params is None else
                                {"network": "periodic 3-D conv encoder-decoder, 906772 parameters, BF16 weights",
                                 "trained": {k: warm_meta.get(k) for k in ("train", "epochs", "final_val_loss")},
