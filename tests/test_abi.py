@@ -56,3 +56,30 @@ def test_batch_argument_errors_without_gpu():
                             ctypes.byref(o), ctypes.cast(out, engine._DP), ctypes.cast(res, ctypes.c_void_p), None)
     assert rc == -1
     assert b"out of range" in L.mdft_last_error()
+
+
+def _c_fields(text, name):
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if decl:
+            out += [re.sub(r"[\s*]", "", v).split("[")[0] for v in re.split(r",", re.sub(r"^[\w\s]+?\s(?=[\w*]+(\s*,|$))", "", decl))]
+    return out
+
+
+def _f_fields(text, name):
+    body = re.search(r"type, bind\(C\) :: %s\n(.*?)end type" % name, text, re.S).group(1)
+    out = []
+    for line in body.splitlines():
+        if "::" in line:
+            out += [v.strip() for v in line.split("::")[1].split("!")[0].split(",")]
+    return out
+
+
+@pytest.mark.parametrize("name", ["mdft_desc", "mdft_minimize_opts", "mdft_minimize_result"])
+def test_fortran_interface_types_match_the_header(name):
+    h = open(os.path.join(ROOT, "include", "mdft_b200.h")).read()
+    f = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    assert _f_fields(f, name) == _c_fields(h, name)

@@ -109,3 +109,12 @@ def test_network_argument_errors_without_gpu():
     assert L.mdft_warm_net_num_params(None, ctypes.byref(n)) == -1
     assert L.mdft_set_warm_net(None, None) == -1
     assert L.mdft_warm_target(None, None, None, None) == -1
+
+
+def test_shipped_parameters_load():
+    import os
+    assert os.path.exists(warmstart.WEIGHTS)
+    p, meta = warmstart.load_params()
+    assert p.size == W.num_params() and np.isfinite(p).all()
+    assert np.array_equal(p, W.bf16_round(p))                      # stored as BF16
+    assert meta["train"] == 2000 and meta["final_val_loss"] < 0.1
