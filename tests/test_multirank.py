@@ -57,3 +57,32 @@ def test_reference_arm_runs_on_rank_zero_only():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
                         "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def _rank_dies(rank, world, port, q):
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "mdft-dev_general_b200")]
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    import bench
+    if rank == 1:
+        os._exit(3)  # this replica dies between steps, before the timing reduction
+    try:
+        bench.max_over_ranks(100.0, world, "cpu")
+        q.put((rank, "no error"))
+    except Exception as e:  # noqa: BLE001 - the collective's error is the detection
+        q.put((rank, type(e).__name__))
+
+
+def test_a_dead_replica_ends_the_others_collective_with_an_error():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_dies, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    rank, what = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+    assert rank == 0 and what != "no error"
+    assert procs[1].exitcode == 3
