@@ -64,3 +64,19 @@ def test_charge_corrections_values():
     psch = -SV.quadrupole_trace * SV.n0 * 2909.857
     assert abs(c - (pbc + psch)) < 1e-12
     assert O.charge_corrections(0.0, 20.0, 71.0, 0.8, SV.n0) == 0.0
+
+
+@pytest.mark.parametrize("mmax", [1, 2, 3])
+def test_projections_of_a_real_field_are_hermitian(tmp_path, mmax):
+    # p(m, -mu', 0) = (-1)^mu' conj p(m, mu', 0) for any real o(omega): the reference's sign
+    # and conjugation conventions (angl2proj, src/module_orientation_projection_transform.f90:159-199)
+    # with d^m_{-mu',0} = (-1)^mu' d^m_{mu',0}
+    o = O.Oracle(8, 4.0, mmax, cases.ck_path(tmp_path, mmax), 2.477, 0.0333)
+    plist = [(m, mup, mu) for m in range(mmax + 1) for mup in range(-m, m + 1) for mu in range(0, m + 1, 2)]
+    idx = {t: i for i, t in enumerate(plist)}
+    assert len(plist) == o.np
+    for seed in range(3):
+        p = o.angl2proj(np.random.default_rng(seed).uniform(0.0, 2.0, o.no))
+        for m, mup, mu in plist:
+            if mu == 0:
+                assert abs(p[idx[(m, -mup, 0)]] - (-1) ** mup * np.conj(p[idx[(m, mup, 0)]])) < 1e-14
