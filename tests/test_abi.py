@@ -83,3 +83,25 @@ def test_fortran_interface_types_match_the_header(name):
     h = open(os.path.join(ROOT, "include", "mdft_b200.h")).read()
     f = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     assert _f_fields(f, name) == _c_fields(h, name)
+
+
+def test_ck_table_checks_without_gpu(tmp_path):
+    # the reference's c(k) assertions (src/module_read_c_luc.f90:102-108, src/module_input.f90:638-646)
+    # run before any device call: a table shorter than the grid's qmax, and a non-uniform abscissa
+    from mdft_b200 import synth
+    L = engine.lib()
+    h = ctypes.c_void_p()
+    short = str(tmp_path / "short.txt")
+    synth.make_ck_file(short, 1, kmax=2.0, dk=0.02)
+    d = engine._Desc(16, 16, 16, 8.0, 8.0, 8.0, 1, 2, 298.0, 0.0333, short.encode(), 0, 0)
+    assert L.mdft_create(ctypes.byref(d), ctypes.byref(h)) == -2
+    assert b"rows needed" in L.mdft_last_error()
+    lines = open(short).read().split("\n")
+    first = next(i for i, l in enumerate(lines) if i > 15 and l.strip()[:1].isdigit())  # first data row
+    parts = lines[first + 5].split(None, 1)
+    lines[first + 5] = "%.6f %s" % (float(parts[0]) + 0.005, parts[1])
+    bad = str(tmp_path / "bad.txt")
+    open(bad, "w").write("\n".join(lines))
+    d = engine._Desc(16, 16, 16, 8.0, 8.0, 8.0, 1, 2, 298.0, 0.0333, bad.encode(), 0, 0)
+    assert L.mdft_create(ctypes.byref(d), ctypes.byref(h)) == -2
+    assert b"uniform" in L.mdft_last_error()
