@@ -45,9 +45,9 @@ CK_SEED = 20260001
 PGTOL = 1e-4
 PGTOL_REF = 1e-6
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from the ncu
-# captures summarised in profiles/ncu_gather_traffic_api_64cubed_mmax3.md (gather) and
-# profiles/ncu_ozp_project_fft_fp32_64cubed_mmax3.md (oz, project); absent: null
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from one ncu
+# capture of each kernel on this workload (the gather through the public API; the OZ and the
+# projection in a mixed solve); absent: null
 NCU_TRAFFIC_BYTES = {("mixed", "oz"): 65.1e6, ("mixed", "gather"): 559.2e6, ("mixed", "project"): 213.6e6}
 
 

@@ -9,8 +9,8 @@
  *
  * and the set-up and callers those need (vext, guess_density, the L-BFGS
  * loop of energy_minimization, pressure_correction).  A Fortran host binds
- * these entry points with ISO_C_BINDING; the binding stubs are listed in
- * INTEGRATION.md.
+ * these entry points with ISO_C_BINDING (one bind(C) interface per entry point,
+ * with the structs below as bind(C) derived types).
  *
  * Layout: every per-orientation field (xi, vext, df) is the reference's
  * Fortran array (no, nx, ny, nz) with io fastest, i.e. the C index
@@ -134,6 +134,11 @@ typedef struct mdft_minimize_opts {
     double pgtol_mixed; /* MIXED: stop the FP32 phase at max|df| <= this (<= 0: pgtol) */
     int polish;      /* MIXED: 1 = continue with FP64 evaluations until pgtol holds;
                         0 = one FP64 evaluation at the FP32 phase's result          */
+    double guni_tol; /* > 0: the pgtol test also needs |sum_{r,io} w(io) df dv| <= guni_tol,
+                        the gradient along a uniform change of xi (kJ/mol); <= 0: off.
+                        Not in the reference: the solvation free energy's error at a
+                        stopping point follows this sum (about half of it, in kJ/mol),
+                        which converges more slowly than max|df| for small solutes     */
 } mdft_minimize_opts;
 
 typedef struct mdft_minimize_result {
@@ -143,6 +148,7 @@ typedef struct mdft_minimize_result {
     int evaluations; /* energy_and_gradient calls                                 */
     int status;      /* 0 pgtol, 1 f-reduction, 2 line-search failure, 3 itermax   */
     int evaluations_mixed; /* of which FP32-pipeline evaluations (MDFT_PREC_MIXED)   */
+    double guni;     /* sum_{r,io} w(io) df dv at the returned xi (kJ/mol)          */
 } mdft_minimize_result;
 
 /* minimization_using_lbfgs (src/energy_minimization.f90:232-290) with the
@@ -217,7 +223,9 @@ int mdft_get_stage_times(const mdft_handle *h, double *ms5, int *count);
  * per-block partial sums go to a fixed 256 KB array inside the library, one per GPU that
  * loads it, held until the process exits, so npoints is limited to 1,048,576 (larger
  * sizes return MDFT_E_ARG with a message).  The first call on a device looks up that
- * array's device address; make that first call before any stream capture.  Every call
+ * array's device address; make that first call before any stream capture.  After a
+ * cudaDeviceReset the next call on that device looks the address up again (the array
+ * may move with the new context), so that call too belongs before any capture.  Every call
  * shares the array: calls that overlap on the GPU race and must be serialised by the
  * caller.  Same arithmetic as src/module_energy_ideal_and_external.f90:46-73. */
 int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const double *d_w, int no, long long npoints,

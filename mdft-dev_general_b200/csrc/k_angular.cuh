@@ -30,7 +30,8 @@ struct AngularArgs {
     double rho0;
 };
 
-constexpr int kGatherSums = 5;  // per-block partials of k_gather
+// per-block partials of the gathers: F_id, F_ext, F_exc sum, df.d, max|df|, sum w df
+constexpr int kGatherSums = 6;
 
 struct GatherArgs {
     long long N;
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
     T *As = smem;                                    // [Kpad][BM+1]
     T *Bs = As + ((size_t)Kpad * lda + 3) / 4 * 4;   // [BK][BN]
     T *Cs = Bs + kAngBK * kAngBN;                    // [BM][BN+1]
-    __shared__ double red[5][kAngThreads / 32];
+    __shared__ double red[kGatherSums][kAngThreads / 32];
     const long long pt0 = (long long)blockIdx.x * BM;
     const int npts = (int)min((long long)BM, a.N - pt0);
     const T cst = (T)a.cst;
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
         As[(size_t)(2 * ip + 1) * lda + p] = v.y;
     }
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0;
+    double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0, gun = 0.0;
     for (int j0 = 0; j0 < J; j0 += kAngBN) {
         T acc[TM][4];
 #pragma unroll
@@ -211,6 +212,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
                 df[g] = gv;
                 if (a.dvec) gdv = fma(gv, static_cast<const double *>(a.dvec)[g], gdv);
                 gmx = fmax(gmx, fabs(gv));
+                gun = fma(gv, wio, gun);
             } else if (a.df_mode == 2) {
                 df[g] = df[g] + dexc;
             }
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
         fexc += __shfl_down_sync(0xffffffffu, fexc, off);
         gdv += __shfl_down_sync(0xffffffffu, gdv, off);
         gmx = fmax(gmx, __shfl_down_sync(0xffffffffu, gmx, off));
+        gun += __shfl_down_sync(0xffffffffu, gun, off);
     }
     int wid = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (lane == 0) {
@@ -231,16 +234,18 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
         red[2][wid] = fexc;
         red[3][wid] = gdv;
         red[4][wid] = gmx;
+        red[5][wid] = gun;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
         for (int i = 0; i < kAngThreads / 32; ++i) {
             s0 += red[0][i];
             s1 += red[1][i];
             s2 += red[2][i];
             s3 += red[3][i];
             s4 = fmax(s4, red[4][i]);
+            s5 += red[5][i];
         }
         double *pp = partial + kGatherSums * (size_t)blockIdx.x;
         pp[0] = s0;
@@ -248,6 +253,7 @@ __global__ void __launch_bounds__(kAngThreads) k_gather(const typename Cplx<T>::
         pp[2] = s2;
         pp[3] = s3;
         pp[4] = s4;
+        pp[5] = s5;
     }
 }
 
@@ -262,22 +268,21 @@ inline size_t gather_smem_bytes(int BM, int np) {
     return sizeof(T) * (((size_t)Kpad * (BM + 1) + 3) / 4 * 4 + kAngBK * kAngBN + (size_t)BM * (kAngBN + 1));
 }
 
-// Sum n rows of kGatherSums partials into out[0..4] (one block, fixed order): entries 0-3
-// are sums, entry 4 a maximum.
+// Sum n rows of kGatherSums partials into out[0..5] (one block, fixed order): entry 4 is a
+// maximum, the others sums.
 __global__ void k_reduce_sums(const double *__restrict__ partial, long long n, double *__restrict__ out) {
     __shared__ double s[kGatherSums][256];
-    double a[kGatherSums] = {0, 0, 0, 0, 0};
+    double a[kGatherSums] = {0, 0, 0, 0, 0, 0};
     for (long long i = threadIdx.x; i < n; i += blockDim.x) {
         const double *pp = partial + kGatherSums * i;
-        for (int j = 0; j < 4; ++j) a[j] += pp[j];
-        a[4] = fmax(a[4], pp[4]);
+        for (int j = 0; j < kGatherSums; ++j) a[j] = j == 4 ? fmax(a[j], pp[j]) : a[j] + pp[j];
     }
     for (int j = 0; j < kGatherSums; ++j) s[j][threadIdx.x] = a[j];
     __syncthreads();
     for (int off = blockDim.x / 2; off > 0; off >>= 1) {
         if ((int)threadIdx.x < off) {
-            for (int j = 0; j < 4; ++j) s[j][threadIdx.x] += s[j][threadIdx.x + off];
-            s[4][threadIdx.x] = fmax(s[4][threadIdx.x], s[4][threadIdx.x + off]);
+            for (int j = 0; j < kGatherSums; ++j)
+                s[j][threadIdx.x] = j == 4 ? fmax(s[j][threadIdx.x], s[j][threadIdx.x + off]) : s[j][threadIdx.x] + s[j][threadIdx.x + off];
         }
         __syncthreads();
     }

@@ -10,7 +10,7 @@
 // owns points PW w .. PW w + PW-1 (PW = BM/8) and lane l the orientations l, l+32, l+64
 // (NCOL columns of 32), so the matrix products read the projections as broadcasts and B
 // without bank conflicts, and each epilogue store of df is a coalesced 256-byte run.
-// Partial sums (F_id, F_ext, F_exc sum, df.d, max|df|) are kept per thread across tiles
+// Partial sums (F_id, F_ext, F_exc sum, df.d, max|df|, sum w df) are kept per thread across tiles
 // and reduced once per CTA in a fixed order.
 //
 // Used when N is a multiple of 32, no <= 96, the pointers are 16-byte aligned and the
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
     __syncthreads();
 
     const double pre = a.prefactor * a.cst;
-    double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0;
+    double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0, gun = 0.0;
     for (int i = 0; i < nmine; ++i) {
         const int s = i % kGtStages;
         const bool ok = mbar_wait(&full[s], (uint32_t)((i / kGtStages) & 1));
@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
                         if (valid) df[pt0 * no + e] = (TD)gv;
                         if (want_d) gdv = fma(gv, (double)ds[e], gdv);
                         gmx = fmax(gmx, fabs(gv));
+                        gun = fma(gv, wv[c], gun);
                     }
                 }
         }
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
         fexc += __shfl_down_sync(0xffffffffu, fexc, off);
         gdv += __shfl_down_sync(0xffffffffu, gdv, off);
         gmx = fmax(gmx, __shfl_down_sync(0xffffffffu, gmx, off));
+        gun += __shfl_down_sync(0xffffffffu, gun, off);
     }
     if (lane == 0) {
         red[0][warp] = fid;
@@ -230,16 +232,18 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
         red[2][warp] = fexc;
         red[3][warp] = gdv;
         red[4][warp] = gmx;
+        red[5][warp] = gun;
     }
     __syncthreads();
     if (tid == 0) {
-        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
         for (int k = 0; k < kGtThreads / 32; ++k) {
             s0 += red[0][k];
             s1 += red[1][k];
             s2 += red[2][k];
             s3 += red[3][k];
             s4 = fmax(s4, red[4][k]);
+            s5 += red[5][k];
         }
         double *pp = partial + kGatherSums * (size_t)blockIdx.x;
         pp[0] = s0;
@@ -247,6 +251,7 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
         pp[2] = s2;
         pp[3] = s3;
         pp[4] = s4;
+        pp[5] = s5;
     }
 }
 

@@ -4,6 +4,7 @@
 
 #include <mutex>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -21,9 +22,42 @@ constexpr double kEpsDp = 2.220446049250313080847263336181640625e-16;
 // reads back, so nothing carries over between calls; calls that overlap on the GPU race.
 static __device__ __align__(256) double g_partials[2 * kMaxBlocks];
 
-// Device address of g_partials per device, looked up on the first call on that device.
-double *g_partials_addr[kMaxDevices] = {nullptr};
+// Device address of g_partials per device, looked up on the first call on that device and
+// again whenever the current context is not the one it was looked up in: cudaDeviceReset
+// destroys the primary context, and the array may sit elsewhere in the next one.
+struct ScratchSlot {
+    double *addr = nullptr;
+    unsigned long long ctx_id = 0;  // unique id of the context the address belongs to
+};
+ScratchSlot g_slots[kMaxDevices];
 std::mutex g_lock;
+
+// Unique id of the calling thread's current context (cuCtxGetCurrent + cuCtxGetId, reached
+// through the runtime's driver entry points so that the library needs no libcuda link).
+// false when no context is current or the driver does not offer the query.
+bool current_context_id(unsigned long long *id) {
+    using GetCurrentFn = CUresult (*)(CUcontext *);
+    using GetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa{}, qb{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrentFn>(a);
+            get_id = reinterpret_cast<GetIdFn>(b);
+        }
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 // energy_ideal_and_external (src/module_energy_ideal_and_external.f90:46-73) over the
 // points [blockIdx.x*64, +64) of one block: partial F_id, F_ext and df = id+ext gradient.
@@ -118,16 +152,25 @@ extern "C" int mdft_ideal_external_noalloc(const double *d_xi, const double *d_v
     if (dev < 0 || dev >= kMaxDevices) return fail(MDFT_E_ARG, "mdft_ideal_external_noalloc: device ordinal out of range");
     double *scratch;
     {
-        // First call on this device: look up the device address of the fixed array
-        // (host code may not use &g_partials, which is only a host-side stand-in).
+        // First call on this device (or first in a new context): look up the device address
+        // of the fixed array (host code may not use &g_partials, which is only a host-side
+        // stand-in for it).
         std::lock_guard<std::mutex> lk(g_lock);
-        if (!g_partials_addr[dev]) {
+        ScratchSlot &slot = g_slots[dev];
+        unsigned long long id = 0;
+        const bool have_id = current_context_id(&id);
+        if (!slot.addr || !have_id || id != slot.ctx_id) {
             void *p = nullptr;
             e = cudaGetSymbolAddress(&p, g_partials);
             if (e != cudaSuccess) return fail(MDFT_E_CUDA, cudaGetErrorString(e));
-            g_partials_addr[dev] = static_cast<double *>(p);
+            slot.addr = static_cast<double *>(p);
+            // the lookup made the device's context current if none was
+            slot.ctx_id = current_context_id(&id) ? id : 0;
+            if (!slot.ctx_id) slot.addr = nullptr;  // no id to check against: look up on every call
+            scratch = static_cast<double *>(p);
+        } else {
+            scratch = slot.addr;
         }
-        scratch = g_partials_addr[dev];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     k_ideal_external_partials<<<(unsigned)nblk, kThreads, 0, st>>>(d_xi, d_vext, d_w, no, npoints, kT, rho0, dv, d_df, scratch);

@@ -99,8 +99,10 @@ void regrid_axis(int n, double d, int np_, double dp, double off, std::vector<in
     w.assign(n, 0.0);
     for (int k = 1; k <= np_ - 1; ++k) {
         const double x0 = (k - 1) * dp + off, x1 = k * dp + off;
-        const int lo = std::max(1, (int)std::ceil(x0 / d + 1));
-        const int hi = std::min(n, (int)std::floor(x1 / d + 1));
+        // node range in double, clamped to [0, n+1] before the conversion to int
+        const double flo = std::ceil(x0 / d + 1), fhi = std::floor(x1 / d + 1);
+        const int lo = std::max(1, (int)std::min<double>(std::max<double>(flo, 0.0), n + 1.0));
+        const int hi = std::min(n, (int)std::min<double>(std::max<double>(fhi, 0.0), n + 1.0));
         for (int i = lo; i <= hi; ++i) {
             const double x = (i - 1) * d;
             cell[i - 1] = k - 1;
@@ -239,6 +241,11 @@ int mdft_read_density_bin(mdft_handle *h, const char *path, int nsite, const dou
         set_error("%s: bad grid in header", path);
         return MDFT_E_IO;
     }
+    for (int a = 0; a < 3; ++a)
+        if (!(std::isfinite(d3[a]) && d3[a] > 0.0 && d3[a] * n3[a] <= 1.0e9)) {
+            set_error("%s: bad grid spacing in header (%g)", path, d3[a]);
+            return MDFT_E_IO;
+        }
     // the file's box centred in this one (src/module_density.f90:129-131)
     const double off[3] = {(g.lx - d3[0] * n3[0]) / 2, (g.ly - d3[1] * n3[1]) / 2, (g.lz - d3[2] * n3[2]) / 2};
     if (nsite_p > nsite) { set_error("%s: %d solute sites in the file, %d given", path, nsite_p, nsite); return MDFT_E_ARG; }

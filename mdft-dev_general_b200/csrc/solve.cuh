@@ -12,20 +12,21 @@ inline unsigned vec_grid() { return kRedBlocks; }
 
 // Evaluation in two halves so that more work can be queued before the synchronise:
 // eval_launch queues the pipeline at x (gradient into g; with dvec also g.dvec and max|g|
-// from the gather pass), eval_finish waits and reads f, g.dvec and max|g|.
+// from the gather pass), eval_finish waits and reads f, g.dvec, max|g| and sum w g dv.
 int eval_launch(mdft_handle *h, const void *x, double *g, const void *dvec, bool v32 = false, bool x32 = false) {
     return run_pipeline(h, x, g, 1, 1, dvec, v32, x32);
 }
 
-int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
+int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax, double *guni = nullptr) {
     double fid, fext, fexc;
     int rc = finish_sums(h, &fid, &fext, &fexc);
     if (rc) return rc;
     *f = combine(h, fid, fext, fexc);
-    const double gdv = h->h_sums[3], gmx = h->h_sums[4];
+    const double gdv = h->h_sums[3], gmx = h->h_sums[4], gun = h->h_sums[5] * h->g.dv;
     if (gd) *gd = gdv;
     if (gmax) *gmax = gmx;
-    if (!std::isfinite(gdv) || !std::isfinite(gmx)) {
+    if (guni) *guni = gun;
+    if (!std::isfinite(gdv) || !std::isfinite(gmx) || !std::isfinite(gun)) {
         set_error("non-finite gradient");
         return MDFT_E_NUMERIC;
     }
@@ -35,10 +36,10 @@ int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax) {
 // x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.  v32: g and dvec
 // are FP32 vectors (the minimiser's mixed solves).
 int eval_fg(mdft_handle *h, const void *x, double *g, const void *dvec, double *f, double *gd, double *gmax,
-            bool v32 = false, bool x32 = false) {
+            bool v32 = false, bool x32 = false, double *guni = nullptr) {
     int rc = eval_launch(h, x, g, dvec, v32, x32);
     if (rc) return rc;
-    return eval_finish(h, f, gd, gmax);
+    return eval_finish(h, f, gd, gmax, guni);
 }
 
 int lbfgs_alloc(mdft_handle *h, int m) {
@@ -741,15 +742,17 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     }
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
-    double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0;
+    double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0, guni = 0;
     int iter = 0, nfgv = 0, status = 3;
     const bool fresh = H.col == 0;
     PendingPair pend;
-    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32, x32))) return rc;
+    // projgr's test (max|df| <= pgtol), plus, when asked, the uniform-mode gradient bound
+    auto converged = [&](double gm, double gu) { return gm <= o->pgtol && (o->guni_tol <= 0.0 || std::fabs(gu) <= o->guni_tol); };
+    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32, x32, &guni))) return rc;
     nfgv = 1;
     trace_iter(h, x32 ? nullptr : xc, 0, nfgv, f, gmax, 0.0);
     double sbgnrm = gmax;
-    if (sbgnrm <= o->pgtol) { status = 0; goto done; }
+    if (converged(sbgnrm, guni)) { status = 0; goto done; }
     if ((rc = history_dots_now(h, H, gc))) return rc;  // s_i.g, y_i.g, g.g at the start point
     while (iter < o->itermax) {
         // ---- search direction (stores the pair accepted last step) and the first trial ----
@@ -763,7 +766,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         fold = f;
         gdold = gd;
         int ifun = 0, iback = 0, info = 0;
-        double gmax_t = gmax;
+        double gmax_t = gmax, guni_t = guni;
         // the slot a pair accepted in this step would take, and the slots that stay
         const int tnext = H.col < m ? H.slot(H.col) : H.head;
         DotsPlan P;
@@ -802,7 +805,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 // the history's products with this trial gradient, queued before the one
                 // synchronise of the step (used if the trial is accepted)
                 if ((rc = launch_history_dots(h, H, gt, gc, L.d.p, stp, P))) return rc;
-                if ((rc = eval_finish(h, &f, &gd, &gmax_t))) return rc;
+                if ((rc = eval_finish(h, &f, &gd, &gmax_t, &guni_t))) return rc;
                 const double stp_eval = stp;
                 task = dcsrch(f, gd, stp, ftol, gtol, xtol, 0.0, stpmx, false, LS);
                 // Approximate Wolfe test (Hager and Zhang, SIAM J. Optim. 16 (2005) 170, eq. 4.1):
@@ -835,9 +838,10 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         std::swap(xc, xt);
         std::swap(gc, gt);
         gmax = gmax_t;
+        guni = guni_t;
         sbgnrm = gmax;
         trace_iter(h, x32 ? nullptr : xc, iter, nfgv, f, gmax, stp);
-        if (sbgnrm <= o->pgtol) { status = 0; goto done; }
+        if (converged(sbgnrm, guni)) { status = 0; goto done; }
         if ((fold - f) <= o->ftol_abs) { status = 1; goto done; }
         // ---- BFGS update (matupd) ----
         double dr, ddum;
@@ -889,6 +893,7 @@ done:
     if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;
     res->f = f;
     res->pgnorm = sbgnrm;
+    res->guni = guni;
     res->iterations = iter;
     res->evaluations = nfgv;
     res->status = status;
@@ -930,11 +935,12 @@ int solve_phases(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_resu
             rc = minimize_impl(h, o, res, H, false);
             res->iterations += r1.iterations;
         } else if (!rc) {
-            double f = 0.0, gmax = 0.0;
-            rc = eval_fg(h, h->lb.x.p, h->df.p, nullptr, &f, nullptr, &gmax);
+            double f = 0.0, gmax = 0.0, guni = 0.0;
+            rc = eval_fg(h, h->lb.x.p, h->df.p, nullptr, &f, nullptr, &gmax, false, false, &guni);
             *res = r1;
             res->f = f;
             res->pgnorm = gmax;
+            res->guni = guni;
             res->evaluations = 1;
         }
         res->evaluations_mixed = r1.evaluations;

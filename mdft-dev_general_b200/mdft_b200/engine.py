@@ -50,12 +50,12 @@ class _Sizes(C.Structure):
 
 class _MinOpts(C.Structure):
     _fields_ = [("m", C.c_int), ("pgtol", C.c_double), ("ftol_abs", C.c_double), ("itermax", C.c_int),
-                ("precision", C.c_int), ("pgtol_mixed", C.c_double), ("polish", C.c_int)]
+                ("precision", C.c_int), ("pgtol_mixed", C.c_double), ("polish", C.c_int), ("guni_tol", C.c_double)]
 
 
 class _MinRes(C.Structure):
     _fields_ = [("f", C.c_double), ("pgnorm", C.c_double), ("iterations", C.c_int), ("evaluations", C.c_int),
-                ("status", C.c_int), ("evaluations_mixed", C.c_int)]
+                ("status", C.c_int), ("evaluations_mixed", C.c_int), ("guni", C.c_double)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -277,24 +277,24 @@ class Engine:
         return xi
 
     def minimize(self, xi, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64, pgtol_mixed=0.0,
-                 polish=1):
+                 polish=1, guni_tol=0.0):
         x = np.array(xi, dtype=np.float64, copy=True).reshape(self.shape)
-        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish, guni_tol)
         r = _MinRes()
         _check(lib().mdft_minimize(self.h, _p(x), C.byref(o), C.byref(r)))
         return x, dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
-                       evaluations_mixed=r.evaluations_mixed)
+                       evaluations_mixed=r.evaluations_mixed, guni=r.guni)
 
     def guess_density_device(self, d_xi: int):
         _check(lib().mdft_guess_density_device(self.h, C.c_void_p(d_xi)))
 
     def minimize_device(self, d_xi: int, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
-                        pgtol_mixed=0.0, polish=1):
-        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
+                        pgtol_mixed=0.0, polish=1, guni_tol=0.0):
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish, guni_tol)
         r = _MinRes()
         _check(lib().mdft_minimize_device(self.h, C.c_void_p(d_xi), C.byref(o), C.byref(r)))
         return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
-                    evaluations_mixed=r.evaluations_mixed)
+                    evaluations_mixed=r.evaluations_mixed, guni=r.guni)
 
     @property
     def launch_count(self) -> int:
@@ -310,7 +310,7 @@ class Engine:
         return dict(dG=out[0], pmv=out[1], pbulk=out[2], deltaN=out[3])
 
     def solve(self, solute, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
-              xi_out=None, pgtol_mixed=0.0, polish=1):
+              xi_out=None, pgtol_mixed=0.0, polish=1, guni_tol=0.0):
         """vext -> guess_density -> L-BFGS -> pressure correction for one solute (main.f90's flow)."""
         q = np.ascontiguousarray(solute.q, dtype=np.float64)
         sg = np.ascontiguousarray(solute.sig, dtype=np.float64)
@@ -322,7 +322,7 @@ class Engine:
         vx = np.array(solvent.xyz, dtype=np.float64)
         if xi_out is not None:
             assert xi_out.dtype == np.float64 and xi_out.flags.c_contiguous and xi_out.size == int(np.prod(self.shape))
-        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish, guni_tol)
         r = _MinRes()
         out = np.zeros(6)
         _check(lib().mdft_solve(self.h, len(q), _p(q), _p(sg), _p(ep), _p(xyz), len(vq), _p(vq), _p(vs), _p(ve), _p(vx),
@@ -330,7 +330,7 @@ class Engine:
         self.lj_tail = float(out[3])
         return dict(dG=out[0], f=out[1], pmv=out[2], lj_tail=out[3], pbulk=out[4], deltaN=out[5], pgnorm=r.pgnorm,
                     iterations=r.iterations, evaluations=r.evaluations, status=r.status,
-                    evaluations_mixed=r.evaluations_mixed)
+                    evaluations_mixed=r.evaluations_mixed, guni=r.guni)
 
     # -- the reference's density file -------------------------------------------
     def write_density_bin(self, path, solute, xi=None, full=False):
@@ -389,7 +389,7 @@ class Engine:
 
 
 def solve_batch(engines, solutes, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,
-                pgtol_mixed=0.0, polish=1, handles=None, xi_out=None):
+                pgtol_mixed=0.0, polish=1, handles=None, xi_out=None, guni_tol=0.0):
     """Solve many solutes concurrently: one host worker per engine (each engine has its own
     device buffers and stream), solutes assigned by `handles` (index per solute, -1 or None:
     the next free engine).  xi_out: optional list of host arrays (or None entries) for the
@@ -404,7 +404,7 @@ def solve_batch(engines, solutes, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=
         arr[i] = _Solute(len(q), _p(q), _p(sg), _p(ep), _p(xyz), -1 if handles is None else int(handles[i]), _p(xo))
     hs = (C.c_void_p * len(engines))(*[e.h for e in engines])
     vq, vs, ve, vx = (np.array(v, dtype=np.float64) for v in (solvent.q, solvent.sig, solvent.eps, solvent.xyz))
-    o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish)
+    o = _MinOpts(m, pgtol, ftol_abs, itermax, precision, pgtol_mixed, polish, guni_tol)
     out = np.zeros(6 * max(1, n))
     res = (_MinRes * max(1, n))()
     rc = (C.c_int * max(1, n))()
@@ -413,5 +413,5 @@ def solve_batch(engines, solutes, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=
     del keep
     return [dict(dG=out[6 * i], f=out[6 * i + 1], pmv=out[6 * i + 2], lj_tail=out[6 * i + 3], pbulk=out[6 * i + 4],
                  deltaN=out[6 * i + 5], pgnorm=res[i].pgnorm, iterations=res[i].iterations, evaluations=res[i].evaluations,
-                 status=res[i].status, evaluations_mixed=res[i].evaluations_mixed) for i in range(n)]
+                 status=res[i].status, evaluations_mixed=res[i].evaluations_mixed, guni=res[i].guni) for i in range(n)]
 

@@ -24,6 +24,24 @@ CASES = {
     "rand8_m5": dict(n=8, L=4.0, mmax=5, solute="none", seed=6, rvdw=1.9, xseed=16, dk=0.1),
 }
 
+# The benchmark workloads and every FFT length the engine dispatches on: the single LJ ion
+# (sigma 2.5, eps 0.5, q +1) at the centre of a 20 A box on 32^3 at mmax 1; a 24-site
+# random-walk solute (6 A radius) in a 32 A box on 64^3 at mmax 3; the uneven batch's
+# 48^3 and 96^3 grids (0.5 A spacing); a 128-long z axis.  c(k) tabulated with dk 0.01.
+CONFIG_CASES = {
+    "ion32_m1": dict(n=32, L=20.0, mmax=1, solute="ion", seed=21, rvdw=10.0, xseed=31, dk=0.01, kmax=12.0),
+    "mol64_m3": dict(n=64, L=32.0, mmax=3, solute="walk24", seed=22, rvdw=10.0, xseed=32, dk=0.01, kmax=12.0,
+                     radius=6.0),
+    "mol48_m3": dict(n=48, L=24.0, mmax=3, solute="walk10", seed=23, rvdw=10.0, xseed=33, dk=0.01, kmax=12.0,
+                     radius=6.0),
+    "mol96_m1": dict(n=96, L=48.0, mmax=1, solute="walk12", seed=24, rvdw=10.0, xseed=34, dk=0.01, kmax=12.0,
+                     radius=6.0),
+    "mol32x128_m1": dict(n=(32, 32, 128), L=(16.0, 16.0, 64.0), mmax=1, solute="walk6", seed=25, rvdw=7.9,
+                         xseed=35, dk=0.01, kmax=14.0, radius=4.0),
+}
+
+ALL_CASES = {**CASES, **CONFIG_CASES}
+
 
 def ck_path(directory, mmax, kmax=14.0, dk=None, seed=20260000):
     if dk is None:
@@ -34,15 +52,25 @@ def ck_path(directory, mmax, kmax=14.0, dk=None, seed=20260000):
     return path
 
 
+def case_ck(directory, case):
+    """The c(k) file of a case (its mmax, and its dk and kmax where it names them)."""
+    return ck_path(directory, case["mmax"], kmax=case.get("kmax", 14.0), dk=case.get("dk"))
+
+
+def box_of(case):
+    L = case["L"]
+    return tuple(L) if not np.isscalar(L) else (L,) * 3
+
+
 def solute_of(case):
     kind = case["solute"]
     if kind == "ion":
         s = synth.ion_solute()
     elif kind.startswith("walk"):
-        s = synth.random_walk_solute(int(kind[4:]), seed=case["seed"], radius=2.0)
+        s = synth.random_walk_solute(int(kind[4:]), seed=case["seed"], radius=case.get("radius", 2.0))
     else:
         return None
-    s.xyz = synth.center_solute(s.xyz, (case["L"],) * 3)
+    s.xyz = synth.center_solute(s.xyz, box_of(case))
     return s
 
 

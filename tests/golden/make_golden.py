@@ -1,6 +1,6 @@
 """Generate tests/golden/*.npz with the FP64 CPU oracle.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [case ...]
 Each fixture stores, for one seeded case of tests/cases.py, the oracle's
 F, {F_id, F_ext, F_exc, correction}, df at 128 seeded indices, sum(df) and
 sum(df^2), and the vext checksum.  Inputs are regenerated from the seeds.
@@ -19,9 +19,9 @@ import cases  # noqa: E402
 
 
 def run_case(name, ckdir):
-    c = cases.CASES[name]
+    c = cases.ALL_CASES[name]
     sv = cases.SOLVENT
-    ck = cases.ck_path(ckdir, c["mmax"])
+    ck = cases.case_ck(ckdir, c)
     o = O.Oracle(c["n"], c["L"], c["mmax"], ck, sv.kT, sv.n0)
     sol = cases.solute_of(c)
     lj = 0.0
@@ -39,14 +39,14 @@ def run_case(name, ckdir):
                 vext_sum=vext.sum(), vext_sq=(np.minimum(vext, 1e3) ** 2).sum(), lj_tail=lj)
 
 
-def main():
+def main(names):
     out = os.path.join(ROOT, "tests", "golden")
     with tempfile.TemporaryDirectory() as ckdir:
-        for name in cases.CASES:
+        for name in names or cases.ALL_CASES:
             r = run_case(name, ckdir)
             np.savez(os.path.join(out, name + ".npz"), **r)
             print(name, r["f"], r["terms"])
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -15,10 +15,10 @@ pytestmark = pytest.mark.gpu
 SV = cases.SOLVENT
 
 
-@pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2", "rand12_m3", "mol24_m3", "rand8_m5"])
+@pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2", "rand12_m3", "mol24_m3", "rand8_m5"] + sorted(cases.CONFIG_CASES))
 def test_mixed_energy_gradient(tmp_path, name):
-    c = cases.CASES[name]
-    ck = cases.ck_path(tmp_path, c["mmax"])
+    c = cases.ALL_CASES[name]
+    ck = cases.case_ck(tmp_path, c)
     o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
     sol = cases.solute_of(c)
     if sol is not None:

@@ -1,6 +1,8 @@
 """The reference's density file: the library's writer against the restatement's parser and
 the C oracle's angl2proj, and the restart reader (proj2angl + re-grid) against the literal
 loops of read_restart_file (oracle/restart_ref.py)."""
+import struct
+
 import numpy as np
 import pytest
 
@@ -102,5 +104,17 @@ def test_restart_onto_a_larger_box_and_higher_mmax(tmp_path):
         f.write(head)
     with pytest.raises(MdftError):
         eb.read_density_bin(str(tmp_path / "short.bin"), sb, xi_start=start)
+    # a corrupt grid spacing (zero, negative, NaN, huge) is refused before any interpolation;
+    # the spacing record's data sits at bytes 72..96 (after five framed integer records)
+    with open(path, "rb") as f:
+        whole = bytearray(f.read())
+    assert struct.unpack_from("<i", whole, 68)[0] == 24
+    for bad in (0.0, -0.5, float("nan"), float("inf"), 1e300):
+        patched = bytearray(whole)
+        struct.pack_into("<d", patched, 80, bad)
+        with open(str(tmp_path / "bad_spacing.bin"), "wb") as f:
+            f.write(patched)
+        with pytest.raises(MdftError, match="spacing"):
+            eb.read_density_bin(str(tmp_path / "bad_spacing.bin"), sb, xi_start=start)
     ea.close()
     eb.close()

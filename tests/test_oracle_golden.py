@@ -11,9 +11,9 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def build(name, ckdir):
-    c = cases.CASES[name]
+    c = cases.ALL_CASES[name]
     sv = cases.SOLVENT
-    o = O.Oracle(c["n"], c["L"], c["mmax"], cases.ck_path(ckdir, c["mmax"]), sv.kT, sv.n0)
+    o = O.Oracle(c["n"], c["L"], c["mmax"], cases.case_ck(ckdir, c), sv.kT, sv.n0)
     sol = cases.solute_of(c)
     lj = o.compute_vext(sol, sv, rvdw=c["rvdw"]) if sol is not None else 0.0
     if sol is None:
@@ -22,11 +22,11 @@ def build(name, ckdir):
     return o, lj
 
 
-@pytest.mark.parametrize("name", sorted(cases.CASES))
+@pytest.mark.parametrize("name", sorted(cases.ALL_CASES))
 def test_oracle_matches_golden(tmp_path, name):
     g = np.load(os.path.join(GOLD, name + ".npz"))
     o, lj = build(name, tmp_path)
-    c = cases.CASES[name]
+    c = cases.ALL_CASES[name]
     xi = cases.xi_of(c, o.shape)
     f, df, terms = o.energy_grad(xi)
     assert abs(f - g["f"]) <= 1e-12 * abs(g["f"])
