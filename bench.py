@@ -1,16 +1,20 @@
 #!/usr/bin/env python
-"""Benchmark of the MDFT engine: solutes/s converged at 64^3, mmax 3.
+"""Benchmark of the MDFT engine: solutes/s converged at 64^3, mmax 3, in the headline form
+(mixed precision, optionally from the learned warm start) and in the plain FP64 form.
 
 Workload (one "step" = one solute solved end to end): a seeded 24-site neutral
 solute (random walk, 1.4-1.6 A bonds inside 6 A, sigma U[2.5,3.8], eps
 U[0.2,1.0], q ~ N(0,0.3) shifted to 0) in SPC/E-like 3-site water, 64^3 grid,
 32 A box, mmax 3, synthetic c(k); vext (LJ + Poisson) -> guess_density ->
-L-BFGS (m=5, stop at max|df| <= 1e-4 in FP64; the reference's F-decrease test
-is off, it stops ~1 kJ/mol short of the converged dG) -> pressure correction -> dG.
-Every run re-solves its solutes in FP64 to max|df| <= 1e-6 and reports the largest
-|dG - dG_FP64| (the metric's 0.1 kJ/mol bar).  The steps' solutes are solved through
-mdft_solve_batch on --workers engine handles (default 3), so that solves overlap
-on the GPU.  Synthetic inputs stand in for the reference's data.
+L-BFGS (m=5, stop at max|df| <= 1e-4 and |sum w df dv| <= 0.1 kJ/mol in FP64; the
+reference's F-decrease test is off, it stops ~1 kJ/mol short of the converged dG)
+-> pressure correction -> dG.  The steps' solutes are solved through mdft_solve_batch
+on --workers engine handles (default 3), so that solves overlap on the GPU; each form
+is timed over --regions regions (default 3) and the median is reported.  The plain
+FP64 form solves the same solutes on as many handles with the same stop rule; its rate
+and the ratio are in config.  Every run re-solves its solutes in FP64 to max|df| <= 1e-6
+and reports the largest |dG - dG_FP64| of both forms (the metric's 0.1 kJ/mol bar).
+Synthetic inputs stand in for the reference's data.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -44,6 +48,10 @@ CK_SEED = 20260001
 # against an FP64 solve to 1e-6 (PGTOL_REF) and reports the largest deviation.
 PGTOL = 1e-4
 PGTOL_REF = 1e-6
+# Second stop bound: |sum_{r,io} w df dv| (the gradient along a uniform change of xi), in
+# kJ/mol.  Along FP64 L-BFGS paths the dG error at a stopping point is about half of it, and
+# it converges more slowly than max|df| for small solutes.
+GUNI_TOL = 0.1
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from one ncu
 # capture of each kernel on this workload (the gather through the public API; the OZ and the
@@ -67,6 +75,10 @@ def parse():
                     help="concurrent solves per GPU (engine handles, each with its own buffers and stream)")
     ap.add_argument("--pgtol-mixed", type=float, default=0.0, help="FP32-phase stop (<=0: the final pgtol)")
     ap.add_argument("--polish", type=int, default=1, help="mixed: 1 = FP64 iterations until pgtol, 0 = one FP64 evaluation")
+    ap.add_argument("--guni-tol", type=float, default=GUNI_TOL,
+                    help="also stop only when |sum w df dv| <= this (kJ/mol); <= 0: off")
+    ap.add_argument("--regions", type=int, default=3, help="timed regions per form (the median is reported)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 form's timing")
     ap.add_argument("--solves", type=int, default=0,
                     help="profiling mode: only N solves of the workload (no timing, no reference solves)")
     ap.add_argument("--evals", type=int, default=0,
@@ -159,14 +171,14 @@ def stage_bytes(N, no, np_, c=16):
             "fft_inverse": 2 * np_ * N * c, "gather": N * (np_ * c + 3 * no * 8)}
 
 
-def cpu_oracle_eval_seconds(n, box, mmax, ck, nevals, threads):
-    """Time nevals oracle evaluations of the workload on the host cores."""
+def cpu_oracle_eval_seconds(n, box, mmax, ck, nevals, threads, seed=1000):
+    """Time nevals oracle evaluations of the workload (solute `seed`, guess density) on the host cores."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle import oracle as O
     from mdft_b200 import synth
     sv = synth.Solvent()
     o = O.Oracle(n, box, mmax, ck, sv.kT, sv.n0)
-    s = solute(1000, box)
+    s = solute(seed, box)
     o.compute_vext(s, sv, rvdw=RVDW)
     xi = o.guess_density()
     o.energy_grad(xi)  # first call
@@ -197,34 +209,68 @@ def whole_job_rate(world, steps, t_ms):
 
 
 def reference_arm(args, rank, world):
-    """CPU implementation of the path on the host cores (the C restatement; the
-    Fortran reference cannot be compiled here)."""
+    """CPU implementation of the path on the host cores (the C restatement; the Fortran
+    reference cannot be compiled here): per step one FP64 evaluation of one of the b200 arm's
+    timed solutes at its guess density, extrapolated to a solve by the FP64 evaluations per
+    solve of this workload and stop rule."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    from mdft_b200 import synth
+    sv = synth.Solvent()
     ck = ck_file(MMAX)
-    evals_per_solve = EVALS_PER_SOLVE_FP64
+    seeds = replica_seeds(0, args.warmup + args.steps)[args.warmup:]
+    cache = {}
+
+    def eval_seconds(seed):
+        if seed not in cache:  # set-up (vext, guess density) once per solute, not timed
+            o = O.Oracle(N_GRID, BOX, MMAX, ck, sv.kT, sv.n0)
+            o.compute_vext(solute(seed, BOX), sv, rvdw=RVDW)
+            cache.clear()
+            cache[seed] = (o, o.guess_density())
+        o, xi = cache[seed]
+        t0 = time.perf_counter()
+        o.energy_grad(xi)
+        return time.perf_counter() - t0
+
     times = []
     for i in range(args.warmup + args.steps):
-        t = cpu_oracle_eval_seconds(N_GRID, BOX, MMAX, ck, 1, threads)
+        t = eval_seconds(seeds[i % len(seeds)])
         if i >= args.warmup:
             times.append(t)
     t_eval = float(np.mean(times))
-    v = 1.0 / (t_eval * evals_per_solve)
-    sample = ("one FP64 energy_and_gradient per step at 64^3 mmax3 (%d threads), x %d evaluations per solve "
-              "(count of the FP64 GPU solve of the same workload)" % (threads, evals_per_solve))
+    ev = EVALS_PER_SOLVE_FP64
+    v = 1.0 / (t_eval * ev["mean"])
+    sample = ("one FP64 energy_and_gradient per step of the b200 arm's timed solutes (seeds %d..%d) at their guess "
+              "density, %d OpenMP threads, x %.1f evaluations per FP64 solve (%s); the L-BFGS vector work is not "
+              "counted" % (seeds[0], seeds[-1], threads, ev["mean"], ev["source"]))
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_eval * evals_per_solve * 1e3,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_eval * 1e3,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                      "data": "synthetic", "config": {"workload": "64^3 grid, 32 A box, mmax 3, 24-site solute, synthetic c(k)",
-                                                      "form": "CPU FP64 restatement (oracle), OpenMP"},
+                      "data": "synthetic", "config": {"workload": WORKLOAD % (N_GRID, BOX, MMAX, NSITE),
+                                                      "form": "CPU FP64 restatement (oracle), OpenMP",
+                                                      "extrapolated": "value = 1 / (per-evaluation time x evaluations "
+                                                                      "per solve); ms_per_step is the measured time "
+                                                                      "of one step's sample (one evaluation)",
+                                                      "stop": STOP_TEXT % (PGTOL, GUNI_TOL)},
                       "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
                       "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-# evaluations per FP64 solve of the bench workload (updated from the GPU run; used only
-# to scale the CPU per-evaluation time to solutes/s)
-EVALS_PER_SOLVE_FP64 = 173  # FP64 solves to max|df| <= 1e-4: 204, 168, 148 evaluations
+WORKLOAD = "%d^3 grid, %g A box, mmax %d, %d-site random-walk solute per step, synthetic c(k)"
+STOP_TEXT = ("max|df|<=%g and |sum w df dv|<=%g kJ/mol in FP64 (line-search stall accepted); dG checked against "
+             "FP64 solves to max|df|<=1e-6")
+# Evaluations per plain FP64 solve of this workload and stop rule (the mean over the bench's
+# first 20 solutes on one B200); scales the CPU evaluation time to solutes/s in the reference
+# arm, which cannot count them itself.  The b200 arm counts them in every run and reports both.
+EVALS_PER_SOLVE_FP64 = {"mean": 173.0, "key": (N_GRID, BOX, MMAX, NSITE, CK_SEED, PGTOL, 0.1),
+                        "source": "mean of 20 plain FP64 GPU solves of seeds 5..24"}
+
+
+def median(xs):
+    return float(np.median(np.asarray(xs, dtype=np.float64)))
 
 
 def main():
@@ -245,7 +291,8 @@ def main():
     rvdw = RVDW if not args.quick else 7.9
     ck = ck_file(MMAX)
     sv = synth.Solvent()
-    prec = PREC_FP64 if args.form == "fp64" else PREC_MIXED
+    W = max(1, args.workers)
+    R = max(1, args.regions)
     warm_params, warm_meta, warm_note = None, None, None
     if args.form == "learned":
         from mdft_b200 import warmstart
@@ -255,101 +302,115 @@ def main():
             warm_note = "no trained parameters in the package: solves start from the bulk guess"
     nets = []
 
-    def attach(e):
-        if warm_params is not None:
-            from mdft_b200 import warmstart
-            net = warmstart.WarmNet(n, device=local, params=warm_params)
-            e.set_warm_net(net)
-            nets.append(net)
-        return e
-
-    eng = attach(Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec))
-    stream = torch.cuda.ExternalStream(eng.stream)
-    sols = [solute(sd, box) for sd in replica_seeds(rank, args.warmup + args.steps)]
-    if args.evals:
-        # profiling mode: the same workload's evaluations at the guess density of the first solute
-        eng.compute_vext(sols[0], sv, rvdw=rvdw)
-        xi0 = eng.guess_density()
-        for _ in range(args.evals):
-            f, _, terms = eng.energy_and_gradient(xi0)
-        print(json.dumps({"evals": args.evals, "f": f, "terms": list(map(float, terms))}))
-        eng.close()
-        return
-    opts = dict(m=5, pgtol=args.pgtol, ftol_abs=-1.0, itermax=3000, precision=prec, pgtol_mixed=args.pgtol_mixed,
-                polish=args.polish)
-    if args.solves:
-        # profiling mode: N solves of the timed solutes, nothing else
-        for i in range(args.solves):
-            r = eng.solve(sols[args.warmup + i % args.steps], sv, rvdw=rvdw, **opts)
-        print(json.dumps({"solves": args.solves, "dG": r["dG"], "evaluations": r["evaluations"],
-                          "evaluations_mixed": r["evaluations_mixed"]}))
-        eng.close()
-        for net in nets:
-            net.close()
-        return
-
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- W engine handles solve the steps' solutes concurrently (mdft_solve_batch) ----
-    W = max(1, args.workers)
-    engines = [eng] + [attach(Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec))
-                       for _ in range(W - 1)]
-    streams = [torch.cuda.ExternalStream(e.stream) for e in engines]
+    def opts_of(prec):
+        return dict(m=5, pgtol=args.pgtol, ftol_abs=-1.0, itermax=3000, precision=prec, pgtol_mixed=args.pgtol_mixed,
+                    polish=args.polish, guni_tol=args.guni_tol)
 
-    def timed_batch(idx, xi_bufs=None):
-        """solve sols[idx] on the W handles; device time from an event before every stream's
-        first kernel to one after every stream's last."""
-        master = torch.cuda.current_stream()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(master)
-        for st in streams:
-            st.wait_event(ev0)
-        res = solve_batch(engines, [sols[i] for i in idx], sv, rvdw=rvdw, xi_out=xi_bufs, **opts)
-        for st in streams:
-            e = torch.cuda.Event()
-            e.record(st)
-            master.wait_event(e)
-        ev1.record(master)
-        barrier()
-        return res, ev0.elapsed_time(ev1)
+    class Form:
+        """W engine handles of one precision solving the steps' solutes concurrently."""
 
-    # ---- value: solute in, dG out; density stays in HBM ----
-    # warm-up: every handle solves at least one solute (first-solve allocations happen here)
-    warm = list(range(args.warmup))
-    solve_batch(engines, [sols[i] for i in warm], sv, rvdw=rvdw, handles=[i % W for i in warm], **opts)
-    l0 = sum(e.launch_count for e in engines)
-    barrier()
+        def __init__(self, name):
+            self.name = name
+            self.prec = PREC_FP64 if name == "fp64" else PREC_MIXED
+            self.opts = opts_of(self.prec)
+            self.engines = []
+            for _ in range(W):
+                e = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=self.prec)
+                if name == "learned" and warm_params is not None:
+                    from mdft_b200 import warmstart
+                    net = warmstart.WarmNet(n, device=local, params=warm_params)
+                    e.set_warm_net(net)
+                    nets.append(net)
+                self.engines.append(e)
+            self.streams = [torch.cuda.ExternalStream(e.stream) for e in self.engines]
+
+        def warm(self, idx):
+            # every handle solves at least one solute (first-solve allocations happen here)
+            solve_batch(self.engines, [sols[i] for i in idx], sv, rvdw=rvdw, handles=[k % W for k in range(len(idx))],
+                        **self.opts)
+            barrier()
+
+        def timed(self, idx, xi_bufs=None):
+            """solve sols[idx]; device time from an event before every stream's first kernel to
+            one after every stream's last, the slowest rank's."""
+            master = torch.cuda.current_stream()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(master)
+            for st in self.streams:
+                st.wait_event(ev0)
+            res = solve_batch(self.engines, [sols[i] for i in idx], sv, rvdw=rvdw, xi_out=xi_bufs, **self.opts)
+            for st in self.streams:
+                e = torch.cuda.Event()
+                e.record(st)
+                master.wait_event(e)
+            ev1.record(master)
+            barrier()
+            return res, max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+
+        def launches(self):
+            return sum(e.launch_count for e in self.engines)
+
+        def close(self):
+            for e in self.engines:
+                e.close()
+
+    sols = [solute(sd, box) for sd in replica_seeds(rank, args.warmup + args.steps)]
+    warm_idx = list(range(args.warmup))
     steps_idx = list(range(args.warmup, args.warmup + args.steps))
-    with Clocks(local) as clk:
-        timed, t_ms = timed_batch(steps_idx)
-    launches = sum(e.launch_count for e in engines) - l0
-    t_ms = max_over_ranks(t_ms, world, "cuda")
-    value = whole_job_rate(world, args.steps, t_ms)
-    # evaluations per solve: FP64 ones (the whole FP64 solve; the check/polish of a mixed one)
-    # plus the FP32 evaluations of a mixed solve
-    evals = [r["evaluations"] + r.get("evaluations_mixed", 0) for r in timed]
 
-    # ---- e2e: the same call with each converged density returned to pinned host memory ----
-    xi_pinned = [torch.empty(int(np.prod(eng.shape)), dtype=torch.float64, pin_memory=True) for _ in steps_idx]
-    xi_host = [b.numpy().reshape(eng.shape) for b in xi_pinned]
-    barrier()
-    _, te_ms = timed_batch(steps_idx, xi_bufs=xi_host)
-    e2e_value = whole_job_rate(world, args.steps, max_over_ranks(te_ms, world, "cuda"))
+    if args.evals or args.solves:
+        # profiling modes: N evaluations at the first solute's guess density, or N solves
+        F = Form(args.form)
+        eng = F.engines[0]
+        if args.evals:
+            eng.compute_vext(sols[0], sv, rvdw=rvdw)
+            xi0 = eng.guess_density()
+            for _ in range(args.evals):
+                f, _, terms = eng.energy_and_gradient(xi0)
+            print(json.dumps({"evals": args.evals, "f": f, "terms": list(map(float, terms))}))
+        else:
+            for i in range(args.solves):
+                r = eng.solve(sols[args.warmup + i % args.steps], sv, rvdw=rvdw, **F.opts)
+            print(json.dumps({"solves": args.solves, "dG": r["dG"], "evaluations": r["evaluations"],
+                              "evaluations_mixed": r["evaluations_mixed"], "guni": r["guni"]}))
+        F.close()
+        for net in nets:
+            net.close()
+        return
+
+    # ---- the headline form: R regions of solute in -> dG out (density resident in HBM),
+    # each followed by one region of the same call returning the densities to pinned host memory ----
+    H = Form(args.form)
+    H.warm(warm_idx)
+    xi_pinned = [torch.empty(int(np.prod(H.engines[0].shape)), dtype=torch.float64, pin_memory=True) for _ in steps_idx]
+    xi_host = [b.numpy().reshape(H.engines[0].shape) for b in xi_pinned]
+    rates, rates_e2e, launches = [], [], None
+    with Clocks(local) as clk:
+        for r in range(R):
+            l0 = H.launches()
+            timed, t_ms = H.timed(steps_idx)
+            if launches is None:
+                launches = H.launches() - l0
+            rates.append(whole_job_rate(world, args.steps, t_ms))
+            _, te_ms = H.timed(steps_idx, xi_bufs=xi_host)
+            rates_e2e.append(whole_job_rate(world, args.steps, te_ms))
+    value, e2e_value = median(rates), median(rates_e2e)
+    evals = [r["evaluations"] + r.get("evaluations_mixed", 0) for r in timed]
     s0 = sols[0]
     h2d = 8 * (4 * s0.nsite + 4 * 3 * 2)  # solute q, sig, eps, xyz + solvent sites
     d2h = xi_host[0].nbytes + 8 * 6
-
-    # ---- FP64 reference dG of the timed solutes, converged to PGTOL_REF (outside the timed regions) ----
-    ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
-    dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts, precision=PREC_FP64, pgtol=PGTOL_REF, polish=1))["dG"]
-              for i in range(args.warmup, args.warmup + args.steps)]
-    ref.close()
-    dg_err = [abs(r["dG"] - d) for r, d in zip(timed, dg_ref)]
+    warm_stats = None
+    if args.form == "learned" and warm_params is not None:
+        warm_stats = {"starts": sum(e.warm_stats()["warm_starts"] for e in H.engines),
+                      "fallbacks_to_bulk_guess": sum(e.warm_stats()["fallbacks"] for e in H.engines)}
 
     # ---- roofline of the dominant stage: per-stage CUDA events over evaluations at a converged density ----
+    eng = H.engines[0]
     xi_ref = xi_host[0].copy()
     eng.set_timing(True)
     for _ in range(5):
@@ -357,63 +418,87 @@ def main():
     st, cnt = eng.stage_times()
     eng.set_timing(False)
     per = {k: v / cnt for k, v in st.items()}
-    sb = stage_bytes(n ** 3, eng.no, eng.np, 16 if prec == PREC_FP64 else 8)
+    sb = stage_bytes(n ** 3, eng.no, eng.np, 16 if H.prec == PREC_FP64 else 8)
     dom = max(per, key=per.get)
     peak, peak_kind = measured_peak_hbm()
     achieved = sb[dom] / (per[dom] * 1e-3) / 1e9
-    traffic = NCU_TRAFFIC_BYTES.get(("fp64" if prec == PREC_FP64 else "mixed", dom)) if n == N_GRID else None
+    traffic = NCU_TRAFFIC_BYTES.get(("fp64" if H.prec == PREC_FP64 else "mixed", dom)) if n == N_GRID else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_source": peak_kind, "stage_ms": per,
-            "algorithmic_bytes": sb[dom]}
+            "traffic": traffic, "peak_source": peak_kind, "stage_ms": per, "algorithmic_bytes": sb[dom]}
+    H.close()
+
+    # ---- the plain FP64 form on the same solutes, handles and stop rule (the metric's divisor) ----
+    fp64 = None
+    if args.form != "fp64" and not args.no_compare:
+        P = Form("fp64")
+        P.warm(warm_idx)
+        rates64 = []
+        for r in range(R):
+            timed64, t64 = P.timed(steps_idx)
+            rates64.append(whole_job_rate(world, args.steps, t64))
+        P.close()
+        fp64 = {"value": median(rates64), "regions": rates64,
+                "evaluations_per_solve": [r["evaluations"] for r in timed64], "dG": [r["dG"] for r in timed64]}
+    evals64 = fp64["evaluations_per_solve"] if fp64 else evals
+
+    # ---- FP64 reference dG of the timed solutes, converged to PGTOL_REF (outside the timed regions) ----
+    ref = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=PREC_FP64)
+    dg_ref = [ref.solve(sols[i], sv, rvdw=rvdw, **dict(opts_of(PREC_FP64), pgtol=PGTOL_REF, guni_tol=0.01))["dG"]
+              for i in steps_idx]
+    ref.close()
+    dg_err = [abs(r["dG"] - d) for r, d in zip(timed, dg_ref)]
+    if fp64:
+        err64 = [abs(a - d) for a, d in zip(fp64["dG"], dg_ref)]
+        fp64["dG_error_vs_fp64_max"] = max(err64)
+        fp64["all_within_0.1"] = bool(max(err64) <= 0.1)
+        del fp64["dG"]
 
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and not args.quick:
             threads = os.cpu_count() or 1
-            te_cpu = cpu_oracle_eval_seconds(n, box, MMAX, ck, 2, threads)
-            # the CPU solve is an FP64 solve: scale by the FP64 solve's evaluation count (this
-            # run's when it timed FP64 solves, else the FP64 GPU solves' count on this workload)
-            epsolve = float(np.mean(evals)) if prec == PREC_FP64 else float(EVALS_PER_SOLVE_FP64)
+            te_cpu = cpu_oracle_eval_seconds(n, box, MMAX, ck, 2, threads, seed=replica_seeds(0, args.warmup + 1)[-1])
+            epsolve = float(np.mean(evals64))
             cpu = {"value": 1.0 / (te_cpu * epsolve), "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": "2 FP64 evaluations of the workload on the host (oracle, %d OpenMP threads) x %.1f "
-                             "evaluations per FP64 solve" % (threads, epsolve)}
+                   "sample": "2 FP64 evaluations of the first timed solute at its guess density on the host (oracle, "
+                             "%d OpenMP threads) x %.1f evaluations per FP64 solve (this run's plain FP64 GPU solves); "
+                             "the L-BFGS vector work is not counted" % (threads, epsolve)}
         clocks = clk.summary()
+        form_text = ("plain FP64 from the bulk guess" if H.prec == PREC_FP64 else
+                     ("learned warm start + " if warm_params is not None else "") +
+                     "mixed: FP32 projections, FFTs, OZ, angular transforms, ideal/external terms and "
+                     "L-BFGS vectors (BF16 history) with FP64 sums, then an FP64 check/polish")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == PREC_FP64 else "f32+f64",
+                "warmup": args.warmup, "ms_per_step": 1e3 / value * world, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if H.prec == PREC_FP64 else "f32+f64",
                 "data": "synthetic",
-                "config": {"workload": "%d^3 grid, %g A box, mmax %d, %d-site random-walk solute per step, synthetic c(k)"
-                                       % (n, box, MMAX, NSITE),
-                           "form": ("plain FP64 from the bulk guess" if prec == PREC_FP64 else
-                                    ("learned warm start + " if warm_params is not None else "") +
-                                    "mixed: FP32 projections, FFTs, OZ, angular transforms, ideal/external terms and "
-                                    "L-BFGS vectors (BF16 history) with FP64 sums, then an FP64 check/polish")
-                                   + " (vext + start + L-BFGS m=5 + pressure correction)",
+                "config": {"workload": WORKLOAD % (n, box, MMAX, NSITE),
+                           "form": form_text + " (vext + start + L-BFGS m=5 + pressure correction)",
+                           "fp64_form": fp64,
+                           "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
+                           "speedup_target": 5.0,
                            "warm_start": (
                                {"used": False, "note": "the learned warm start (--form learned) is built and trained; "
-                                                       "on held-out solutes it needs as many evaluations as the bulk "
-                                                       "guess, so this form starts from the bulk guess"}
+                                                       "this form starts from the bulk guess"}
                                if args.form == "mixed" else None) if args.form != "learned" else (
                                {"note": warm_note} if warm_params is None else
-                               {"network": "periodic 3-D conv encoder-decoder, 906772 parameters, BF16 weights",
-                                "trained": {k: warm_meta.get(k) for k in ("train", "epochs", "final_val_loss")},
-                                "starts": sum(e.warm_stats()["warm_starts"] for e in engines),
-                                "fallbacks_to_bulk_guess": sum(e.warm_stats()["fallbacks"] for e in engines)}),
-                           "stop": "max|df|<=%g in FP64 (line-search stall accepted); dG checked against FP64 "
-                                   "solves to max|df|<=%g" % (args.pgtol, PGTOL_REF),
+                               dict({"network": "periodic 3-D conv encoder-decoder, BF16 weights",
+                                     "trained": {k: warm_meta.get(k) for k in ("train", "epochs", "final_val_loss")}},
+                                    **warm_stats)),
+                           "stop": STOP_TEXT % (args.pgtol, args.guni_tol),
                            "l2": "inputs larger than L2 (176 MB per field)",
                            "parallelism": ("replicas" if world > 1 else "single GPU") + ", %d concurrent solves per GPU" % W,
                            "workers": W,
+                           "regions": {"value": rates, "e2e": rates_e2e, "statistic": "median of %d timed regions" % R},
                            "evaluations_per_solve": evals,
                            "fp32_evaluations_per_solve": [r.get("evaluations_mixed", 0) for r in timed],
                            "fp64_evaluations_per_solve": [r["evaluations"] for r in timed],
+                           "evals_per_fp64_solve_constant": EVALS_PER_SOLVE_FP64["mean"],
                            "dG": [r["dG"] for r in timed], "dG_fp64": dg_ref,
                            "dG_error_vs_fp64_max": max(dg_err), "all_within_0.1": bool(max(dg_err) <= 0.1)},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line))
-    for e in engines:
-        e.close()
     for net in nets:
         net.close()
     if world > 1:

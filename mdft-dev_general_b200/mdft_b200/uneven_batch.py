@@ -3,8 +3,9 @@
 64 seeded solutes of 1-40 sites (random walk as the 24-site workload), each on a grid drawn
 from {32, 48, 64, 96}^3 with a box of 0.5 A x nodes and an mmax drawn from {1, 3}.  One
 engine handle per (grid, mmax); each solute is pinned to its handle and mdft_solve_batch runs
-the handles' solves concurrently.  Reported: aggregate solutes/s (wall clock around the
-batch call) and each solute's |dG - dG_FP64|, the FP64 solve to max|df| <= 1e-6 from the
+the handles' solves concurrently.  Stop rule: max|df| <= 1e-4 and |sum w df dv| <= 0.1 kJ/mol.
+Reported: aggregate solutes/s (wall clock around the batch call) and each solute's
+|dG - dG_FP64|, the FP64 solve to max|df| <= 1e-6 (and |sum w df dv| <= 0.01) from the
 bulk guess being the reference.  rvdw is 7.9 A for every solute: the 16 A box of the 32^3
 grid allows at most 8 A (src/module_lennardjones.f90:55-59).
 
@@ -47,7 +48,7 @@ def solutes_of(plan):
     return sols
 
 
-def run(plan, ck_dir, precision, pgtol, solvent, workers_per_combo=1):
+def run(plan, ck_dir, precision, pgtol, solvent, workers_per_combo=1, guni_tol=0.0):
     combos = sorted({(n, m) for _, _, n, m in plan})
     ck = {}
     for m in MMAXES:
@@ -70,7 +71,7 @@ def run(plan, ck_dir, precision, pgtol, solvent, workers_per_combo=1):
         count[(n, m)] = k + 1
     t0 = time.perf_counter()
     res = E.solve_batch(engines, sols, solvent, rvdw=RVDW, m=5, pgtol=pgtol, ftol_abs=-1.0, itermax=5000,
-                        precision=precision, handles=handles)
+                        precision=precision, handles=handles, guni_tol=guni_tol)
     wall = time.perf_counter() - t0
     for e in engines:
         e.close()
@@ -81,6 +82,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--solutes", type=int, default=64)
     ap.add_argument("--pgtol", type=float, default=1e-4)
+    ap.add_argument("--guni-tol", type=float, default=0.1,
+                    help="also stop only when |sum w df dv| <= this (kJ/mol; <= 0: off)")
     ap.add_argument("--workers-per-grid", type=int, default=1)
     ap.add_argument("--forms", default="mixed,fp64", help="forms to time, comma-separated: mixed, fp64")
     ap.add_argument("--report", default=None)
@@ -92,8 +95,8 @@ def main(argv=None):
     out = {}
     for f in forms:
         prec = E.PREC_MIXED if f == "mixed" else E.PREC_FP64
-        out[f] = run(plan, d, prec, a.pgtol, solvent, a.workers_per_grid)
-    ref, t_ref = run(plan, d, E.PREC_FP64, 1e-6, solvent, a.workers_per_grid)
+        out[f] = run(plan, d, prec, a.pgtol, solvent, a.workers_per_grid, a.guni_tol)
+    ref, t_ref = run(plan, d, E.PREC_FP64, 1e-6, solvent, a.workers_per_grid, 0.01)
     rows = []
     for i, (seed, nsite, n, m) in enumerate(plan):
         row = dict(seed=seed, nsite=nsite, n=n, mmax=m, dG_fp64=ref[i]["dG"])
@@ -103,6 +106,7 @@ def main(argv=None):
                         f + "_status": x["status"]})
         rows.append(row)
     summ = dict(solutes=len(plan), handles=len({(n, m) for _, _, n, m in plan}) * a.workers_per_grid, pgtol=a.pgtol,
+                guni_tol=a.guni_tol,
                 rvdw=RVDW, wall_s=dict({f: out[f][1] for f in forms}, fp64_ref_1e6=t_ref))
     for f in forms:
         errs = [abs(r[f + "_err"]) for r in rows]
