@@ -23,6 +23,7 @@
 #include "k_gather_tma.cuh"
 #include "k_ozp.cuh"
 #include "k_project_tma.cuh"
+#include "k_angular_umma.cuh"
 #include "k_vext.cuh"
 
 namespace mdft {
@@ -86,6 +87,13 @@ struct mdft_handle {
     DevBuf<int> oz_ints;
     DevBuf<double> oz_dbls;
     int oz_grid = 0, oz_warps = 8, oz_grid32 = 0, oz_warps32 = 8;
+    // FP32 evaluations: angular contractions on the tensor cores (k_project_umma,
+    // k_gather_umma), with the packed split-BF16 images of A^T and B^T
+    bool um_ok = false;
+    UmmaShape um_ps{}, um_gs{};
+    DevBuf<uint16_t> um_pimg, um_gimg;
+    int um_grid_p = 0, um_grid_g = 0;
+    bool ring_p = false, ring_g = false;  // FP32 phase: the bulk-copy ring forms (one CTA per SM)
     bool ozp_ok = false;  // FP32 evaluations use the thread-per-pair k_ozp
     OzpParams ozp{};
     DevBuf<float2> ozp_cq;  // c interpolated at every |q|^2 of a cubic grid (empty: interpolate per pair)
@@ -148,6 +156,36 @@ int upload_twiddles(DevBuf<double2> &buf, int n) {
     int rc = alloc_check(buf.alloc(n), "fft twiddles", n * sizeof(double2));
     if (rc) return rc;
     return check_cuda(cudaMemcpy(buf.p, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice), "twiddle upload");
+}
+
+// BF16 bits of an FP32 value, rounded to nearest even (finite inputs)
+uint16_t bf16_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+float bf16_value(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+// hi and lo BF16 images (hi then lo) of an [Rp][Kp] operand in the packed tcgen05 layout;
+// value(r, k) is the FP64 entry (0 in the padding)
+template <typename F>
+void pack_split_bf16(int Rp, int Kp, F value, std::vector<uint16_t> &img) {
+    const size_t half = (size_t)Rp * Kp;
+    img.assign(2 * half, 0);
+    for (int r = 0; r < Rp; ++r)
+        for (int k = 0; k < Kp; ++k) {
+            const double v = value(r, k);
+            const uint16_t hi = bf16_bits((float)v);
+            const uint16_t lo = bf16_bits((float)(v - (double)bf16_value(hi)));
+            const size_t off = umma::elem_offset(r, k, Kp, 2) / 2;
+            img[off] = hi;
+            img[half + off] = lo;
+        }
 }
 
 int pick_tl(long long lines_divisor, int n) {
@@ -368,11 +406,30 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     for (int ax = 0; ax < 3; ++ax) tw[ax] = dbl ? (const void *)h->tw64[ax].p : (const void *)h->tw32[ax].p;
     stage_mark(h, 0);
     AngularArgs aa{g.N, g.no, g.np, g.rho0};
-    if (x32 && (dbl || !h->pt_ok32 || !h->vext32.p || ((uintptr_t)xin & 15u) != 0)) {
+    if (x32 && (dbl || (!h->pt_ok32 && !h->um_ok) || !h->vext32.p || ((uintptr_t)xin & 15u) != 0)) {
         set_error("an FP32 point needs the FP32 bulk-copy kernels");
         return MDFT_E_STATE;
     }
-    if (x32) {
+    const bool umma = !dbl && h->um_ok;
+    if (umma) {
+        // tensor-core projection (split BF16); FP32 point in the FP32 phase, else the FP64 xi
+        const int ntiles = (int)(g.N / kUmBM);
+        const unsigned grid = (unsigned)std::min(ntiles, h->um_grid_p);
+        const size_t smem = umma_smem_bytes(h->um_ps);
+        const bool vec = g.no % 4 == 0 && ((uintptr_t)xin & 15u) == 0;
+        if (x32 && h->ring_p) {
+            const unsigned rgrid = (unsigned)std::min(ntiles, h->nsm);
+            const size_t rsmem = project_ring_smem_bytes(h->um_ps, g.no);
+            if (vec) k_project_ring<4><<<rgrid, kRingThreads, rsmem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            else k_project_ring<1><<<rgrid, kRingThreads, rsmem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+        } else if (x32) {
+            if (vec) k_project_umma<float, 4><<<grid, kUmThreads, smem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            else k_project_umma<float, 1><<<grid, kUmThreads, smem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+        } else {
+            if (vec) k_project_umma<double, 4><<<grid, kUmThreads, smem, h->stream>>>(d_xi, h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            else k_project_umma<double, 1><<<grid, kUmThreads, smem, h->stream>>>(d_xi, h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+        }
+    } else if (x32) {
         const int ntiles = (int)(g.N / kPtBM);
         k_project_tma<float, float><<<std::min(ntiles, h->pt_grid_x32), 256, project_tma_smem_bytes<float, float>(g.np, g.no), h->stream>>>(
             static_cast<const float *>(xin), (const float *)A, (float2 *)planes, h->kerr.p, aa, ntiles);
@@ -418,11 +475,39 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     auto al16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
     long long red_blocks = h->nblk_gather;
     const bool tma_gather = gt_ncol > 0 && ga.df_mode != 2 && al16(d_xi) && al16(dvec);
-    if ((vec32 || x32) && !tma_gather) {
+    const bool umma_gather = umma && ga.df_mode != 2;
+    if ((vec32 || x32) && !tma_gather && !umma_gather) {
         set_error("FP32 gradient vectors need the bulk-copy gather");
         return MDFT_E_STATE;
     }
-    if (tma_gather) {
+    if (umma_gather) {
+        // tensor-core gather (split BF16) with the FP32 element-wise epilogue
+        const int ntiles = (int)(g.N / kUmBM);
+        const int grid = std::min(ntiles, h->um_grid_g);
+        const size_t smem = gather_umma_smem_bytes(h->um_gs, g.no);
+        const float2 *pl = (const float2 *)planes;
+        // 4-element vector epilogue with a compile-time orientation count (mmax 3, water), else scalar
+        const bool v84 = g.no == 84 && al16(xin) && al16(dvec) && al16(d_df);
+        float *df32 = reinterpret_cast<float *>(d_df);
+        const float *x32p = static_cast<const float *>(xin);
+        if (x32 && v84 && h->ring_g) {
+            const int rgrid = std::min(ntiles, h->nsm);
+            k_gather_ring<84><<<rgrid, kRingThreads, gather_ring_smem_bytes(h->um_gs, 84), h->stream>>>(pl, h->um_gimg.p, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+            red_blocks = rgrid;
+        } else if (x32 && v84)
+            k_gather_umma<float, float, 84><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+        else if (x32)
+            k_gather_umma<float, float, 0><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+        else if (vec32 && v84)
+            k_gather_umma<double, float, 84><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+        else if (vec32)
+            k_gather_umma<double, float, 0><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+        else if (v84)
+            k_gather_umma<double, double, 84><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+        else
+            k_gather_umma<double, double, 0><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
+        if (!(x32 && v84 && h->ring_g)) red_blocks = grid;
+    } else if (tma_gather) {
         const int ntiles = (int)(g.N / gt_bm<T>());
         const int grid = std::min(ntiles, h->nsm * (dbl ? 1 : 2));
         const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
@@ -653,7 +738,53 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
             if ((rc = allow_smem(fn, maxsmem))) return rc;
     }
     {
-        const size_t rows = std::max<long long>(h->nblk_gather, 2 * h->nsm);
+        // tensor-core angular contractions for FP32 evaluations: N in whole 128-point tiles,
+        // no <= 96, 2np <= 64 (mmax <= 3 for water); MDFT_ANGULAR=ffma keeps the FFMA kernels
+        const char *ang = std::getenv("MDFT_ANGULAR");
+        const bool want = !(ang && std::strcmp(ang, "ffma") == 0);
+        // "umma": register forms only; "ring": the bulk-copy ring forms of both contractions;
+        // default: register projection (measured faster) and ring gather
+        const bool want_ring = !(ang && std::strcmp(ang, "umma") == 0);
+        const bool want_ring_p = ang && std::strcmp(ang, "ring") == 0;
+        h->um_ps = umma_shape(g.no, 2 * g.np);
+        h->um_gs = umma_shape(2 * g.np, g.no);
+        if (want && g.N % kUmBM == 0 && h->um_ps.Kp <= 96 && h->um_gs.Kp <= 64 &&
+            gather_umma_smem_bytes(h->um_gs, g.no) <= dyn_max && umma_smem_bytes(h->um_ps) <= dyn_max) {
+            std::vector<uint16_t> pimg, gimg;
+            const int np2 = 2 * g.np, no = g.no;
+            pack_split_bf16(h->um_ps.Np, h->um_ps.Kp, [&](int n, int io) { return (n < np2 && io < no) ? A[(size_t)io * np2 + n] : 0.0; }, pimg);
+            pack_split_bf16(h->um_gs.Np, h->um_gs.Kp, [&](int io, int k) { return (io < no && k < np2) ? B[(size_t)k * no + io] : 0.0; }, gimg);
+            if ((rc = alloc_check(h->um_pimg.alloc(pimg.size()), "angular operand images", pimg.size() * 2))) return rc;
+            if ((rc = alloc_check(h->um_gimg.alloc(gimg.size()), "angular operand images", gimg.size() * 2))) return rc;
+            cudaMemcpy(h->um_pimg.p, pimg.data(), pimg.size() * 2, cudaMemcpyHostToDevice);
+            cudaMemcpy(h->um_gimg.p, gimg.data(), gimg.size() * 2, cudaMemcpyHostToDevice);
+            const void *pf[] = {(const void *)k_project_umma<float, 4>, (const void *)k_project_umma<float, 1>,
+                                (const void *)k_project_umma<double, 4>, (const void *)k_project_umma<double, 1>};
+            const void *gf[] = {(const void *)k_gather_umma<float, float, 84>, (const void *)k_gather_umma<double, float, 84>,
+                                (const void *)k_gather_umma<double, double, 84>, (const void *)k_gather_umma<float, float, 0>,
+                                (const void *)k_gather_umma<double, float, 0>, (const void *)k_gather_umma<double, double, 0>};
+            for (const void *fn : pf)
+                if ((rc = allow_smem(fn, maxsmem))) return rc;
+            for (const void *fn : gf)
+                if ((rc = allow_smem(fn, maxsmem))) return rc;
+            int bp = 0, bg = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_project_umma<float, 4>, kUmThreads, umma_smem_bytes(h->um_ps));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bg, k_gather_umma<float, float, 84>, kUmThreads,
+                                                          gather_umma_smem_bytes(h->um_gs, g.no));
+            h->um_grid_p = h->nsm * std::max(1, bp);
+            h->um_grid_g = h->nsm * std::max(1, bg);
+            h->um_ok = true;
+            h->ring_p = want_ring_p && project_ring_smem_bytes(h->um_ps, g.no) <= dyn_max;
+            h->ring_g = want_ring && g.no == 84 && gather_ring_smem_bytes(h->um_gs, 84) <= dyn_max;
+            if (h->ring_p) {
+                if ((rc = allow_smem((const void *)k_project_ring<4>, maxsmem))) return rc;
+                if ((rc = allow_smem((const void *)k_project_ring<1>, maxsmem))) return rc;
+            }
+            if (h->ring_g && (rc = allow_smem((const void *)k_gather_ring<84>, maxsmem))) return rc;
+        }
+    }
+    {
+        const size_t rows = std::max<long long>({h->nblk_gather, 2LL * h->nsm, (long long)h->um_grid_g});
         if ((rc = alloc_check(h->partial.alloc(kGatherSums * rows), "partials", 8 * kGatherSums * rows))) return rc;
     }
     if ((rc = alloc_check(h->kerr.alloc(1), "error flag", 4))) return rc;
@@ -727,6 +858,8 @@ int mdft_destroy(mdft_handle *h) {
     if (h->warm) mdft_warm_net_set_stream(h->warm, nullptr);
     h->warm = nullptr;
     h->ozp_cq.free();
+    h->um_pimg.free();
+    h->um_gimg.free();
     h->xi.free(); h->vext.free(); h->vext32.free(); h->df.free(); h->w.free(); h->A.free(); h->B.free();
     h->partial.free(); h->sums.free(); h->planes.free(); h->ctab.free(); h->oz_ints.free(); h->oz_dbls.free();
     for (int i = 0; i < 3; ++i) {

@@ -49,3 +49,67 @@ def test_mixed_solve_free_energy(tmp_path, name):
     assert abs(r32["dG"] - r64["dG"]) <= 0.1, (r32, r64)
     e64.close()
     e32.close()
+
+
+@pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2", "mol24_m3", "mol8_m0", "ion32_m1", "mol64_m3"])
+def test_tensor_core_angular_transforms(tmp_path, name, monkeypatch):
+    # The FP32 evaluation with the angular contractions on the tensor cores (split BF16:
+    # hi*hi + hi*lo + lo*hi, FP32 accumulation) against the same evaluation with the FP32
+    # FFMA kernels (MDFT_ANGULAR=ffma) and against the FP64 oracle.  Bars: the excess term
+    # within 2e-5 of |F_exc| of the oracle's, the total within 2e-6 of |F|, the gradient within
+    # 1e-4 of max|df| (the mixed path's bars); the two FP32 forms within 2e-5 of |F_exc|.
+    c = cases.ALL_CASES[name]
+    ck = cases.case_ck(tmp_path, c)
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    sol = cases.solute_of(c)
+    o.compute_vext(sol, SV, rvdw=c["rvdw"])
+    monkeypatch.setenv("MDFT_ANGULAR", "ffma")
+    e0 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    monkeypatch.delenv("MDFT_ANGULAR")
+    e1 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    for e in (e0, e1):
+        e.set_vext(o.get_vext())
+    xi = cases.xi_of(c, o.shape)
+    fo, dfo, to = o.energy_grad(xi)
+    f0, df0, t0 = e0.energy_and_gradient(xi)
+    f1, df1, t1 = e1.energy_and_gradient(xi)
+    w = e1.weights
+    rho = xi ** 2 * e1.rho0
+    dfid = np.where(rho > np.finfo(float).eps, w * 2 * e1.rho0 * xi * (SV.kT * np.log(rho / e1.rho0) + o.get_vext()), 0.0)
+    exc_o, exc1 = dfo - dfid, df1 - dfid
+    rel_exc = abs(t1[2] - to[2]) / abs(to[2])
+    print("\n%s: F_exc rel err umma %.3e ffma %.3e; F rel err umma %.3e; excess df err / max umma %.3e ffma %.3e"
+          % (name, rel_exc, abs(t0[2] - to[2]) / abs(to[2]), abs(f1 - fo) / abs(fo),
+             np.abs(exc1 - exc_o).max() / np.abs(exc_o).max(), np.abs(df0 - dfid - exc_o).max() / np.abs(exc_o).max()))
+    assert rel_exc <= 2e-5, (t1, to)
+    assert abs(t1[2] - t0[2]) <= 2e-5 * abs(to[2]), (t1, t0)
+    assert abs(f1 - fo) <= 2e-6 * abs(fo)
+    assert np.abs(df1 - dfo).max() <= 1e-4 * np.abs(dfo).max()
+    e0.close()
+    e1.close()
+
+
+@pytest.mark.parametrize("mode", ["ffma", "umma", "ring"])
+def test_tensor_core_forms_in_a_mixed_solve(tmp_path, mode, monkeypatch):
+    # The FP32 phase of a mixed solve (FP32 point, vext, gradient and direction) with each form
+    # of the angular contractions: FFMA kernels, the tensor-core register forms, and the
+    # tensor-core bulk-copy ring forms (the default at 24^3, no = 84).  Each solve's dG is
+    # within 0.1 kJ/mol of the FP64 solve of the same solute (the metric's bar).
+    c = cases.ALL_CASES["mol24_m3"]
+    ck = cases.case_ck(tmp_path, c)
+    sol = cases.solute_of(c)
+    e64 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    r64 = e64.solve(sol, SV, rvdw=c["rvdw"], m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, guni_tol=0.01)
+    e64.close()
+    if mode == "ring":
+        monkeypatch.delenv("MDFT_ANGULAR", raising=False)
+    else:
+        monkeypatch.setenv("MDFT_ANGULAR", mode)
+    e32 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    r32 = e32.solve(sol, SV, rvdw=c["rvdw"], m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=3000, precision=PREC_MIXED,
+                    guni_tol=0.1)
+    print("\n%s: dG %.6f (FP64 %.6f), FP32 evaluations %d, FP64 %d, status %d"
+          % (mode, r32["dG"], r64["dG"], r32["evaluations_mixed"], r32["evaluations"], r32["status"]))
+    assert r32["evaluations_mixed"] > 0
+    assert abs(r32["dG"] - r64["dG"]) <= 0.1, (r32, r64)
+    e32.close()
