@@ -327,6 +327,12 @@ int mdft_warm_net_train_step(mdft_warm_net *net, const float *const *d_in, const
 int mdft_warm_net_take_loss(mdft_warm_net *net, double *mean_loss);
 int mdft_warm_net_launch_count(const mdft_warm_net *net, long long *count);
 int mdft_warm_net_grid(const mdft_warm_net *net, int *nxyz);
+/* A network with nout output channels (1..256): 4 is the m <= 1 form above; 2 np gives the
+ * real and imaginary parts of all np complex projections of the log-density on a handle's
+ * angular grid, in the order of the reference's angl2proj
+ * (src/module_orientation_projection_transform.f90:159-199). */
+int mdft_warm_net_create_n(int nx, int ny, int nz, int nout, int device, mdft_warm_net **out);
+int mdft_warm_net_num_outputs(const mdft_warm_net *net, int *nout);
 
 /* The network's 3 input channels for a solute on h's grid (sites as in mdft_solve). */
 int mdft_warm_features(mdft_handle *h, int nsite, const double *q, const double *sig, const double *eps, const double *xyz,
@@ -337,8 +343,14 @@ int mdft_warm_features(mdft_handle *h, int nsite, const double *q, const double 
 int mdft_warm_target(mdft_handle *h, const double *d_xi, float *d_target, float *d_mask);
 /* Starting density from 4 x N projections (d_xi device; NULL: the handle's solver point). */
 int mdft_warm_expand(mdft_handle *h, const float *d_pred, double *d_xi);
+/* Target and start of either output form: nout = 4 as above, or nout = 2 np (the log-density's
+ * complex projections by the handle's angl2proj as real and imaginary planes; the start is
+ * their proj2angl, src/module_orientation_projection_transform.f90:202-243, clamped and
+ * exponentiated as in the m <= 1 form). */
+int mdft_warm_target_n(mdft_handle *h, const double *d_xi, int nout, float *d_target, float *d_mask);
+int mdft_warm_expand_n(mdft_handle *h, const float *d_pred, int nout, double *d_xi);
 /* Make mdft_solve (and mdft_solve_batch on this handle) start from the network's
- * prediction instead of guess_density; NULL restores the bulk guess.  A warm-started
+ * prediction instead of guess_density (either output form); NULL restores the bulk guess.  A warm-started
  * solve that ends in a line-search failure or at the iteration limit is redone from the
  * bulk guess.  The network must be built for the handle's grid; while attached it runs on
  * the handle's stream (detaching, or mdft_destroy of the handle, returns it to its own).

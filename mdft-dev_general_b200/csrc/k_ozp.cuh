@@ -22,6 +22,10 @@
 namespace mdft {
 
 constexpr int kOzpThreads = 128;
+#ifndef MDFT_OZP_MIN_BLOCKS
+#define MDFT_OZP_MIN_BLOCKS 1
+#endif
+constexpr int kOzpMinBlocks = MDFT_OZP_MIN_BLOCKS;  // resident CTAs asked of the register allocator
 constexpr int kOzpMaxNp = 64;
 constexpr int kOzpMaxRec = 48;
 
@@ -82,7 +86,7 @@ __device__ __forceinline__ void ozp_fmac(float2 &acc, float2 a, float2 b) {  // 
 }
 
 template <int MM, int MR>
-__global__ void __launch_bounds__(kOzpThreads) k_ozp(float2 *__restrict__ planes, const float2 *__restrict__ ctab, Oz2Args a,
+__global__ void __launch_bounds__(kOzpThreads, kOzpMinBlocks) k_ozp(float2 *__restrict__ planes, const float2 *__restrict__ ctab, Oz2Args a,
                                                      OzpParams pp, const float2 *__restrict__ cq) {
     using S = OzShape<MM, MR>;
     constexpr int NP = S::np();

@@ -1,6 +1,7 @@
 // Warm-start network: a periodic 3-D convolutional encoder-decoder that maps a solute's
-// potential channels (3 x N) to the m <= 1 projections of the converged log-density
-// (4 x N).  Forward, backward and Adam run on the device with the kernels of
+// potential channels (3 x N) to projections of the converged log-density: the 4 m <= 1
+// real-basis projections (nout = 4), or the real and imaginary parts of all np complex
+// projections of the solver's angular grid (nout = 2 np).  Forward, backward and Adam run on the device with the kernels of
 // k_warmnet.cuh; the host here owns the parameters, the activation buffers and the
 // launch order.  There is no counterpart in the reference (it always starts from the
 // bulk guess, src/module_density.f90:267-284).
@@ -13,8 +14,9 @@
 //   u2 up 128->64 + e2, c2 conv3 64->64        level 2    (up: linear, then the skip add)
 //   u1 up 64->32 + e1, c1 conv3 32->32         level 1
 //   u0 up 32->16 + e0b, c0 conv3 16->16        level 0
-//   head conv1 16->4 (linear)
-// 906,772 parameters (weights and biases), BF16 in the kernels, FP32 master copy for Adam.
+//   head conv1 16->nout (linear)
+// 906,772 parameters at nout = 4 (weights and biases), BF16 in the kernels, FP32 master
+// copy for Adam.
 #include "../../include/mdft_b200.h"
 
 #include <cmath>
@@ -47,6 +49,13 @@ const LayerSpec kLayers[kNL] = {
 
 int kvol(int kind) { return kind == kConv3 ? 27 : (kind == kHead ? 1 : 8); }
 long long nweights(const LayerSpec &L) { return (long long)L.cin * L.cout * kvol(L.kind); }
+// the layer and tensor tables with the network's own output count in the head
+LayerSpec layer_of(int nout, int l) {
+    LayerSpec L = kLayers[l];
+    if (L.kind == kHead) L.cout = nout;
+    return L;
+}
+int channels_of(int nout, int t) { return t == kNT - 1 ? nout : kTensors[t].c; }
 
 int cuda_rc(cudaError_t e, const char *what) {
     if (e == cudaSuccess) return MDFT_OK;
@@ -96,6 +105,7 @@ struct Rng {
 struct mdft_warm_net {
     int device = 0;
     int nx = 0, ny = 0, nz = 0;
+    int nout = 4;  // output channels (head width)
     cudaStream_t stream = nullptr;
     cudaStream_t own = nullptr;
     long long nparam = 0;
@@ -113,6 +123,8 @@ struct mdft_warm_net {
 
     Vol vol(int level) const { return Vol{nz >> level, ny >> level, nx >> level}; }
     long long nvox(int level) const { return vol(level).n(); }
+    LayerSpec layer(int l) const { return layer_of(nout, l); }
+    int channels(int t) const { return channels_of(nout, t); }
 };
 
 namespace {
@@ -144,7 +156,7 @@ const float *tensor_in(mdft_warm_net *net, int t, const float *in) { return t ==
 void forward(mdft_warm_net *net, const float *in) {
     const __nv_bfloat16 *P = net->pb.p;
     for (int l = 0; l < kNL; ++l) {
-        const LayerSpec &L = kLayers[l];
+        const LayerSpec L = net->layer(l);
         const int lx = kTensors[L.x].level, ly = kTensors[L.y].level;
         const float *x = tensor_in(net, L.x, in);
         float *out = L.gelu ? net->z[l].p : net->act[L.y].p;
@@ -175,13 +187,13 @@ void backward(mdft_warm_net *net, const float *in, const float *target, const fl
     for (int t = 1; t < kNT - 1; ++t) cudaMemsetAsync(net->grad[t].p, 0, net->grad[t].bytes(), st);
     const long long nv0 = net->nvox(0);
     const int nblk = 296;
-    k_mse<<<nblk, 256, 0, st>>>(net->act[kNT - 1].p, target, mask, net->grad[kNT - 1].p, net->lpart.p, 4, nv0,
-                                (float)(1.0 / (4.0 * (double)nv0)));
+    k_mse<<<nblk, 256, 0, st>>>(net->act[kNT - 1].p, target, mask, net->grad[kNT - 1].p, net->lpart.p, net->nout, nv0,
+                                (float)(1.0 / ((double)net->nout * (double)nv0)));
     k_sum_into<<<1, 256, 0, st>>>(net->lpart.p, nblk, net->lacc.p);
     net->launches += 2;
     float *G = net->g.p;
     for (int l = kNL - 1; l >= 0; --l) {
-        const LayerSpec &L = kLayers[l];
+        const LayerSpec L = net->layer(l);
         const int lx = kTensors[L.x].level, ly = kTensors[L.y].level;
         const Vol vx = net->vol(lx), vy = net->vol(ly);
         float *gy = net->grad[L.y].p;
@@ -231,12 +243,12 @@ int ensure_train(mdft_warm_net *net) {
     cudaMemsetAsync(net->m.p, 0, n * 4, net->stream);
     cudaMemsetAsync(net->v.p, 0, n * 4, net->stream);
     for (int t = 1; t < kNT; ++t) {
-        const size_t c = (size_t)kTensors[t].c * net->nvox(kTensors[t].level);
+        const size_t c = (size_t)net->channels(t) * net->nvox(kTensors[t].level);
         if ((rc = cuda_rc(net->grad[t].alloc(c), "activation gradients"))) return rc;
     }
     long long cap = 1;
     for (int l = 0; l < kNL; ++l) {
-        const LayerSpec &L = kLayers[l];
+        const LayerSpec L = net->layer(l);
         int ns;
         long long per;
         const int K3 = kvol(L.kind);
@@ -266,8 +278,13 @@ int check_net(const mdft_warm_net *net) {
 extern "C" {
 
 int mdft_warm_net_create(int nx, int ny, int nz, int device, mdft_warm_net **out) {
+    return mdft_warm_net_create_n(nx, ny, nz, 4, device, out);
+}
+
+int mdft_warm_net_create_n(int nx, int ny, int nz, int nout, int device, mdft_warm_net **out) {
     if (!out) { set_error("null argument"); return MDFT_E_ARG; }
     *out = nullptr;
+    if (nout < 1 || nout > 256) { set_error("warm-start network outputs %d: must be in [1, 256]", nout); return MDFT_E_ARG; }
     if (nx < 8 || ny < 8 || nz < 8 || nx % 8 || ny % 8 || nz % 8) {
         set_error("warm-start network grid %dx%dx%d: every dimension must be a multiple of 8", nx, ny, nz);
         return MDFT_E_ARG;
@@ -277,12 +294,13 @@ int mdft_warm_net_create(int nx, int ny, int nz, int device, mdft_warm_net **out
     mdft_warm_net *net = new mdft_warm_net;
     net->device = device;
     net->nx = nx; net->ny = ny; net->nz = nz;
+    net->nout = nout;
     long long off = 0;
     for (int l = 0; l < kNL; ++l) {
         net->woff[l] = off;
-        off += nweights(kLayers[l]);
+        off += nweights(net->layer(l));
         net->boff[l] = off;
-        off += kLayers[l].cout;
+        off += net->layer(l).cout;
     }
     net->nparam = off;
     auto fail = [&](int r) { delete net; return r; };
@@ -293,12 +311,12 @@ int mdft_warm_net_create(int nx, int ny, int nz, int device, mdft_warm_net **out
     cudaMemsetAsync(net->p.p, 0, (size_t)off * 4, net->stream);
     cudaMemsetAsync(net->pb.p, 0, (size_t)off * 2, net->stream);
     for (int t = 1; t < kNT; ++t) {
-        const size_t c = (size_t)kTensors[t].c * net->nvox(kTensors[t].level);
+        const size_t c = (size_t)net->channels(t) * net->nvox(kTensors[t].level);
         if ((rc = cuda_rc(net->act[t].alloc(c), "activations"))) return fail(rc);
     }
     for (int l = 0; l < kNL; ++l)
         if (kLayers[l].gelu) {
-            const size_t c = (size_t)kLayers[l].cout * net->nvox(kTensors[kLayers[l].y].level);
+            const size_t c = (size_t)net->layer(l).cout * net->nvox(kTensors[kLayers[l].y].level);
             if ((rc = cuda_rc(net->z[l].alloc(c), "pre-activations"))) return fail(rc);
         }
     if ((rc = cuda_rc(net->lacc.alloc(1), "loss"))) return fail(rc);
@@ -372,7 +390,7 @@ int mdft_warm_net_init(mdft_warm_net *net, unsigned long long seed) {
     std::vector<float> h((size_t)net->nparam, 0.f);
     Rng r{seed};
     for (int l = 0; l < kNL; ++l) {
-        const LayerSpec &L = kLayers[l];
+        const LayerSpec L = net->layer(l);
         // He-normal: fan-in = the inputs one output sums (the coarse channels for up-sampling)
         const double fan = L.kind == kUp ? (double)L.cin : (double)L.cin * kvol(L.kind);
         const double sd = (L.kind == kHead ? 0.1 : 1.0) * std::sqrt((L.kind == kHead ? 1.0 : 2.0) / fan);
@@ -463,6 +481,14 @@ int mdft_warm_net_launch_count(const mdft_warm_net *net, long long *count) {
     if (rc) return rc;
     if (!count) { set_error("null argument"); return MDFT_E_ARG; }
     *count = net->launches;
+    return MDFT_OK;
+}
+
+int mdft_warm_net_num_outputs(const mdft_warm_net *net, int *nout) {
+    int rc = check_net(net);
+    if (rc) return rc;
+    if (!nout) { set_error("null argument"); return MDFT_E_ARG; }
+    *nout = net->nout;
     return MDFT_OK;
 }
 

@@ -16,6 +16,11 @@
 // exact projections for the Gauss-Legendre x uniform-phi quadrature of mmax >= 1.  The
 // complex projections p(m <= 1, mu', mu = 0) of the reference's angl2proj
 // (src/module_orientation_projection_transform.f90:159-199) span the same functions.
+// Projection form (networks with nout = 2 np): target [2 np][N] = the real and imaginary
+// parts of the np complex projections of the same clamped f with the handle's angl2proj
+// matrix A (src/module_orientation_projection_transform.f90:159-199), in the reference's
+// projection order; the start expands a prediction with the handle's proj2angl matrix B
+// (:202-243): f(omega) = sum_k pred_k B_k(omega), clamped and exponentiated as below.
 // Mask (FP32, [N]): 1 where some orientation is outside the hard core (vext < vmax).
 // Start: f = a_0 + a . u clamped to [-2, 4], xi = exp(f/2), and xi = 0 wherever
 // guess_density puts 0 (vext >= vmax, src/module_density.f90:267-284).  The start's floor
@@ -117,7 +122,66 @@ __global__ void k_warm_expand(const float *__restrict__ pred, const double *__re
     }
 }
 
+// projection form: A is [no][2np] (angl2proj), one thread per point
+__global__ void k_warm_target_proj(const double *__restrict__ xi, const double *__restrict__ vext, const double *__restrict__ A,
+                                   float *__restrict__ target, float *__restrict__ mask, int no, int nk, long long N, double vmax) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+        const double *x = xi + p * no;
+        const double *v = vext + p * no;
+        bool open = false;
+        for (int io = 0; io < no; ++io) open = open || v[io] < vmax;
+        for (int k = 0; k < nk; ++k) {
+            double acc = 0.0;
+            for (int io = 0; io < no; ++io) {
+                const double xv = x[io];
+                const double f = fmin(fmax(xv > 0.0 ? 2.0 * log(xv) : kWarmFloor, kWarmFloor), kWarmCeil);
+                acc = fma(f, A[(size_t)io * nk + k], acc);
+            }
+            target[(size_t)k * N + p] = (float)acc;
+        }
+        if (mask) mask[p] = open ? 1.f : 0.f;
+    }
+}
+
+// projection form: B is [2np][no] (proj2angl)
+__global__ void k_warm_expand_proj(const float *__restrict__ pred, const double *__restrict__ vext, const double *__restrict__ B,
+                                   double *__restrict__ xi, int no, int nk, long long N, double vmax) {
+    const long long n = N * no;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long p = i / no;
+        const int io = (int)(i - p * no);
+        double f = 0.0;
+        for (int k = 0; k < nk; ++k) f = fma((double)pred[(size_t)k * N + p], B[(size_t)k * no + io], f);
+        f = fmin(fmax(f, kWarmStartFloor), kWarmCeil);
+        xi[i] = vext[i] >= vmax ? 0.0 : exp(0.5 * f);
+    }
+}
+
 double guess_vmax(const mdft_handle *h) { return (-std::log(kEpsDp) - (double)0.05f) * h->g.kT; }
+
+// the output forms a handle accepts: 4 (m <= 1 real basis) or 2 np (all projections)
+int check_warm_nout(const mdft_handle *h, int nout) {
+    if (nout == 4 || nout == 2 * h->g.np) return MDFT_OK;
+    set_error("warm-start output count %d: 4 (m <= 1) or %d (all projections of this grid)", nout, 2 * h->g.np);
+    return MDFT_E_ARG;
+}
+
+int warm_tables(mdft_handle *h, double4 *norm);
+
+// prediction -> starting density in d_xi, in the form of nout outputs
+int warm_expand_any(mdft_handle *h, const float *pred, int nout, double *d_xi) {
+    const Grid &g = h->g;
+    if (nout == 4) {
+        double4 norm;
+        int rc = warm_tables(h, &norm);
+        if (rc) return rc;
+        k_warm_expand<<<vec_grid(), 256, 0, h->stream>>>(pred, h->vext.p, h->wdir.p, d_xi, g.no, g.N, guess_vmax(h));
+    } else {
+        k_warm_expand_proj<<<vec_grid(), 256, 0, h->stream>>>(pred, h->vext.p, h->B.p, d_xi, g.no, 2 * g.np, g.N, guess_vmax(h));
+    }
+    h->launches += 1;
+    return check_cuda(cudaGetLastError(), "warm-start expand");
+}
 
 // {u_x, u_y, u_z, w} per orientation on the device, and the projection normalisations
 int warm_tables(mdft_handle *h, double4 *norm) {
@@ -181,9 +245,9 @@ int warm_start_impl(mdft_handle *h, int nsite, const double *q, const double *si
     h->launches += after - before;
     const float *pred = nullptr;
     if ((rc = mdft_warm_net_output(h->warm, &pred))) return rc;
-    k_warm_expand<<<vec_grid(), 256, 0, h->stream>>>(pred, h->vext.p, h->wdir.p, d_xi, g.no, g.N, guess_vmax(h));
-    h->launches += 1;
-    return check_cuda(cudaGetLastError(), "warm start");
+    int nout = 4;
+    if ((rc = mdft_warm_net_num_outputs(h->warm, &nout))) return rc;
+    return warm_expand_any(h, pred, nout, d_xi);
 }
 
 }  // namespace
@@ -202,35 +266,44 @@ int mdft_warm_features(mdft_handle *h, int nsite, const double *q, const double 
 }
 
 int mdft_warm_target(mdft_handle *h, const double *d_xi, float *d_target, float *d_mask) {
+    return mdft_warm_target_n(h, d_xi, 4, d_target, d_mask);
+}
+
+int mdft_warm_target_n(mdft_handle *h, const double *d_xi, int nout, float *d_target, float *d_mask) {
     if (!h || !d_target) { set_error("null argument"); return MDFT_E_ARG; }
+    int rc0 = check_warm_nout(h, nout);
+    if (rc0) return rc0;
     if (!h->have_vext) { set_error("no vext yet"); return MDFT_E_STATE; }
     if (!d_xi) {
         if (!h->lb.x.p) { set_error("no solve has run on this handle"); return MDFT_E_STATE; }
         d_xi = h->lb.x.p;
     }
-    double4 norm;
-    int rc = warm_tables(h, &norm);
-    if (rc) return rc;
     const Grid &g = h->g;
-    k_warm_target<<<vec_grid(), 256, 0, h->stream>>>(d_xi, h->vext.p, h->wdir.p, d_target, d_mask, g.no, g.N, guess_vmax(h), norm);
+    if (nout == 4) {
+        double4 norm;
+        int rc = warm_tables(h, &norm);
+        if (rc) return rc;
+        k_warm_target<<<vec_grid(), 256, 0, h->stream>>>(d_xi, h->vext.p, h->wdir.p, d_target, d_mask, g.no, g.N, guess_vmax(h), norm);
+    } else {
+        k_warm_target_proj<<<vec_grid(), 256, 0, h->stream>>>(d_xi, h->vext.p, h->A.p, d_target, d_mask, g.no, 2 * g.np, g.N,
+                                                              guess_vmax(h));
+    }
     h->launches += 1;
     return check_cuda(cudaGetLastError(), "warm-start target");
 }
 
-int mdft_warm_expand(mdft_handle *h, const float *d_pred, double *d_xi) {
+int mdft_warm_expand(mdft_handle *h, const float *d_pred, double *d_xi) { return mdft_warm_expand_n(h, d_pred, 4, d_xi); }
+
+int mdft_warm_expand_n(mdft_handle *h, const float *d_pred, int nout, double *d_xi) {
     if (!h || !d_pred) { set_error("null argument"); return MDFT_E_ARG; }
+    int rc0 = check_warm_nout(h, nout);
+    if (rc0) return rc0;
     if (!h->have_vext) { set_error("no vext yet"); return MDFT_E_STATE; }
     if (!d_xi) {
         if (!h->lb.x.p) { set_error("no solve has run on this handle"); return MDFT_E_STATE; }
         d_xi = h->lb.x.p;
     }
-    double4 norm;
-    int rc = warm_tables(h, &norm);
-    if (rc) return rc;
-    const Grid &g = h->g;
-    k_warm_expand<<<vec_grid(), 256, 0, h->stream>>>(d_pred, h->vext.p, h->wdir.p, d_xi, g.no, g.N, guess_vmax(h));
-    h->launches += 1;
-    return check_cuda(cudaGetLastError(), "warm-start expand");
+    return warm_expand_any(h, d_pred, nout, d_xi);
 }
 
 int mdft_set_warm_net(mdft_handle *h, mdft_warm_net *net) {
@@ -245,6 +318,9 @@ int mdft_set_warm_net(mdft_handle *h, mdft_warm_net *net) {
             return MDFT_E_ARG;
         }
         if (h->g.no < 2) { set_error("warm start needs mmax >= 1"); return MDFT_E_ARG; }
+        int nout = 0;
+        if ((rc = mdft_warm_net_num_outputs(net, &nout))) return rc;
+        if ((rc = check_warm_nout(h, nout))) return rc;
     }
     cudaStreamSynchronize(h->stream);
     // a network that is detached goes back to its own stream
