@@ -54,9 +54,9 @@ PGTOL_REF = 1e-6
 GUNI_TOL = 0.1
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from one ncu
-# capture of each kernel on this workload (the gather through the public API; the OZ and the
-# projection in a mixed solve); absent: null
-NCU_TRAFFIC_BYTES = {("mixed", "oz"): 65.1e6, ("mixed", "gather"): 559.2e6, ("mixed", "project"): 213.6e6}
+# capture of each FP32-phase kernel in a mixed solve of this workload (k_gather_ring<84>,
+# k_project_umma<float,4>, k_ozp<3,2>); absent: null
+NCU_TRAFFIC_BYTES = {("mixed", "oz"): 65.1e6, ("mixed", "gather"): 393.2e6, ("mixed", "project"): 112.1e6}
 
 
 def parse():
@@ -165,10 +165,13 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def stage_bytes(N, no, np_, c=16):
-    """Algorithmic bytes per evaluation of each stage (c = bytes per complex projection value)."""
-    return {"project": N * (no * 8 + np_ * c), "fft_forward": 2 * np_ * N * c, "oz": 2 * np_ * N * c,
-            "fft_inverse": 2 * np_ * N * c, "gather": N * (np_ * c + 3 * no * 8)}
+def stage_bytes(N, no, np_, c=16, r=8):
+    """Algorithmic bytes per evaluation of each stage inside a solve (c = bytes per complex
+    projection value, r = bytes per real value of the point, vext, gradient and direction):
+    the projection reads xi and writes the planes; each FFT direction and the OZ read and write
+    them; the gather reads them, xi, vext and the search direction and writes the gradient."""
+    return {"project": N * (no * r + np_ * c), "fft_forward": 2 * np_ * N * c, "oz": 2 * np_ * N * c,
+            "fft_inverse": 2 * np_ * N * c, "gather": N * (np_ * c + 4 * no * r)}
 
 
 def cpu_oracle_eval_seconds(n, box, mmax, ck, nevals, threads, seed=1000):
@@ -296,8 +299,9 @@ def main():
     warm_params, warm_meta, warm_note = None, None, None
     if args.form == "learned":
         from mdft_b200 import warmstart
-        if os.path.exists(warmstart.WEIGHTS):
-            warm_params, warm_meta = warmstart.load_params()
+        wpath = warmstart.default_weights()
+        if wpath:
+            warm_params, warm_meta = warmstart.load_params(wpath)
         else:
             warm_note = "no trained parameters in the package: solves start from the bulk guess"
     nets = []
@@ -323,7 +327,7 @@ def main():
                 e = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=self.prec)
                 if name == "learned" and warm_params is not None:
                     from mdft_b200 import warmstart
-                    net = warmstart.WarmNet(n, device=local, params=warm_params)
+                    net = warmstart.WarmNet(n, device=local, params=warm_params, nout=warm_meta["nout"])
                     e.set_warm_net(net)
                     nets.append(net)
                 self.engines.append(e)
@@ -409,22 +413,22 @@ def main():
         warm_stats = {"starts": sum(e.warm_stats()["warm_starts"] for e in H.engines),
                       "fallbacks_to_bulk_guess": sum(e.warm_stats()["fallbacks"] for e in H.engines)}
 
-    # ---- roofline of the dominant stage: per-stage CUDA events over evaluations at a converged density ----
+    # ---- roofline of the dominant stage: per-stage CUDA events over every evaluation of one
+    # solve of the first timed solute (the FP32 phase's kernels in the mixed forms) ----
     eng = H.engines[0]
-    xi_ref = xi_host[0].copy()
     eng.set_timing(True)
-    for _ in range(5):
-        eng.energy_and_gradient(xi_ref)  # in the engine's evaluation precision
+    eng.solve(sols[steps_idx[0]], sv, rvdw=rvdw, **H.opts)
     st, cnt = eng.stage_times()
     eng.set_timing(False)
     per = {k: v / cnt for k, v in st.items()}
-    sb = stage_bytes(n ** 3, eng.no, eng.np, 16 if H.prec == PREC_FP64 else 8)
+    sb = stage_bytes(n ** 3, eng.no, eng.np, 16, 8) if H.prec == PREC_FP64 else stage_bytes(n ** 3, eng.no, eng.np, 8, 4)
     dom = max(per, key=per.get)
     peak, peak_kind = measured_peak_hbm()
     achieved = sb[dom] / (per[dom] * 1e-3) / 1e9
     traffic = NCU_TRAFFIC_BYTES.get(("fp64" if H.prec == PREC_FP64 else "mixed", dom)) if n == N_GRID else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_source": peak_kind, "stage_ms": per, "algorithmic_bytes": sb[dom]}
+            "traffic": traffic, "peak_source": peak_kind, "stage_ms": per, "algorithmic_bytes": sb[dom],
+            "timed": "every evaluation of one solve (%d), per-stage CUDA events on the handle's stream" % cnt}
     H.close()
 
     # ---- the plain FP64 form on the same solutes, handles and stop rule (the metric's divisor) ----
@@ -482,8 +486,11 @@ def main():
                                                        "this form starts from the bulk guess"}
                                if args.form == "mixed" else None) if args.form != "learned" else (
                                {"note": warm_note} if warm_params is None else
-                               dict({"network": "periodic 3-D conv encoder-decoder, BF16 weights",
-                                     "trained": {k: warm_meta.get(k) for k in ("train", "epochs", "final_val_loss")}},
+                               dict({"network": "periodic 3-D conv encoder-decoder, BF16 weights, %d outputs (%s)"
+                                                % (warm_meta["nout"], "m <= 1 real basis" if warm_meta["nout"] == 4
+                                                   else "all projections of the log-density"),
+                                     "trained": {k: warm_meta.get(k) for k in ("train", "epochs", "final_val_loss",
+                                                                               "solver")}},
                                     **warm_stats)),
                            "stop": STOP_TEXT % (args.pgtol, args.guni_tol),
                            "l2": "inputs larger than L2 (176 MB per field)",

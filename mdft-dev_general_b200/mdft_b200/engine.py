@@ -130,10 +130,14 @@ SIGNATURES = {
     "mdft_warm_net_take_loss": (C.c_int, [C.c_void_p, _DP]),
     "mdft_warm_net_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "mdft_warm_net_grid": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "mdft_warm_net_create_n": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "mdft_warm_net_num_outputs": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mdft_warm_features": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP, _DP, _DP, _DP,
                                      C.c_double, C.c_void_p]),
     "mdft_warm_target": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mdft_warm_expand": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mdft_warm_target_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "mdft_warm_expand_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "mdft_set_warm_net": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mdft_get_warm_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
 }
@@ -359,14 +363,14 @@ class Engine:
         _check(lib().mdft_warm_features(self.h, len(q), _p(q), _p(sg), _p(ep), _p(xyz), len(vq), _p(vq), _p(vs), _p(ve),
                                         _p(vx), float(rvdw), C.c_void_p(d_feat)))
 
-    def warm_target(self, d_target: int, d_mask: int | None = None, d_xi: int | None = None):
-        """4 x N log-density projections (and the N-point loss mask) of the density d_xi
-        (device; None: the last solve's result)."""
-        _check(lib().mdft_warm_target(self.h, None if d_xi is None else C.c_void_p(d_xi), C.c_void_p(d_target),
-                                      None if d_mask is None else C.c_void_p(d_mask)))
+    def warm_target(self, d_target: int, d_mask: int | None = None, d_xi: int | None = None, nout: int = 4):
+        """Training target (nout x N: 4 = the m <= 1 real basis, 2 np = all complex projections as
+        real and imaginary planes) and mask (N) from a converged density (default: the last solve)."""
+        _check(lib().mdft_warm_target_n(self.h, None if d_xi is None else C.c_void_p(d_xi), int(nout), C.c_void_p(d_target),
+                                        None if d_mask is None else C.c_void_p(d_mask)))
 
-    def warm_expand(self, d_pred: int, d_xi: int):
-        _check(lib().mdft_warm_expand(self.h, C.c_void_p(d_pred), C.c_void_p(d_xi)))
+    def warm_expand(self, d_pred: int, d_xi: int, nout: int = 4):
+        _check(lib().mdft_warm_expand_n(self.h, C.c_void_p(d_pred), int(nout), C.c_void_p(d_xi)))
 
     def set_warm_net(self, net):
         """Start solves on this engine from `net`'s prediction (None: from the bulk guess)."""

@@ -9,7 +9,7 @@ reference has no counterpart: its solves start from guess_density
 Device memory for the training set is held in torch CUDA tensors (plumbing only: every
 kernel that touches them is the library's).
 
-    python -m mdft_b200.warmstart --train 600 --val 40 --out weights.npz
+    python -m mdft_b200.warmstart --train 2000 --val 50 --epochs 12 [--form proj|m1] [--eval 200]
 """
 from __future__ import annotations
 
@@ -25,7 +25,9 @@ import numpy as np
 from . import engine as E
 from . import synth
 
-WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "warmstart_weights.npz")
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "warmstart_weights.npz")  # m <= 1 form
+# all projections of the log-density (56 outputs at mmax 3): the form the solver starts from
+WEIGHTS_PROJ = os.path.join(os.path.dirname(os.path.abspath(__file__)), "warmstart_weights_proj.npz")
 TRAIN_N, TRAIN_BOX = 48, 24.0   # 0.5 A spacing, as the 64^3 / 32 A evaluation grid
 EVAL_N, EVAL_BOX = 64, 32.0
 MMAX = 3
@@ -42,11 +44,13 @@ def bf16_round(x: np.ndarray) -> np.ndarray:
 class WarmNet:
     """The warm-start network on one GPU for one grid (dimensions multiples of 8)."""
 
-    def __init__(self, n: int, device: int = 0, seed: int | None = 20260401, params: np.ndarray | None = None):
+    def __init__(self, n: int, device: int = 0, seed: int | None = 20260401, params: np.ndarray | None = None,
+                 nout: int = 4):
         h = C.c_void_p()
-        E._check(E.lib().mdft_warm_net_create(n, n, n, device, C.byref(h)))
+        E._check(E.lib().mdft_warm_net_create_n(n, n, n, int(nout), device, C.byref(h)))
         self.h = h.value
         self.n = n
+        self.nout = int(nout)
         c = C.c_longlong()
         E._check(E.lib().mdft_warm_net_num_params(self.h, C.byref(c)))
         self.nparam = c.value
@@ -117,7 +121,17 @@ def save_params(path: str, params: np.ndarray, meta: dict | None = None):
 def load_params(path: str = WEIGHTS) -> tuple[np.ndarray, dict]:
     z = np.load(path)
     p = (z["bf16"].astype(np.uint32) << 16).view(np.float32)
-    return p, json.loads(str(z["meta"]))
+    meta = json.loads(str(z["meta"]))
+    meta.setdefault("nout", 4)
+    return p, meta
+
+
+def default_weights() -> str | None:
+    """The parameter file the solver's learned start uses: the all-projection form when shipped."""
+    for p in (WEIGHTS_PROJ, WEIGHTS):
+        if os.path.exists(p):
+            return p
+    return None
 
 
 def config4_solute(seed: int):
@@ -132,9 +146,10 @@ def centred(sol, box):
     return synth.Solute(q=sol.q, sig=sol.sig, eps=sol.eps, xyz=synth.center_solute(sol.xyz, box))
 
 
-def make_training_set(engines, seeds, solvent, rvdw=10.0, pgtol=1e-4, precision=E.PREC_FP64, log=None):
-    """Solve every seeded solute with the plain solver (from the bulk guess) on the given
-    engines, one host thread per engine, and keep each one's channels, target and mask on
+def make_training_set(engines, seeds, solvent, rvdw=10.0, pgtol=1e-4, precision=E.PREC_FP64, log=None, nout=4,
+                      guni_tol=0.0):
+    """Solve every seeded solute with the solver (from the bulk guess) on the given engines,
+    one host thread per engine, and keep each one's channels, target (nout x N) and mask on
     the device.  Returns (samples, per-solute results)."""
     n = engines[0].shape[0] * engines[0].shape[1] * engines[0].shape[2]
     box = engines[0].box
@@ -155,12 +170,13 @@ def make_training_set(engines, seeds, solvent, rvdw=10.0, pgtol=1e-4, precision=
                 return
             try:
                 sol = centred(config4_solute(seeds[i]), box)
-                r = eng.solve(sol, solvent, rvdw=rvdw, pgtol=pgtol, ftol_abs=-1.0, itermax=5000, precision=precision)
+                r = eng.solve(sol, solvent, rvdw=rvdw, pgtol=pgtol, ftol_abs=-1.0, itermax=5000, precision=precision,
+                              guni_tol=guni_tol)
                 feat = T.empty((3, n), dtype=T.float32, device=torch_dev)
-                tgt = T.empty((4, n), dtype=T.float32, device=torch_dev)
+                tgt = T.empty((nout, n), dtype=T.float32, device=torch_dev)
                 mask = T.empty((n,), dtype=T.float32, device=torch_dev)
                 eng.warm_features(sol, solvent, feat.data_ptr(), rvdw=rvdw)
-                eng.warm_target(tgt.data_ptr(), mask.data_ptr())
+                eng.warm_target(tgt.data_ptr(), mask.data_ptr(), nout=nout)
                 T.cuda.synchronize(torch_dev)
                 samples[i] = (feat, tgt, mask)
                 results[i] = dict(seed=seeds[i], nsite=len(sol.q), dG=r["dG"], evaluations=r["evaluations"],
@@ -212,27 +228,29 @@ def evaluate_loss(net: WarmNet, samples) -> float:
     return tot / max(1, len(samples))
 
 
-def evaluate_heldout(params, seeds, solvent, ck, workers=3, pgtol=1e-4, pgtol_ref=1e-6, log=None):
+def evaluate_heldout(params, seeds, solvent, ck, workers=3, pgtol=1e-4, pgtol_ref=1e-6, log=None, nout=4, guni_tol=0.1):
     """Held-out solutes at 64^3: plain FP64 solves from the bulk guess to max|df| <= pgtol_ref
-    (the dG reference), then mixed-precision solves to pgtol from the bulk guess and from the
-    network's prediction, each form as one concurrent batch over `workers` engines.  Returns
-    per-solute rows and a summary (evaluations, solutes/s by wall clock, |dG - FP64|)."""
+    (the dG reference), then mixed-precision solves to pgtol (and |sum w df dv| <= guni_tol)
+    from the bulk guess and from the network's prediction, each form as one concurrent batch
+    over `workers` engines.  Returns per-solute rows and a summary (evaluations, solutes/s by
+    wall clock, |dG - FP64|)."""
     sols = [centred(config4_solute(sd), (EVAL_BOX,) * 3) for sd in seeds]
     out = {}
-    forms = [("fp64_ref", E.PREC_FP64, pgtol_ref, False), ("mixed_cold", E.PREC_MIXED, pgtol, False),
-             ("mixed_warm", E.PREC_MIXED, pgtol, True)]
+    forms = [("fp64_ref", E.PREC_FP64, pgtol_ref, False, 0.01), ("mixed_cold", E.PREC_MIXED, pgtol, False, guni_tol),
+             ("mixed_warm", E.PREC_MIXED, pgtol, True, guni_tol)]
     fallbacks = 0
-    for name, prec, tol, warm in forms:
+    for name, prec, tol, warm, gtol in forms:
         engs = [E.Engine(EVAL_N, EVAL_BOX, MMAX, ck, temperature=solvent.temperature, n0=solvent.n0, precision=prec)
                 for _ in range(workers)]
         nets = []
         if warm:
             for e in engs:
-                net = WarmNet(EVAL_N, device=e.device, params=params)
+                net = WarmNet(EVAL_N, device=e.device, params=params, nout=nout)
                 e.set_warm_net(net)
                 nets.append(net)
         t0 = time.time()
-        res = E.solve_batch(engs, sols, solvent, m=5, pgtol=tol, ftol_abs=-1.0, itermax=5000, precision=prec)
+        res = E.solve_batch(engs, sols, solvent, m=5, pgtol=tol, ftol_abs=-1.0, itermax=5000, precision=prec,
+                            guni_tol=gtol)
         wall = time.time() - t0
         if warm:
             fallbacks = sum(e.warm_stats()["fallbacks"] for e in engs)
@@ -289,7 +307,11 @@ def main(argv=None):
     ap.add_argument("--eval", type=int, default=0, help="held-out 64^3 solutes to compare cold and warm solves on")
     ap.add_argument("--eval-seed0", type=int, default=50000000)
     ap.add_argument("--eval-only", default=None, help="parameter file: skip training, only the held-out comparison")
-    ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--form", default="proj", choices=["proj", "m1"],
+                    help="proj: all projections of the log-density (2 np outputs); m1: the m <= 1 real basis (4)")
+    ap.add_argument("--solver", default="mixed", choices=["mixed", "fp64"], help="precision of the training-set solves")
+    ap.add_argument("--guni-tol", type=float, default=0.1, help="uniform-mode stop bound of the solves (kJ/mol)")
+    ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
     t0 = time.time()
@@ -306,26 +328,31 @@ def main(argv=None):
     if a.eval_only:
         params, meta = load_params(a.eval_only)
         rows, summ = evaluate_heldout(params, [a.eval_seed0 + i for i in range(a.eval)], solvent, ck,
-                                      workers=a.workers, pgtol=a.pgtol, log=log)
+                                      workers=a.workers, pgtol=a.pgtol, log=log, nout=meta["nout"], guni_tol=a.guni_tol)
         log("held-out: %s" % json.dumps(summ))
         if a.report:
             with open(a.report, "w") as f:
                 json.dump(dict(meta=meta, summary=summ, heldout=rows), f)
         return
-    engines = [E.Engine(TRAIN_N, TRAIN_BOX, MMAX, ck, temperature=solvent.temperature, n0=solvent.n0)
+    prec = E.PREC_MIXED if a.solver == "mixed" else E.PREC_FP64
+    engines = [E.Engine(TRAIN_N, TRAIN_BOX, MMAX, ck, temperature=solvent.temperature, n0=solvent.n0, precision=prec)
                for _ in range(a.workers)]
+    nout = 4 if a.form == "m1" else 2 * engines[0].np
+    out_path = a.out or (WEIGHTS if a.form == "m1" else WEIGHTS_PROJ)
     seeds = [a.seed0 + i for i in range(a.train + a.val)]
-    samples, res = make_training_set(engines, seeds, solvent, pgtol=a.pgtol, log=log)
+    samples, res = make_training_set(engines, seeds, solvent, pgtol=a.pgtol, log=log, nout=nout, precision=prec,
+                                     guni_tol=a.guni_tol)
     tgen = time.time() - t0
     log("training set: %d solutes in %.1f s (%.1f evaluations per solve)" %
         (len(samples), tgen, np.mean([r["evaluations"] for r in res])))
     for e in engines:
         e.close()
-    net = WarmNet(TRAIN_N)
+    net = WarmNet(TRAIN_N, nout=nout)
     t1 = time.time()
     hist = train(net, samples[:a.train], epochs=a.epochs, batch=a.batch, lr=a.lr, val=samples[a.train:], log=log)
     ttrain = time.time() - t1
-    meta = dict(train=a.train, val=a.val, epochs=a.epochs, batch=a.batch, lr=a.lr, pgtol=a.pgtol, seed0=a.seed0,
+    meta = dict(nout=nout, form=a.form, solver=a.solver, guni_tol=a.guni_tol,
+                train=a.train, val=a.val, epochs=a.epochs, batch=a.batch, lr=a.lr, pgtol=a.pgtol, seed0=a.seed0,
                 grid=[TRAIN_N, TRAIN_BOX], final_train_loss=hist[-1][1], final_val_loss=hist[-1][2],
                 gen_seconds=tgen, train_seconds=ttrain)
     params = net.get_params()
@@ -335,11 +362,11 @@ def main(argv=None):
     rows, summ = [], {}
     if a.eval > 0:
         rows, summ = evaluate_heldout(bf16_round(params), [a.eval_seed0 + i for i in range(a.eval)], solvent, ck,
-                                      workers=a.workers, pgtol=a.pgtol, log=log)
+                                      workers=a.workers, pgtol=a.pgtol, log=log, nout=nout, guni_tol=a.guni_tol)
         meta["heldout"] = summ
         log("held-out: %s" % json.dumps(summ))
-    save_params(a.out, params, meta)
-    log("saved %s (%d parameters): %s" % (a.out, len(params), json.dumps(meta)))
+    save_params(out_path, params, meta)
+    log("saved %s (%d parameters): %s" % (out_path, len(params), json.dumps(meta)))
     if a.report:
         with open(a.report, "w") as f:
             json.dump(dict(meta=meta, history=hist, solves=res, heldout=rows), f)

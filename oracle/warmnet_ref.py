@@ -7,7 +7,9 @@ __graft_entry__.smoke() as the checker, never by the product).
   autograd gives the reference gradients of the library's forward and backward kernels.
 * numpy restatements of the solver-side kernels: the input channels from the solute
   sites, the m <= 1 log-density projections of a density with their loss mask, and the
-  starting density built from projections.
+  starting density built from projections; the same for the projection form (all np
+  complex projections of the log-density by the C oracle's angl2proj, the start by its
+  proj2angl).
 
 The warm start has no counterpart in the reference (whose solves start from
 guess_density, src/module_density.f90:267-284); the definitions restated here are the
@@ -19,7 +21,8 @@ import math
 
 import numpy as np
 
-# (kind, input tensor, output tensor, cin, cout, skip tensor, GELU)
+# (kind, input tensor, output tensor, cin, cout, skip tensor, GELU); the head's cout is the
+# network's output count (4 here; layers(nout) for other widths)
 CONV3, DOWN, UP, HEAD = 0, 1, 2, 3
 LAYERS = [
     (CONV3, 0, 1, 3, 16, -1, 1), (CONV3, 1, 2, 16, 16, -1, 1), (DOWN, 2, 3, 16, 32, -1, 1),
@@ -40,14 +43,18 @@ def weight_shape(kind, cin, cout):
     return (cout, cin, 1, 1, 1)
 
 
-def num_params() -> int:
-    return sum(int(np.prod(weight_shape(k, ci, co))) + co for k, _, _, ci, co, _, _ in LAYERS)
+def layers(nout: int = 4):
+    return [(k, x, y, ci, nout if k == HEAD else co, sk, g) for k, x, y, ci, co, sk, g in LAYERS]
 
 
-def unpack(flat, torch):
+def num_params(nout: int = 4) -> int:
+    return sum(int(np.prod(weight_shape(k, ci, co))) + co for k, _, _, ci, co, _, _ in layers(nout))
+
+
+def unpack(flat, torch, nout: int = 4):
     """Flat parameter vector (per layer: weights, then biases) -> list of (W, b) tensors."""
     out, off = [], 0
-    for k, _, _, ci, co, _, _ in LAYERS:
+    for k, _, _, ci, co, _, _ in layers(nout):
         shp = weight_shape(k, ci, co)
         n = int(np.prod(shp))
         out.append((flat[off:off + n].reshape(shp), flat[off + n:off + n + co]))
@@ -56,13 +63,13 @@ def unpack(flat, torch):
     return out
 
 
-def forward(flat, x, torch):
+def forward(flat, x, torch, nout: int = 4):
     """x: (3, nz, ny, nx) float64 tensor; flat: parameter tensor (the library uses BF16
     weights, so pass weights rounded to BF16 for a like-for-like comparison)."""
     F = torch.nn.functional
-    params = unpack(flat, torch)
+    params = unpack(flat, torch, nout)
     t = {0: x.unsqueeze(0)}
-    for (k, xi, yi, ci, co, skip, gelu), (W, b) in zip(LAYERS, params):
+    for (k, xi, yi, ci, co, skip, gelu), (W, b) in zip(layers(nout), params):
         a = t[xi]
         if k == CONV3:
             y = F.conv3d(F.pad(a, (1, 1, 1, 1, 1, 1), mode="circular"), W, b)
@@ -77,9 +84,9 @@ def forward(flat, x, torch):
 
 
 def loss(y, target, mask):
-    """sum_v mask_v sum_c (y - t)^2 / (4 N), the library's training loss."""
+    """sum_v mask_v sum_c (y - t)^2 / (C N), the library's training loss (C outputs)."""
     n = y.shape[1] * y.shape[2] * y.shape[3]
-    return (((y - target) ** 2).sum(0) * mask).sum() / (4.0 * n)
+    return (((y - target) ** 2).sum(0) * mask).sum() / (float(y.shape[0]) * n)
 
 
 def bf16_round(x: np.ndarray) -> np.ndarray:
@@ -88,11 +95,11 @@ def bf16_round(x: np.ndarray) -> np.ndarray:
     return b.astype(np.uint32).view(np.float32)
 
 
-def bf16_weights(flat: np.ndarray) -> np.ndarray:
+def bf16_weights(flat: np.ndarray, nout: int = 4) -> np.ndarray:
     """The library's kernel parameters: weights rounded to BF16, biases kept FP32."""
     out = np.array(flat, dtype=np.float32, copy=True)
     off = 0
-    for k, _, _, ci, co, _, _ in LAYERS:
+    for k, _, _, ci, co, _, _ in layers(nout):
         n = int(np.prod(weight_shape(k, ci, co)))
         out[off:off + n] = bf16_round(out[off:off + n])
         off += n + co
@@ -167,5 +174,39 @@ def expand(pred, vext, table, vmax):
     """pred: 4 x (nz, ny, nx) -> xi (nz, ny, nx, no)."""
     u = table[:, :3]
     f = pred[0][..., None] + sum(pred[k + 1][..., None] * u[:, k] for k in range(3))
+    f = np.clip(f, START_FLOOR, CEIL)
+    return np.where(vext >= vmax, 0.0, np.exp(0.5 * f))
+
+
+# projection form -----------------------------------------------------------
+def angular_maps(orc):
+    """(A, B) of the C oracle: A (no, np) complex with angl2proj(o) = o @ A; B (2 np, no) real
+    with proj2angl(p) = sum_k [Re p, Im p]_k B_k (both maps are linear)."""
+    no, np_ = orc.no, orc.np
+    A = np.stack([orc.angl2proj(np.eye(no)[i]) for i in range(no)])
+    B = np.zeros((2 * np_, no))
+    for ip in range(np_):
+        for c, val in ((0, 1.0), (1, 1.0j)):
+            p = np.zeros(np_, dtype=np.complex128)
+            p[ip] = val
+            B[2 * ip + c] = orc.proj2angl(p)
+    return A, B
+
+
+def target_proj(xi, vext, A, vmax):
+    """xi, vext: (nz, ny, nx, no).  Returns the 2 np planes (Re, Im of each projection, in
+    the projection order) of clamp(2 ln xi), and the mask."""
+    with np.errstate(divide="ignore"):
+        f = np.where(xi > 0, 2.0 * np.log(np.where(xi > 0, xi, 1.0)), FLOOR)
+    f = np.clip(f, FLOOR, CEIL)
+    p = f @ A  # (nz, ny, nx, np) complex
+    planes = np.stack([p.real, p.imag], axis=-1).reshape(p.shape[:3] + (-1,))
+    mask = (vext < vmax).any(-1).astype(np.float64)
+    return np.moveaxis(planes, -1, 0), mask
+
+
+def expand_proj(pred, vext, B, vmax):
+    """pred: 2 np x (nz, ny, nx) -> xi (nz, ny, nx, no)."""
+    f = np.tensordot(np.moveaxis(pred, 0, -1), B, axes=([3], [0]))
     f = np.clip(f, START_FLOOR, CEIL)
     return np.where(vext >= vmax, 0.0, np.exp(0.5 * f))

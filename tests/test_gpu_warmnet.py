@@ -150,6 +150,70 @@ def test_target_and_expand_match_oracle(sys16):
     assert np.abs(out.cpu().numpy() - rx).max() <= 1e-12 * rx.max()
 
 
+def test_projection_form_network_matches_oracle():
+    # a network with the projection form's head (2 np outputs at mmax 2: 28): forward and every
+    # parameter gradient against torch float64 autograd
+    nout = 28
+    net = warmstart.WarmNet(N16, seed=15, nout=nout)
+    rng = np.random.default_rng(16)
+    x = rng.standard_normal((3, N16, N16, N16)).astype(np.float32)
+    t = rng.standard_normal((nout, N16, N16, N16)).astype(np.float32)
+    m = (rng.random((N16, N16, N16)) > 0.25).astype(np.float32)
+    dx, dt, dm = _dev(x), _dev(t), _dev(m)
+    out = torch.empty((nout, N16, N16, N16), device="cuda")
+    net.forward(dx.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    p = W.bf16_weights(net.get_params(), nout).astype(np.float64)
+    pt = torch.tensor(p, requires_grad=True)
+    y = W.forward(pt, torch.tensor(x, dtype=torch.float64), torch, nout)
+    got = out.cpu().numpy()
+    assert np.abs(got - y.detach().numpy()).max() < 1e-5 * np.abs(y.detach().numpy()).max()
+    g, loss = net.gradients(dx.data_ptr(), dt.data_ptr(), dm.data_ptr())
+    L = W.loss(y, torch.tensor(t, dtype=torch.float64), torch.tensor(m, dtype=torch.float64))
+    L.backward()
+    assert abs(loss - L.item()) <= 1e-5 * abs(L.item())
+    ref = pt.grad.numpy()
+    off = 0
+    for li, (k, _, _, ci, co, _, _) in enumerate(W.layers(nout)):
+        n = int(np.prod(W.weight_shape(k, ci, co)))
+        for a, b, what in ((off, off + n, "W"), (off + n, off + n + co, "b")):
+            e = np.abs(g[a:b] - ref[a:b]).max() / np.abs(ref[a:b]).max()
+            assert e < 2e-4, (li, what, e)
+        off += n + co
+    net.close()
+
+
+def test_projection_form_target_and_expand_match_oracle(sys16):
+    c, ck, e, _, _ = sys16
+    n = c["n"]
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    A, B = W.angular_maps(o)
+    nout = 2 * e.np
+    vext = e.get_vext()
+    rng = np.random.default_rng(17)
+    xi = rng.uniform(0.2, 2.5, e.shape)
+    xi[vext >= _vmax(e.kT)] = 0.0
+    dxi = _dev(xi, torch.float64)
+    tgt = torch.empty((nout, n ** 3), device="cuda")
+    mask = torch.empty((n ** 3,), device="cuda")
+    e.warm_target(tgt.data_ptr(), mask.data_ptr(), d_xi=dxi.data_ptr(), nout=nout)
+    torch.cuda.synchronize()
+    rt, rm = W.target_proj(xi, vext, A, _vmax(e.kT))
+    assert np.abs(tgt.cpu().numpy() - rt.reshape(nout, -1)).max() <= 1e-5 * max(1.0, np.abs(rt).max())
+    assert np.array_equal(mask.cpu().numpy(), rm.reshape(-1).astype(np.float32))
+    # the start from planes of a real field's projections (the form a trained network predicts)
+    raw = rng.uniform(-0.5, 0.5, e.shape)
+    pr = raw @ A
+    pred = np.moveaxis(np.stack([pr.real, pr.imag], -1).reshape(n, n, n, -1), -1, 0).astype(np.float32)
+    dp = _dev(pred.reshape(nout, -1))
+    out = torch.empty(e.shape, dtype=torch.float64, device="cuda")
+    e.warm_expand(dp.data_ptr(), out.data_ptr(), nout=nout)
+    torch.cuda.synchronize()
+    rx = W.expand_proj(pred.astype(np.float64), vext, B, _vmax(e.kT))
+    assert np.abs(out.cpu().numpy() - rx).max() <= 1e-12 * rx.max()
+    o.close()
+
+
 @pytest.mark.parametrize("precision", [0, PREC_MIXED])
 def test_warm_started_solve_reaches_the_cold_result(sys16, precision):
     c, ck, _, sol, _ = sys16

@@ -39,7 +39,7 @@ def test_parameter_file_round_trip(tmp_path):
     path = str(tmp_path / "w.npz")
     warmstart.save_params(path, p, dict(note="x"))
     q, meta = warmstart.load_params(path)
-    assert meta == dict(note="x")
+    assert meta == dict(note="x", nout=4)  # files without an output count are the m <= 1 form
     assert np.array_equal(q, W.bf16_round(p))
 
 
@@ -118,3 +118,30 @@ def test_shipped_parameters_load():
     assert p.size == W.num_params() and np.isfinite(p).all()
     assert np.array_equal(p, W.bf16_round(p))                      # stored as BF16
     assert meta["train"] == 2000 and meta["final_val_loss"] < 0.1
+
+
+def test_projection_form_round_trip(grid16):
+    # a band-limited log-density (proj2angl of projections of a real field) projects to
+    # planes whose expansion rebuilds the density: the projection form loses nothing there
+    c, o = grid16
+    A, B = W.angular_maps(o)
+    rng = np.random.default_rng(4)
+    n, no = 6, len(o.weights)
+    raw = rng.uniform(-0.6, 0.6, (n, n, n, no))
+    f = np.einsum("zyxk,kn->zyxn", np.moveaxis(np.stack([(raw @ A).real, (raw @ A).imag], -1).reshape(n, n, n, -1), -1, 0)
+                  .transpose(1, 2, 3, 0), B)
+    assert f.min() > W.START_FLOOR and f.max() < W.CEIL
+    xi = np.exp(0.5 * f)
+    vext = np.zeros_like(xi)
+    t, mask = W.target_proj(xi, vext, A, vmax=1e3)
+    assert t.shape == (2 * o.np, n, n, n) and mask.min() == 1.0
+    assert np.abs(W.expand_proj(t, vext, B, 1e3) - xi).max() < 1e-12 * xi.max()
+
+
+def test_network_head_width():
+    # the head's width is the output count; the other layers do not change
+    assert W.num_params(56) - W.num_params(4) == (56 - 4) * (16 + 1)
+    import torch
+    flat = torch.zeros(W.num_params(28), dtype=torch.float64)
+    y = W.forward(flat, torch.zeros((3, 8, 8, 8), dtype=torch.float64), torch, nout=28)
+    assert tuple(y.shape) == (28, 8, 8, 8)
