@@ -17,11 +17,12 @@ int eval_launch(mdft_handle *h, const void *x, double *g, const void *dvec, bool
     return run_pipeline(h, x, g, 1, 1, dvec, v32, x32);
 }
 
-int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax, double *guni = nullptr) {
+int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax, double *guni = nullptr, double *fscale = nullptr) {
     double fid, fext, fexc;
     int rc = finish_sums(h, &fid, &fext, &fexc);
     if (rc) return rc;
     *f = combine(h, fid, fext, fexc);
+    if (fscale) *fscale = std::fabs(fid) + std::fabs(fext) + std::fabs(fexc) + std::fabs(h->const_corr);
     const double gdv = h->h_sums[3], gmx = h->h_sums[4], gun = h->h_sums[5] * h->g.dv;
     if (gd) *gd = gdv;
     if (gmax) *gmax = gmx;
@@ -36,10 +37,10 @@ int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax, double *gun
 // x, g device vectors of n; dvec may be null.  Leaves f, g.dvec and max|g|.  v32: g and dvec
 // are FP32 vectors (the minimiser's mixed solves).
 int eval_fg(mdft_handle *h, const void *x, double *g, const void *dvec, double *f, double *gd, double *gmax,
-            bool v32 = false, bool x32 = false, double *guni = nullptr) {
+            bool v32 = false, bool x32 = false, double *guni = nullptr, double *fscale = nullptr) {
     int rc = eval_launch(h, x, g, dvec, v32, x32);
     if (rc) return rc;
-    return eval_finish(h, f, gd, gmax, guni);
+    return eval_finish(h, f, gd, gmax, guni, fscale);
 }
 
 int lbfgs_alloc(mdft_handle *h, int m) {
@@ -396,9 +397,14 @@ namespace {
 // History of the compact limited-memory matrix.  Slots head, head+1, ... (mod m) hold the
 // pairs oldest first; Gram entries are kept by slot: sy[i*m+j] = s_i.y_j (i not newer than
 // j), yy[i*m+j] = y_i.y_j, and sg/yg = s_i.g, y_i.g at the current gradient.
-// Relative rounding noise of F assumed for the FP32 phase of a mixed solve (FP32 planes,
-// FP64 sums): the tolerance of its approximate Wolfe test.
+// Relative rounding noise assumed for the FP32 phase of a mixed solve (FP32 planes and
+// per-element arithmetic, FP64 sums), relative to the size of the terms F is the sum of
+// (|F_id| + |F_ext| + |F_exc| + |constant|, which can exceed |F| by orders of magnitude):
+// the tolerance of its approximate Wolfe test.
 constexpr double kMixedNoiseRel = 1e-6;
+// Trial points one line search of the FP32 phase may evaluate; more means the search is
+// chasing rounding noise, and the phase ends as at a failed search (the FP64 phase goes on).
+constexpr int kMixedMaxTrials = 8;
 
 struct LbfgsHist {
     int m = 0, col = 0, head = 0;
@@ -742,13 +748,13 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     }
     const double epsmch = kEpsDp;
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
-    double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0, guni = 0;
+    double f = 0, fold = 0, stp = 0, gd = 0, gdold = 0, gmax = 0, dd = 0, guni = 0, fscale = 0, fscale_t = 0;
     int iter = 0, nfgv = 0, status = 3;
     const bool fresh = H.col == 0;
     PendingPair pend;
     // projgr's test (max|df| <= pgtol), plus, when asked, the uniform-mode gradient bound
     auto converged = [&](double gm, double gu) { return gm <= o->pgtol && (o->guni_tol <= 0.0 || std::fabs(gu) <= o->guni_tol); };
-    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32, x32, &guni))) return rc;
+    if ((rc = eval_fg(h, xc, gc, nullptr, &f, nullptr, &gmax, v32, x32, &guni, &fscale))) return rc;
     nfgv = 1;
     trace_iter(h, x32 ? nullptr : xc, 0, nfgv, f, gmax, 0.0);
     double sbgnrm = gmax;
@@ -784,6 +790,10 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 ++nfgv;
                 iback = ifun - 1;
                 if (iback >= 20) break;
+                if (noise_rel > 0.0 && ifun > kMixedMaxTrials) {  // FP32 phase: the search chases noise
+                    iback = 20;
+                    break;
+                }
                 if (ifun > 1) {  // the first trial point came with the direction
                     if (x32) {
                         const float *d32 = reinterpret_cast<const float *>(L.d.p);
@@ -805,14 +815,14 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
                 // the history's products with this trial gradient, queued before the one
                 // synchronise of the step (used if the trial is accepted)
                 if ((rc = launch_history_dots(h, H, gt, gc, L.d.p, stp, P))) return rc;
-                if ((rc = eval_finish(h, &f, &gd, &gmax_t, &guni_t))) return rc;
+                if ((rc = eval_finish(h, &f, &gd, &gmax_t, &guni_t, &fscale_t))) return rc;
                 const double stp_eval = stp;
                 task = dcsrch(f, gd, stp, ftol, gtol, xtol, 0.0, stpmx, false, LS);
                 // Approximate Wolfe test (Hager and Zhang, SIAM J. Optim. 16 (2005) 170, eq. 4.1):
-                // when F carries rounding noise of relative size noise_rel, a trial whose F is
-                // within that noise of F(0) and whose slope satisfies
-                // sigma g'(0) <= g'(stp) <= (2 delta - 1) g'(0) is accepted.
-                if (task == LS_FG && noise_rel > 0.0 && f <= fold + noise_rel * std::fabs(fold) &&
+                // when F carries rounding noise of relative size noise_rel (relative to the
+                // terms it sums), a trial whose F is within that noise of F(0) and whose slope
+                // satisfies sigma g'(0) <= g'(stp) <= (2 delta - 1) g'(0) is accepted.
+                if (task == LS_FG && noise_rel > 0.0 && f <= fold + noise_rel * fscale &&
                     gd >= 0.9 * gdold && gd <= -0.8 * gdold) {
                     stp = stp_eval;
                     task = LS_CONV;
@@ -839,6 +849,7 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
         std::swap(gc, gt);
         gmax = gmax_t;
         guni = guni_t;
+        fscale = fscale_t;
         sbgnrm = gmax;
         trace_iter(h, x32 ? nullptr : xc, iter, nfgv, f, gmax, stp);
         if (converged(sbgnrm, guni)) { status = 0; goto done; }
