@@ -26,6 +26,10 @@ constexpr int kOzpThreads = 128;
 #define MDFT_OZP_MIN_BLOCKS 1
 #endif
 constexpr int kOzpMinBlocks = MDFT_OZP_MIN_BLOCKS;  // resident CTAs asked of the register allocator
+#ifndef MDFT_OZD_MIN_BLOCKS
+#define MDFT_OZD_MIN_BLOCKS 2
+#endif
+constexpr int kOzdMinBlocks = MDFT_OZD_MIN_BLOCKS;
 constexpr int kOzpMaxNp = 64;
 constexpr int kOzpMaxRec = 48;
 
@@ -294,6 +298,252 @@ __global__ void __launch_bounds__(kOzpThreads, kOzpMinBlocks) k_ozp(float2 *__re
                 }
                 u.x *= sg;
                 u.y *= sg;
+                if (selfconj && nyq) u.y = -u.y;
+                const size_t off = (size_t)S::pidx(m, khi, mu2) * a.N;
+                if (!selfconj) planes[off + kq] = s;
+                planes[off + km] = u;
+            }
+        }
+}
+
+// The same step with the rotation matrices factored: R^m_{mu' chi}(q) = e^{-i mu' alpha}
+// D^m_{mu' chi}, alpha the azimuth of q (0 when q is along z) and D real -- the recursion of
+// src/module_rotation.f90:119-247 pairs indices as m = x + u in every term, so the phases
+// factor out of it and D follows the same recursion in real arithmetic from
+// D^1(x, x1) = Re(R^1(x, x1) e^{i x alpha}).  A rotation then costs a phase per input and two
+// FMAs per term instead of four, and D takes half the registers of R.  The reference's
+// flush of R's parts below epsilon(1.) (:491-492) is not reproduced (FP32 evaluations
+// only; its effect is below FP32 rounding of the sums).
+template <int MM, int MR, int NH>
+__device__ __forceinline__ float ozd_dget(const float (&D1)[9], const float (&Dh)[NH], int l, int m, int m1) {
+    using S = OzShape<MM, MR>;
+    if (l == 0) return 1.f;
+    if (l == 1) return D1[(m + 1) * 3 + (m1 + 1)];
+    if (m1 >= S::m1min(m)) return Dh[S::hidx(l, m, m1)];
+    const float s = ((m + m1) & 1) ? -1.f : 1.f;
+    return s * Dh[S::hidx(l, -m, -m1)];
+}
+
+template <int MM, int MR>
+__global__ void __launch_bounds__(kOzpThreads, kOzdMinBlocks) k_ozd(float2 *__restrict__ planes, const float2 *__restrict__ ctab, Oz2Args a,
+                                                     OzpParams pp, const float2 *__restrict__ cq) {
+    using S = OzShape<MM, MR>;
+    constexpr int NP = S::np();
+    constexpr int NH = S::nhalf() > 0 ? S::nhalf() : 1;
+    constexpr int B = kOzpThreads;
+    extern __shared__ __align__(16) float2 ozp_smem[];  // [2 NP][B]: q side, then -q side
+    const int t = threadIdx.x;
+    float2 *sq = ozp_smem + t;
+    float2 *smq = ozp_smem + NP * B + t;
+    const long long kk = (long long)blockIdx.x * B + t;
+    if (kk >= a.nk) return;
+    const int ix = (int)(kk % a.nx), iy = (int)((kk / a.nx) % a.ny), iz = (int)(kk / ((long long)a.nx * a.ny));
+    const int ixm = (a.nx - ix) % a.nx, iym = (a.ny - iy) % a.ny, izm = (a.nz - iz) % a.nz;
+    if ((iz == 0 || 2 * iz == a.nz) && (long long)iy * a.nx + ix > (long long)iym * a.nx + ixm) return;  // partner is the q
+    const bool selfconj = ix == ixm && iy == iym && iz == izm;
+    const bool nyq = (2 * ix == a.nx) || (2 * iy == a.ny) || (2 * iz == a.nz);
+    const long long kq = ((long long)iz * a.ny + iy) * a.nx + ix;
+    const long long km = ((long long)izm * a.ny + iym) * a.nx + ixm;
+
+    const double qx = (ix <= a.nx / 2 ? ix : ix - a.nx) * a.twopi_lx;
+    const double qy = (iy <= a.ny / 2 ? iy : iy - a.ny) * a.twopi_ly;
+    const double qz = (iz <= a.nz / 2 ? iz : iz - a.nz) * a.twopi_lz;
+
+    // ---- the l = 1 block of the q frame (as k_ozp), then D^1 = Re(R^1 e^{i x alpha}) ----
+    float D1[9];
+    float2 ph[MM + 1];  // e^{-i mu alpha}, mu = 0..MM (negative mu: the conjugates)
+    {
+        float r3[3], r2[3], r1[3];
+        if (qx == 0.0 && qy == 0.0 && qz == 0.0) { r3[0] = 0; r3[1] = 0; r3[2] = 1; }
+        else { r3[0] = (float)qx; r3[1] = (float)qy; r3[2] = (float)qz; }
+        if (r3[0] != 0.f || r3[1] != 0.f) { r2[0] = -r3[1]; r2[1] = r3[0]; r2[2] = 0; }
+        else { r2[0] = 0; r2[1] = r3[2]; r2[2] = -r3[1]; }
+        const float n3 = sqrtf(r3[0] * r3[0] + r3[1] * r3[1] + r3[2] * r3[2]);
+        const float n2 = sqrtf(r2[0] * r2[0] + r2[1] * r2[1] + r2[2] * r2[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { r3[i] /= n3; r2[i] /= n2; }
+        r1[0] = r2[1] * r3[2] - r2[2] * r3[1];
+        r1[1] = r2[2] * r3[0] - r2[0] * r3[2];
+        r1[2] = r2[0] * r3[1] - r2[1] * r3[0];
+        const float sqrt2 = 1.4142135623730950488016887242097f;
+        float2 R1[9];
+        R1[0] = make_float2((r2[1] + r1[0]) * 0.5f, (r1[1] - r2[0]) * 0.5f);   // (-1,-1)
+        R1[1] = make_float2(r3[0] / sqrt2, r3[1] / sqrt2);                    // (-1, 0)
+        R1[2] = make_float2((r2[1] - r1[0]) * 0.5f, (-r1[1] - r2[0]) * 0.5f);  // (-1, 1)
+        R1[3] = make_float2(r1[2] / sqrt2, -r2[2] / sqrt2);                   // ( 0,-1)
+        R1[4] = make_float2(r3[2], 0.f);                                      // ( 0, 0)
+        R1[5] = make_float2(-r1[2] / sqrt2, -r2[2] / sqrt2);                  // ( 0, 1)
+        R1[6] = make_float2((r2[1] - r1[0]) * 0.5f, (r1[1] + r2[0]) * 0.5f);   // ( 1,-1)
+        R1[7] = make_float2(-r3[0] / sqrt2, r3[1] / sqrt2);                   // ( 1, 0)
+        R1[8] = make_float2((r2[1] + r1[0]) * 0.5f, (r2[0] - r1[1]) * 0.5f);   // ( 1, 1)
+        // e^{-i alpha} = (qx - i qy) / |q_xy| (1 along z), and its powers
+        const float rho = sqrtf((float)(qx * qx + qy * qy));
+        const float2 e1 = rho > 0.f ? make_float2((float)qx / rho, -(float)qy / rho) : make_float2(1.f, 0.f);
+        ph[0] = make_float2(1.f, 0.f);
+#pragma unroll
+        for (int k = 1; k <= MM; ++k) ph[k] = make_float2(ph[k - 1].x * e1.x - ph[k - 1].y * e1.y, ph[k - 1].x * e1.y + ph[k - 1].y * e1.x);
+        // D^1(x, .) = Re(R^1(x, .) e^{+i x alpha}): x = -1 multiplies by e^{-i alpha}, x = 1 by its conjugate
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float2 a0 = R1[j], a2 = R1[6 + j];
+            D1[j] = a0.x * e1.x - a0.y * e1.y;      // x = -1
+            D1[3 + j] = R1[3 + j].x;                // x = 0
+            D1[6 + j] = a2.x * e1.x + a2.y * e1.y;  // x = 1: Re(a2 conj(e1))
+        }
+    }
+    float Dh[NH];
+    if constexpr (MM >= 2) {
+#pragma unroll
+        for (int l = 2; l <= MM; ++l) {
+#pragma unroll
+            for (int m = -l; m <= l; ++m) {
+#pragma unroll
+                for (int m1 = S::m1min(m); m1 <= l; ++m1) {
+                    const int e = S::hidx(l, m, m1);
+                    const int l1 = l - 1;
+                    float val = 0.f;
+                    auto term = [&](int tt, int xm, int xm1, int um, int um1) {
+                        if (um < -l1 || um > l1 || um1 < -l1 || um1 > l1) return;
+                        val += pp.rc[3 * e + tt] * D1[(xm + 1) * 3 + (xm1 + 1)] * ozd_dget<MM, MR, NH>(D1, Dh, l1, um, um1);
+                    };
+                    if (m1 < l) {
+                        if (m == -l) term(0, -1, 0, m + 1, m1);
+                        else if (m == l) term(0, 1, 0, m - 1, m1);
+                        else { term(0, 0, 0, m, m1); term(1, 1, 0, m - 1, m1); term(2, -1, 0, m + 1, m1); }
+                    } else {
+                        if (m == -l) term(0, -1, 1, m + 1, m1 - 1);
+                        else if (m == l) term(0, 1, 1, m - 1, m1 - 1);
+                        else { term(0, 0, 1, m, m1 - 1); term(1, 1, 1, m - 1, m1 - 1); term(2, -1, 1, m + 1, m1 - 1); }
+                    }
+                    Dh[e] = val;
+                }
+            }
+        }
+    }
+    auto phase = [&](int mu) {  // e^{-i mu alpha}
+        const float2 p = ph[mu < 0 ? -mu : mu];
+        return mu < 0 ? make_float2(p.x, -p.y) : p;
+    };
+
+    // ---- forward rotation (:505-523): t = drho e^{-i mu' alpha}, then the real D ----
+#pragma unroll
+    for (int m = 0; m <= MM; ++m)
+#pragma unroll
+        for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+            float2 tq[2 * MM + 1], tm[2 * MM + 1];
+#pragma unroll
+            for (int mup = -m; mup <= m; ++mup) {
+                const size_t off = (size_t)S::pidx(m, mup, mu2) * a.N;
+                const float2 p = phase(mup), x = planes[off + kq], y = planes[off + km];
+                tq[mup + m] = make_float2(x.x * p.x - x.y * p.y, x.x * p.y + x.y * p.x);
+                tm[mup + m] = make_float2(y.x * p.x - y.y * p.y, y.x * p.y + y.y * p.x);
+            }
+            const float sg = (m & 1) ? -1.f : 1.f;
+#pragma unroll
+            for (int khi = -m; khi <= m; ++khi) {
+                float2 s = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int mup = -m; mup <= m; ++mup) {
+                    const float d = ozd_dget<MM, MR, NH>(D1, Dh, m, mup, khi), dm = ozd_dget<MM, MR, NH>(D1, Dh, m, mup, -khi);
+                    s.x = fmaf(tq[mup + m].x, d, s.x);
+                    s.y = fmaf(tq[mup + m].y, d, s.y);
+                    u.x = fmaf(tm[mup + m].x, dm, u.x);
+                    u.y = fmaf(tm[mup + m].y, dm, u.y);
+                }
+                const int o = S::pidx(m, khi, mu2);
+                sq[o * B] = s;
+                smq[o * B] = make_float2(sg * u.x, sg * u.y);
+            }
+        }
+
+    // ---- interpolated c (:534-539) and the OZ sums (:561-606), as k_ozp ----
+    const double nrm = sqrt(qx * qx + qy * qy + qz * qz);
+    const double eff = nrm / a.dq + 1.0;
+    const int iq = (int)eff;
+    const float alpha = (float)(eff - iq);
+    const float2 *c0 = ctab + (size_t)(iq - 1) * a.ncoef;
+    const float2 *c1 = ctab + (size_t)iq * a.ncoef;
+    const float2 *crow = nullptr;
+    if (cq) {
+        const int sx = ix <= a.nx / 2 ? ix : ix - a.nx, sy = iy <= a.ny / 2 ? iy : iy - a.ny, sz = iz <= a.nz / 2 ? iz : iz - a.nz;
+        crow = cq + (size_t)(sx * sx + sy * sy + sz * sz) * a.ncoef;
+    }
+#pragma unroll
+    for (int khi = -MM; khi <= MM; ++khi) {
+        constexpr int BMAX = 2 * (MM / MR + 1) * (MM + 1);
+        float2 gs[BMAX], gm[BMAX];
+        int nb = 0;
+#pragma unroll
+        for (int m = (khi < 0 ? -khi : khi); m <= MM; ++m)
+#pragma unroll
+            for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+                const int ip = S::pidx(m, khi, mu2);
+                float2 s = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
+                int k = 0;
+#pragma unroll
+                for (int n = (khi < 0 ? -khi : khi); n <= MM; ++n)
+#pragma unroll
+                    for (int nu2 = -n / MR; nu2 <= n / MR; ++nu2, ++k) {
+                        const int ia = pp.ia0[ip] + k;
+                        float2 ce;
+                        if (crow) {
+                            ce = crow[ia];
+                        } else {
+                            const float2 A0 = c0[ia], A1 = c1[ia];
+                            ce.x = alpha * A1.x + (1.f - alpha) * A0.x;
+                            ce.y = alpha * A1.y + (1.f - alpha) * A0.y;
+                        }
+                        const int jp = S::pidx(n, khi, nu2 < 0 ? -nu2 : nu2);
+                        if (nu2 < 0) {
+                            ozp_fma(s, ce, sq[jp * B]);
+                            ozp_fma(u, ce, smq[jp * B]);
+                        } else {
+                            ozp_fmac(s, ce, smq[jp * B]);
+                            ozp_fmac(u, ce, sq[jp * B]);
+                        }
+                    }
+                gs[nb] = s;
+                gm[nb] = u;
+                ++nb;
+            }
+        nb = 0;
+#pragma unroll
+        for (int m = (khi < 0 ? -khi : khi); m <= MM; ++m)
+#pragma unroll
+            for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+                const int ip = S::pidx(m, khi, mu2);
+                sq[ip * B] = gs[nb];
+                smq[ip * B] = gm[nb];
+                ++nb;
+            }
+    }
+
+    // ---- back rotation with conj(R) = e^{+i mu' alpha} D (:611-641), straight to the planes ----
+#pragma unroll
+    for (int m = 0; m <= MM; ++m)
+#pragma unroll
+        for (int mu2 = 0; mu2 <= m / MR; ++mu2) {
+            float2 g[2 * MM + 1], gmv[2 * MM + 1];
+#pragma unroll
+            for (int k = -m; k <= m; ++k) {
+                g[k + m] = sq[S::pidx(m, k, mu2) * B];
+                gmv[k + m] = smq[S::pidx(m, k, mu2) * B];
+            }
+            const float sg = (m & 1) ? -1.f : 1.f;
+#pragma unroll
+            for (int khi = -m; khi <= m; ++khi) {  // output (m, mup = khi, mu2)
+                float2 s = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int k = -m; k <= m; ++k) {
+                    const float d = ozd_dget<MM, MR, NH>(D1, Dh, m, khi, k), dm = ozd_dget<MM, MR, NH>(D1, Dh, m, khi, -k);
+                    s.x = fmaf(g[k + m].x, d, s.x);
+                    s.y = fmaf(g[k + m].y, d, s.y);
+                    u.x = fmaf(gmv[k + m].x, dm, u.x);
+                    u.y = fmaf(gmv[k + m].y, dm, u.y);
+                }
+                const float2 p = phase(-khi);  // e^{+i mup alpha}
+                s = make_float2(s.x * p.x - s.y * p.y, s.x * p.y + s.y * p.x);
+                u = make_float2(sg * (u.x * p.x - u.y * p.y), sg * (u.x * p.y + u.y * p.x));
                 if (selfconj && nyq) u.y = -u.y;
                 const size_t off = (size_t)S::pidx(m, khi, mu2) * a.N;
                 if (!selfconj) planes[off + kq] = s;

@@ -95,6 +95,7 @@ struct mdft_handle {
     int um_grid_p = 0, um_grid_g = 0;
     bool ring_p = false, ring_g = false;  // FP32 phase: the bulk-copy ring forms (one CTA per SM)
     bool ozp_ok = false;  // FP32 evaluations use the thread-per-pair k_ozp
+    bool ozd = false;     // ... in its factored-rotation form k_ozd (MDFT_OZ=ozp: the unfactored one)
     OzpParams ozp{};
     DevBuf<float2> ozp_cq;  // c interpolated at every |q|^2 of a cubic grid (empty: interpolate per pair)
     size_t oz_smem = 0, oz_smem32 = 0;
@@ -356,22 +357,23 @@ int launch_fft_t(mdft_handle *h, typename Cplx<T>::t *planes, const void *const 
     return check_cuda(cudaGetLastError(), "fft launch");
 }
 
-// FP32 OZ, thread per pair: the instantiation for (mmax, mrso)
+// FP32 OZ, thread per pair: the instantiation for (mmax, mrso); factored: the form with the
+// rotation matrices split into phases and a real matrix (k_ozd), else k_ozp
 template <int MM, int MR>
-const void *ozp_fn() { return (const void *)k_ozp<MM, MR>; }
-const void *ozp_kernel(int mmax, int mrso) {
+const void *ozp_fn(bool factored) { return factored ? (const void *)k_ozd<MM, MR> : (const void *)k_ozp<MM, MR>; }
+const void *ozp_kernel(int mmax, int mrso, bool factored = false) {
     if (mrso == 2) {
         switch (mmax) {
-            case 0: return ozp_fn<0, 2>();
-            case 1: return ozp_fn<1, 2>();
-            case 2: return ozp_fn<2, 2>();
-            case 3: return ozp_fn<3, 2>();
+            case 0: return ozp_fn<0, 2>(factored);
+            case 1: return ozp_fn<1, 2>(factored);
+            case 2: return ozp_fn<2, 2>(factored);
+            case 3: return ozp_fn<3, 2>(factored);
         }
     } else if (mrso == 1) {
         switch (mmax) {
-            case 0: return ozp_fn<0, 1>();
-            case 1: return ozp_fn<1, 1>();
-            case 2: return ozp_fn<2, 1>();
+            case 0: return ozp_fn<0, 1>(factored);
+            case 1: return ozp_fn<1, 1>(factored);
+            case 2: return ozp_fn<2, 1>(factored);
         }
     }
     return nullptr;
@@ -382,7 +384,7 @@ void launch_ozp(mdft_handle *h, float2 *planes, const float2 *ctab, const Oz2Arg
     const size_t smem = ozp_smem_bytes(g.np);
     const float2 *cq = h->ozp_cq.p;
     void *args[] = {(void *)&planes, (void *)&ctab, (void *)&oz, (void *)&h->ozp, (void *)&cq};
-    cudaLaunchKernel(ozp_kernel(g.mmax, g.mrso), dim3(grid), dim3(kOzpThreads), args, smem, h->stream);
+    cudaLaunchKernel(ozp_kernel(g.mmax, g.mrso, h->ozd), dim3(grid), dim3(kOzpThreads), args, smem, h->stream);
 }
 
 void stage_mark(mdft_handle *h, int i) {
@@ -836,6 +838,9 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         if (fn && build_ozp_params(g, h->ct, h->ozp) && ozp_smem_bytes(g.np) <= dyn_max) {
             if ((rc = allow_smem(fn, maxsmem))) return rc;
             h->ozp_ok = true;
+            const char *ozsel = std::getenv("MDFT_OZ");
+            h->ozd = !(ozsel && std::strcmp(ozsel, "ozp") == 0);
+            if ((rc = allow_smem(ozp_kernel(g.mmax, g.mrso, true), maxsmem))) return rc;
             std::vector<float2> c32(h->ct.c.size() / 2);  // the FP32 table as the kernels read it
             for (size_t i = 0; i < c32.size(); ++i) c32[i] = make_float2((float)h->ct.c[2 * i], (float)h->ct.c[2 * i + 1]);
             std::vector<float2> cq = build_ozp_cq(g, h->ct, c32);

@@ -113,3 +113,32 @@ def test_tensor_core_forms_in_a_mixed_solve(tmp_path, mode, monkeypatch):
     assert r32["evaluations_mixed"] > 0
     assert abs(r32["dG"] - r64["dG"]) <= 0.1, (r32, r64)
     e32.close()
+
+
+@pytest.mark.parametrize("name", ["ion16_m1", "mol16_m2", "mol24_m3", "mol8_m0", "mol64_m3", "mol32x128_m1"])
+def test_oz_factored_rotations(tmp_path, name, monkeypatch):
+    # The FP32 OZ with R(q) = e^{-i mu' alpha} D(q) (k_ozd, the default) against the kernel that
+    # runs the reference's complex recursion (k_ozp, MDFT_OZ=ozp) and against the FP64 oracle,
+    # at the mixed path's bars (energy 2e-6 of |F|, gradient 1e-4 of max|df|); the excess terms
+    # of the two FP32 kernels agree to 1e-5 of |F_exc|.
+    c = cases.ALL_CASES[name]
+    ck = cases.case_ck(tmp_path, c)
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    o.compute_vext(cases.solute_of(c), SV, rvdw=c["rvdw"])
+    monkeypatch.setenv("MDFT_OZ", "ozp")
+    e0 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    monkeypatch.delenv("MDFT_OZ")
+    e1 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    for e in (e0, e1):
+        e.set_vext(o.get_vext())
+    xi = cases.xi_of(c, o.shape)
+    fo, dfo, to = o.energy_grad(xi)
+    f0, df0, t0 = e0.energy_and_gradient(xi)
+    f1, df1, t1 = e1.energy_and_gradient(xi)
+    print("\n%s: F_exc oracle %.12g ozp %.12g ozd %.12g; df err ozd %.3e" % (name, to[2], t0[2], t1[2],
+                                                                            np.abs(df1 - dfo).max() / np.abs(dfo).max()))
+    assert abs(t1[2] - t0[2]) <= 1e-5 * abs(t0[2]), (t1, t0)
+    assert abs(f1 - fo) <= 2e-6 * abs(fo)
+    assert np.abs(df1 - dfo).max() <= 1e-4 * np.abs(dfo).max()
+    e0.close()
+    e1.close()
