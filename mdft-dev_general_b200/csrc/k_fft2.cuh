@@ -18,15 +18,17 @@
 namespace mdft {
 
 __host__ __device__ constexpr int count_factor(int n, int f) { return (n % f == 0 && n > 1) ? 1 + count_factor(n / f, f) : 0; }
-__host__ __device__ constexpr int npass_of(int n) {
-    return count_factor(n, 4) + count_factor(n / (1 << (2 * count_factor(n, 4))), 2) +
-           count_factor(n / (1 << (2 * count_factor(n, 4))) / (1 << count_factor(n / (1 << (2 * count_factor(n, 4))), 2)), 3);
-}
-// radix of pass p for length n: all 4s, then 2s, then 3s
+__host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+// passes of length n: all radix-8 passes, then 4s, 2s and 3s on what is left
+__host__ __device__ constexpr int n8_of(int n) { return count_factor(n, 8); }
+__host__ __device__ constexpr int r8_of(int n) { return n / ipow(8, n8_of(n)); }  // the part after the 8s
+__host__ __device__ constexpr int n4_of(int n) { return count_factor(r8_of(n), 4); }
+__host__ __device__ constexpr int n2_of(int n) { return count_factor(r8_of(n) / ipow(4, n4_of(n)), 2); }
+__host__ __device__ constexpr int n3_of(int n) { return count_factor(r8_of(n) / ipow(4, n4_of(n)) / ipow(2, n2_of(n)), 3); }
+__host__ __device__ constexpr int npass_of(int n) { return n8_of(n) + n4_of(n) + n2_of(n) + n3_of(n); }
+// radix of pass p for length n: all 8s, then 4s, 2s, 3s
 __host__ __device__ constexpr int radix_of(int n, int p) {
-    return p < count_factor(n, 4) ? 4
-           : p < count_factor(n, 4) + count_factor(n / (1 << (2 * count_factor(n, 4))), 2) ? 2
-                                                                                               : 3;
+    return p < n8_of(n) ? 8 : p < n8_of(n) + n4_of(n) ? 4 : p < n8_of(n) + n4_of(n) + n2_of(n) ? 2 : 3;
 }
 // product of the radices before pass p (the Stockham span Ns)
 __host__ __device__ constexpr int span_of(int n, int p) { return p == 0 ? 1 : span_of(n, p - 1) * radix_of(n, p - 1); }
@@ -48,6 +50,35 @@ __device__ __forceinline__ void dft_small(typename Cplx<T>::t (&v)[R], int sign)
         v[1] = cadd(d02, wd);
         v[2] = csub(s02, s13);
         v[3] = csub(d02, wd);
+    } else if constexpr (R == 8) {
+        // radix 2 between j and j + 4, twiddles w^j (w = e^{sign 2 pi i / 8}), then two radix-4
+        // DFTs: the even outputs from the sums, the odd outputs from the twiddled differences
+        const T h = (T)0.70710678118654752440084436210484903928;
+        C a[4], b[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            a[j] = cadd(v[j], v[j + 4]);
+            b[j] = csub(v[j], v[j + 4]);
+        }
+        const T sg = (T)sign;
+        // b1 *= (1 + i sg)/sqrt2, b2 *= i sg, b3 *= (-1 + i sg)/sqrt2
+        C t;
+        t.x = h * (b[1].x - sg * b[1].y);
+        t.y = h * (b[1].y + sg * b[1].x);
+        b[1] = t;
+        t.x = -sg * b[2].y;
+        t.y = sg * b[2].x;
+        b[2] = t;
+        t.x = h * (-b[3].x - sg * b[3].y);
+        t.y = h * (-b[3].y + sg * b[3].x);
+        b[3] = t;
+        dft_small<T, 4>(a, sign);
+        dft_small<T, 4>(b, sign);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[2 * k] = a[k];
+            v[2 * k + 1] = b[k];
+        }
     } else {  // R == 3
         const T c3 = (T)-0.5;
         const T s3 = (T)sign * (T)0.86602540378443864676372317075294;
