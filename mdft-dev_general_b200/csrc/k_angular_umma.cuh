@@ -690,49 +690,79 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_project_ring(const float *_
 }
 
 // Shared-memory plan of k_gather_ring: B hi/lo, A hi/lo, the accumulator tile [128][NO],
-// w(io), and kGrStages stages of one 32-point sub-tile of x, vext and the direction.
+// and kGrStages stages of one 32-point sub-tile of x, vext and the direction.
 constexpr int kGrStages = 3;
 constexpr int kGrSub = 32;                 // points per streamed sub-tile
 constexpr int kGrPer = kUmBM / kGrSub;     // sub-tiles per tile
+// one thread per 4-orientation chunk of a sub-tile: every thread has the same work per stage
+template <int NO> __host__ __device__ constexpr int gather_ring_threads() { return kGrSub * NO / 4; }
 inline size_t gather_ring_smem_bytes(const UmmaShape &s, int no) {
-    return umma_smem_bytes(s) + (size_t)kUmBM * no * 4 + (size_t)round_up(no, 4) * 4 + (size_t)kGrStages * 3 * kGrSub * no * 4;
+    return umma_smem_bytes(s) + (size_t)kUmBM * no * 4 + (size_t)kGrStages * 3 * kGrSub * no * 4;
+}
+
+// log(v) for the ring epilogue: the hardware base-2 logarithm (lg2.approx; absolute error
+// about 2^-22 in log2, below the FP32 rounding of the other terms of df) times ln 2.  v is
+// x^2 > eps / rho0 or 1, never subnormal.
+__device__ __forceinline__ float ring_log(float v) {
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+    return r * 0.693147180559945309417232121458176568f;
 }
 
 // S7 + ideal/external for the FP32 phase (x, vext, df, direction all FP32; NO % 4 == 0):
 // x, vext and the direction of each 32-point sub-tile arrive by bulk copy kGrStages
 // sub-tiles ahead; the projections of the next tile are loaded into registers while the
-// current tile's MMAs run.
+// current tile's MMAs run.  Each thread owns one 4-orientation chunk of every sub-tile
+// (point 4t / NO, orientations 4t % NO ..), so its w(io) stay in registers.
+//
+// Per element (x, vext v, accumulator a = sum_ip conj-product, weight w):
+//   occ = rho0 x^2 > eps;  lg = log x^2 (occ)
+//   df  = 2 rho0 w x (pre a + [occ] (kT lg + v))
+//   F_exc term = pre rho0 w a (x^2 - 1);  F_id term = kT dv rho0 w ([occ] x^2 (lg - 1) + 1);
+//   F_ext term = dv rho0 [occ] w x^2 v
+// (the arithmetic of gather_elem with the constant factors taken out of the sums; the
+// constant part of F_id, kT dv rho0 sum w, is added per tile in FP64).
 template <int NO>
-__global__ void __launch_bounds__(kRingThreads, 1) k_gather_ring(const float2 *__restrict__ planes, const uint16_t *__restrict__ bimg,
+__global__ void __launch_bounds__(gather_ring_threads<NO>(), 1) k_gather_ring(const float2 *__restrict__ planes, const uint16_t *__restrict__ bimg,
                                                                const float *__restrict__ xi, const float *__restrict__ vext,
                                                                const double *__restrict__ w, float *__restrict__ df,
                                                                double *__restrict__ partial, int *__restrict__ err,
                                                                GatherArgs a, UmmaShape s, int ntiles) {
     static_assert(NO % 4 == 0, "vector epilogue needs no % 4 == 0");
+    constexpr int NT = gather_ring_threads<NO>();
+    static_assert(NT % 32 == 0, "whole warps");
+    static_assert(NT <= 1024, "one CTA of at most 1024 threads");
+    constexpr int kWarps = NT / 32, kGroupWarps = kWarps / 4;  // warps per tensor-memory lane quarter
     extern __shared__ __align__(128) unsigned char um_smem[];
     __shared__ uint64_t bar, sfull[kGrStages];
     __shared__ uint32_t tmem_slot;
-    __shared__ double red[kGatherSums][kRingThreads / 32];
+    __shared__ double red[kGatherSums][kWarps];
+    __shared__ double wsum_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int np = a.np, KC = s.Kp / 8;
-    constexpr int kTasks = kUmBM * 8 / kRingThreads;  // 8-element chunks of the P tile per thread (Kp <= 64)
-    if (tid == 0)
+    constexpr int kTasks = (kUmBM * 8 + NT - 1) / NT;  // 8-element chunks of the P tile per thread (Kp <= 64)
+    if (tid == 0) {
         for (int k = 0; k < kGrStages; ++k) mbar_init(&sfull[k], 1);
+        double ws = 0.0;
+        for (int io = 0; io < NO; ++io) ws += w[io];
+        wsum_s = ws;
+    }
     UmmaCta c;
     umma_cta_setup(um_smem, bimg, s, &tmem_slot, &bar, c);  // also fences the barrier inits
     float *vt = reinterpret_cast<float *>(um_smem + umma_smem_bytes(s));  // [128][NO]
-    float *ws = vt + (size_t)kUmBM * NO;
-    float *ring = ws + round_up(NO, 4);  // stage k: x, vext, d of kGrSub points each
-    constexpr int SUB = kGrSub * NO;     // floats per array per sub-tile
-    for (int io = tid; io < NO; io += kRingThreads) ws[io] = (float)w[io];
+    float *ring = vt + (size_t)kUmBM * NO;  // stage k: x, vext, d of kGrSub points each
+    constexpr int SUB = kGrSub * NO;        // floats per array per sub-tile
     const bool want_v = a.do_ideal != 0, want_d = a.dvec != nullptr, store = a.df_mode == 1;
     const float *dvec = static_cast<const float *>(a.dvec);
-    GatherConsts k;
-    k.pre = (float)(a.prefactor * a.cst);
-    k.r0 = (float)a.rho0;
-    k.kT = (float)a.kT;
-    k.dv = (float)a.dv;
-    k.kTdv = (float)(a.kT * a.dv);
+    const float pre = (float)(a.prefactor * a.cst), kT = (float)a.kT;
+    const float er0 = (float)(2.220446049250313080847263336181640625e-16 / a.rho0);  // rho0 x^2 > eps
+    const int io0 = (4 * tid) % NO;
+    float wv[4], w2v[4];  // w(io) and 2 rho0 w(io) of this thread's orientations
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        wv[u] = (float)w[io0 + u];
+        w2v[u] = (float)(2.0 * a.rho0 * w[io0 + u]);
+    }
     const int nmine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int nsub = kGrPer * nmine;
     auto tile0 = [&](int i) { return (long long)((int)blockIdx.x + i * (int)gridDim.x) * kUmBM; };
@@ -751,15 +781,17 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_gather_ring(const float2 *_
     };
     if (tid == 0)
         for (int G = 0; G < kGrStages && G < nsub; ++G) copy_sub(G);
-    __syncthreads();  // ws
+    __syncthreads();  // wsum_s
+    const double cid = a.kT * a.dv * a.rho0, cext = a.dv * a.rho0, cexc = (double)pre * a.rho0;
+    const double tile_id = want_v ? cid * (double)kUmBM * wsum_s : 0.0;  // constant part of F_id per tile
     double fid = 0.0, fext = 0.0, fexc = 0.0, gdv = 0.0, gmx = 0.0, gun = 0.0;
     float pv[kTasks][8];
-    if (nmine > 0) gather_load<kRingThreads, kTasks>(planes, a.N, tile0(0), np, KC, pv);
+    if (nmine > 0) gather_load<NT, kTasks>(planes, a.N, tile0(0), np, KC, pv);
     bool aborted = false;  // a failed wait anywhere in the block, seen through the barrier's OR
     for (int i = 0; i < nmine && !aborted; ++i) {
 #pragma unroll
         for (int q = 0; q < kTasks; ++q) {
-            const int t = tid + q * kRingThreads;
+            const int t = tid + q * NT;
             const int m = t % kUmBM, kc = t / kUmBM;
             if (kc < KC) store_split8(c, s.Kp, m, 8 * kc, pv[q]);
         }
@@ -770,15 +802,15 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_gather_ring(const float2 *_
             umma_issue(c, s, &bar);
             ++miss;
         }
-        if (i + 1 < nmine) gather_load<kRingThreads, kTasks>(planes, a.N, tile0(i + 1), np, KC, pv);
+        if (i + 1 < nmine) gather_load<NT, kTasks>(planes, a.N, tile0(i + 1), np, KC, pv);
         const bool ok = umma::wait_phase(&bar, (uint32_t)(i & 1));
         if (tid == 0 && ok) ++mdone;
         if (__syncthreads_or(!ok)) { aborted = true; break; }
         umma::fence_after_sync();
-        {
+        if (warp < 4 * kGroupWarps) {
             const int q4 = warp & 3, h = warp >> 2;
             const int r = 32 * q4 + lane;
-            for (int cc = h; cc < s.Np / 16; cc += kRingThreads / 128) {
+            for (int cc = h; cc < s.Np / 16; cc += kGroupWarps) {
                 float acc[16];
                 umma::ld16(c.tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(16 * cc), acc);
                 umma::ld_wait();
@@ -791,8 +823,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_gather_ring(const float2 *_
         }
         umma::fence_before_sync();
         __syncthreads();  // accumulator tile complete; tensor memory free for the next tile's MMAs
-        // the tile's terms of each sum in FP32 (about 21 per thread), then one FP64 addition per
-        // sum: the FP32 -> FP64 conversions stay off the per-element path
+        // the tile's terms of each sum in FP32 (kGrPer * 4 per thread), then one FP64 addition
+        // per sum: the FP32 -> FP64 conversions stay off the per-element path
         float tid_ = 0.f, text = 0.f, texc = 0.f, tgd = 0.f, tgm = 0.f, tgu = 0.f;
         for (int j = 0; j < kGrPer; ++j) {
             const int G = kGrPer * i + j, st = G % kGrStages;
@@ -801,34 +833,41 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_gather_ring(const float2 *_
             if (okc) {
                 const float *xsv = ring + (size_t)st * 3 * SUB, *vsv = xsv + SUB, *dsv = xsv + 2 * SUB;
                 const float *acc = vt + (size_t)kGrSub * j * NO;
-                const long long e0 = (tile0(i) + (long long)kGrSub * j) * NO;
-                for (int ch = tid; ch < SUB / 4; ch += kRingThreads) {
-                    const int io = (4 * ch) % NO;
-                    const float4 xv = reinterpret_cast<const float4 *>(xsv)[ch];
-                    const float4 vv = want_v ? reinterpret_cast<const float4 *>(vsv)[ch] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    const float4 av = reinterpret_cast<const float4 *>(acc)[ch];
-                    const float4 wv = *reinterpret_cast<const float4 *>(ws + io);
-                    const float gx = gather_elem_f(k, want_v, av.x, wv.x, xv.x, vv.x, tid_, text, texc);
-                    const float gy = gather_elem_f(k, want_v, av.y, wv.y, xv.y, vv.y, tid_, text, texc);
-                    const float gz = gather_elem_f(k, want_v, av.z, wv.z, xv.z, vv.z, tid_, text, texc);
-                    const float gw = gather_elem_f(k, want_v, av.w, wv.w, xv.w, vv.w, tid_, text, texc);
-                    if (store) {
-                        *reinterpret_cast<float4 *>(df + e0 + 4 * ch) = make_float4(gx, gy, gz, gw);
-                        if (want_d) {
-                            const float4 dd = reinterpret_cast<const float4 *>(dsv)[ch];
-                            tgd = fmaf(gx, dd.x, fmaf(gy, dd.y, fmaf(gz, dd.z, fmaf(gw, dd.w, tgd))));
-                        }
-                        tgm = fmaxf(tgm, fmaxf(fmaxf(fabsf(gx), fabsf(gy)), fmaxf(fabsf(gz), fabsf(gw))));
-                        tgu = fmaf(gx, wv.x, fmaf(gy, wv.y, fmaf(gz, wv.z, fmaf(gw, wv.w, tgu))));
+                const float4 x4 = reinterpret_cast<const float4 *>(xsv)[tid];
+                const float4 v4 = want_v ? reinterpret_cast<const float4 *>(vsv)[tid] : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 a4 = reinterpret_cast<const float4 *>(acc)[tid];
+                const float xs[4] = {x4.x, x4.y, x4.z, x4.w}, vs[4] = {v4.x, v4.y, v4.z, v4.w}, as[4] = {a4.x, a4.y, a4.z, a4.w};
+                float g[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float x = xs[u], x2 = x * x;
+                    const bool occ = want_v && x2 > er0;
+                    const float lg = ring_log(occ ? x2 : 1.0f);
+                    const float wx2 = occ ? wv[u] * x2 : 0.0f;
+                    tid_ = fmaf(wx2, lg - 1.0f, tid_);
+                    text = fmaf(wx2, vs[u], text);
+                    const float inner = occ ? fmaf(kT, lg, vs[u]) : 0.0f;
+                    g[u] = (w2v[u] * x) * fmaf(pre, as[u], inner);
+                    texc = fmaf(wv[u] * as[u], fmaf(x, x, -1.0f), texc);
+                }
+                if (store) {
+                    const long long e0 = (tile0(i) + (long long)kGrSub * j) * NO;
+                    *reinterpret_cast<float4 *>(df + e0 + 4 * tid) = make_float4(g[0], g[1], g[2], g[3]);
+                    if (want_d) {
+                        const float4 dd = reinterpret_cast<const float4 *>(dsv)[tid];
+                        tgd = fmaf(g[0], dd.x, fmaf(g[1], dd.y, fmaf(g[2], dd.z, fmaf(g[3], dd.w, tgd))));
                     }
+                    tgm = fmaxf(tgm, fmaxf(fmaxf(fabsf(g[0]), fabsf(g[1])), fmaxf(fabsf(g[2]), fabsf(g[3]))));
+                    tgu = fmaf(g[0], wv[0], fmaf(g[1], wv[1], fmaf(g[2], wv[2], fmaf(g[3], wv[3], tgu))));
                 }
             }
             if (__syncthreads_or(!okc)) { aborted = true; break; }  // stage st consumed by every thread
             if (tid == 0 && G + kGrStages < nsub) copy_sub(G + kGrStages);
         }
-        fid += (double)tid_;
-        fext += (double)text;
-        fexc += (double)texc;
+        if (tid == 0) fid += tile_id;
+        fid += cid * (double)tid_;
+        fext += cext * (double)text;
+        fexc += cexc * (double)texc;
         gdv += (double)tgd;
         gmx = fmax(gmx, (double)tgm);
         gun += (double)tgu;
@@ -864,7 +903,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_gather_ring(const float2 *_
     __syncthreads();
     if (tid == 0) {
         double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
-        for (int kk = 0; kk < kRingThreads / 32; ++kk) {
+        for (int kk = 0; kk < kWarps; ++kk) {
             s0 += red[0][kk];
             s1 += red[1][kk];
             s2 += red[2][kk];

@@ -174,15 +174,58 @@ __global__ void __launch_bounds__(xy_threads<T, N>(), (xy_threads<T, N>() <= 512
 template <typename T, int N> __host__ __device__ constexpr size_t xy_smem_bytes() { return sizeof(typename Cplx<T>::t) * (N + (size_t)N * (N + 1)); }
 
 // Persistent form of k_fft_xy: each CTA walks the planes blockIdx.x, +gridDim.x, ...  A plane
-// (N x N contiguous values) arrives by one bulk copy into one of two shared-memory buffers
-// while the other is transformed, and leaves by one bulk store.  The Stockham passes read
-// and write the unpadded plane without bank conflicts (x: consecutive threads take
-// consecutive points of a line; y: consecutive lines).  Waits are bounded; a wait that runs
+// (N x N contiguous values) arrives by bulk copy into one of two shared-memory buffers while
+// the other is transformed, and leaves by bulk store.  Waits are bounded; a wait that runs
 // out sets *err and the CTA stops.
+//
+// FP32, N = 64 (two radix-8 passes per axis): rows are stored 72 values apart (the copies go
+// row by row), so that the four rows one warp touches fall on alternate halves of the
+// shared-memory banks, and the first x pass writes its outputs 8j + r at 9j + r (an 8 x 9
+// padded transpose); with that, every pass reads and writes without bank conflicts.
+// Otherwise the plane is one contiguous copy and the x passes take consecutive points of a
+// line per thread (y: consecutive lines).
+template <typename T, int N> __host__ __device__ constexpr bool xy_padded() { return N == 64 && sizeof(T) == 4; }
+template <typename T, int N> __host__ __device__ constexpr int xy_row() { return xy_padded<T, N>() ? 72 : N; }
 template <typename T, int N> __host__ __device__ constexpr size_t xy_tma_smem_bytes() {
-    return sizeof(typename Cplx<T>::t) * (2 * (size_t)N * N + N);
+    return sizeof(typename Cplx<T>::t) * (2 * (size_t)N * xy_row<T, N>() + N);
 }
 template <typename T, int N> __host__ __device__ constexpr bool xy_tma_fits() { return xy_tma_smem_bytes<T, N>() <= 200 * 1024; }
+
+// The x transforms of a padded 64 x 64 plane (row stride 72): thread t takes butterfly
+// j = t % 8 of row t / 8 in both radix-8 passes.  A warp owns its four rows, so only warp
+// barriers separate the passes; the caller's block barrier follows.
+template <typename T, int THREADS>
+__device__ __forceinline__ void fft64_rows_padded(typename Cplx<T>::t *buf, const typename Cplx<T>::t *tw, int sign) {
+    using C = typename Cplx<T>::t;
+    constexpr int P = 72;
+    static_assert(THREADS == 512, "one butterfly of one row per thread");
+    const int j = threadIdx.x & 7;
+    C *b = buf + (threadIdx.x >> 3) * P;
+    C v[8];
+    // pass 1 (span 1): inputs j + 8r, outputs 8j + r stored at 9j + r
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = b[j + 8 * r];
+    dft_small<T, 8>(v, sign);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) b[9 * j + r] = v[r];
+    __syncwarp();
+    // pass 2 (span 8): inputs j + 8r (stored at 9r + j) twiddled by w^(jr), outputs j + 8r
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        C x = b[9 * r + j];
+        if (r > 0) {
+            C w = tw[(j * r) & 63];
+            if (sign < 0) w.y = -w.y;
+            x = cmul(x, w);
+        }
+        v[r] = x;
+    }
+    dft_small<T, 8>(v, sign);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) b[j + 8 * r] = v[r];
+}
 
 template <typename T, int N>
 __global__ void __launch_bounds__(xy_threads<T, N>()) k_fft_xy_tma(typename Cplx<T>::t *__restrict__ data,
@@ -190,50 +233,72 @@ __global__ void __launch_bounds__(xy_threads<T, N>()) k_fft_xy_tma(typename Cplx
                                                                   long long nplanes, int *__restrict__ err) {
     using C = typename Cplx<T>::t;
     constexpr int THREADS = xy_threads<T, N>();
-    constexpr uint32_t kPlane = (uint32_t)(sizeof(C) * N * N);
+    constexpr bool PAD = xy_padded<T, N>();
+    constexpr int P = xy_row<T, N>();  // row stride in shared memory
+    constexpr uint32_t kPlane = (uint32_t)(sizeof(C) * N * N), kRow = (uint32_t)(sizeof(C) * N);
     extern __shared__ __align__(128) unsigned char xyt_smem[];
     C *buf0 = reinterpret_cast<C *>(xyt_smem);
-    C *twl = buf0 + 2 * N * N;
+    C *twl = buf0 + 2 * N * P;
     __shared__ uint64_t full[2];
     __shared__ int abort_flag;
     const int tid = threadIdx.x;
     const long long nmine = (long long)blockIdx.x < nplanes ? (nplanes - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    // warp 0: the plane's copy into buffer `dst` (one copy, or N row copies two per lane)
+    auto load_plane = [&](C *dst, const C *src, uint64_t *bar) {
+        if (tid == 0) mbar_arrive_expect_tx(bar, kPlane);
+        if constexpr (PAD) {
+            __syncwarp();
+            for (int r = tid; r < N; r += 32) bulk_load(dst + r * P, src + r * N, kRow, bar);
+        } else if (tid == 0) {
+            bulk_load(dst, src, kPlane, bar);
+        }
+    };
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
         mbar_fence_init();
         abort_flag = 0;
-        if (nmine > 0) {
-            mbar_arrive_expect_tx(&full[0], kPlane);
-            bulk_load(buf0, data + (size_t)blockIdx.x * N * N, kPlane, &full[0]);
-        }
+    }
+    if (tid < 32 && nmine > 0) {
+        __syncwarp();
+        load_plane(buf0, data + (size_t)blockIdx.x * N * N, &full[0]);
     }
     for (int i = tid; i < N; i += THREADS) twl[i] = tw[i];
     __syncthreads();
     long long i = 0;
     for (; i < nmine; ++i) {
         const int s = (int)(i & 1);
-        C *buf = buf0 + s * N * N;
+        C *buf = buf0 + s * N * P;
         const long long p = blockIdx.x + i * gridDim.x;
-        if (tid == 0 && i + 1 < nmine) {
-            bulk_wait_read_all();  // the other buffer's last store has been read out
-            mbar_arrive_expect_tx(&full[s ^ 1], kPlane);
-            bulk_load(buf0 + (s ^ 1) * N * N, data + (size_t)(p + gridDim.x) * N * N, kPlane, &full[s ^ 1]);
+        if (tid < 32 && i + 1 < nmine) {
+            bulk_wait_read_all();  // the other buffer's last stores (this lane's) have been read out
+            __syncwarp();
+            load_plane(buf0 + (s ^ 1) * N * P, data + (size_t)(p + gridDim.x) * N * N, &full[s ^ 1]);
         }
         if (!mbar_wait(&full[s], (uint32_t)((i >> 1) & 1))) abort_flag = 1;
         __syncthreads();
         if (abort_flag) break;
-        fft_lines<T, N, 0, N, THREADS, false>(buf, 1, N, twl, sign);  // along x: line = y
-        fft_lines<T, N, 0, N, THREADS, true>(buf, N, 1, twl, sign);   // along y: line = x
+        if constexpr (PAD) {
+            fft64_rows_padded<T, THREADS>(buf, twl, sign);  // along x
+            __syncthreads();
+        } else {
+            fft_lines<T, N, 0, N, THREADS, false>(buf, 1, N, twl, sign);  // along x: line = y
+        }
+        fft_lines<T, N, 0, N, THREADS, true>(buf, P, 1, twl, sign);             // along y: line = x
         fence_proxy_async_smem();
         __syncthreads();
-        if (tid == 0) {
+        if constexpr (PAD) {
+            if (tid < 32) {
+                for (int r = tid; r < N; r += 32) bulk_store(data + (size_t)p * N * N + r * N, buf + r * P, kRow);
+                bulk_commit();
+            }
+        } else if (tid == 0) {
             bulk_store(data + (size_t)p * N * N, buf, kPlane);
             bulk_commit();
         }
     }
-    if (tid == 0) {
-        if (abort_flag) {
+    if (tid < 32) {
+        if (tid == 0 && abort_flag) {
             atomicExch(err, 1);
             // the copy issued for the next plane gets a bounded wait before the CTA exits
             if (i + 1 < nmine) (void)mbar_wait(&full[(i + 1) & 1], (uint32_t)(((i + 1) >> 1) & 1));
@@ -263,9 +328,20 @@ __global__ void __launch_bounds__(256) k_fft_z(typename Cplx<T>::t *__restrict__
     C *g = data + p * plane + iy * nx + ix0;
     const long long zs = (long long)nx * ny;
     for (int i = threadIdx.x; i < N; i += 256) twl[i] = tw[i];
-    for (int f = threadIdx.x; f < N * TL; f += 256) {
-        const int i = f / TL, l = f % TL;
-        buf[i * LD + l] = g[i * zs + l];
+    {
+        // all loads of the column tile in flight before the first shared-memory store
+        constexpr int PER = (N * TL + 255) / 256;
+        C t[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int f = threadIdx.x + 256 * k;
+            if ((N * TL) % 256 == 0 || f < N * TL) t[k] = g[(f / TL) * zs + f % TL];
+        }
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int f = threadIdx.x + 256 * k;
+            if ((N * TL) % 256 == 0 || f < N * TL) buf[(f / TL) * LD + f % TL] = t[k];
+        }
     }
     __syncthreads();
     fft_lines<T, N, 0, TL, 256, true>(buf, LD, 1, twl, sign);
