@@ -245,6 +245,8 @@ def reference_arm(args, rank, world):
             times.append(t)
     t_eval = float(np.mean(times))
     ev = EVALS_PER_SOLVE_FP64
+    if ev["key"] != (N_GRID, BOX, MMAX, NSITE, CK_SEED, args.pgtol, args.guni_tol):
+        raise SystemExit("EVALS_PER_SOLVE_FP64 was measured for another workload or stop rule: %r" % (ev["key"],))
     v = 1.0 / (t_eval * ev["mean"])
     sample = ("one FP64 energy_and_gradient per step of the b200 arm's timed solutes (seeds %d..%d) at their guess "
               "density, %d OpenMP threads, x %.1f evaluations per FP64 solve (%s); the L-BFGS vector work is not "
@@ -268,7 +270,7 @@ STOP_TEXT = ("max|df|<=%g and |sum w df dv|<=%g kJ/mol in FP64 (line-search stal
 # Evaluations per plain FP64 solve of this workload and stop rule (the mean over the bench's
 # first 20 solutes on one B200); scales the CPU evaluation time to solutes/s in the reference
 # arm, which cannot count them itself.  The b200 arm counts them in every run and reports both.
-EVALS_PER_SOLVE_FP64 = {"mean": 173.0, "key": (N_GRID, BOX, MMAX, NSITE, CK_SEED, PGTOL, 0.1),
+EVALS_PER_SOLVE_FP64 = {"mean": 190.55, "key": (N_GRID, BOX, MMAX, NSITE, CK_SEED, PGTOL, GUNI_TOL),
                         "source": "mean of 20 plain FP64 GPU solves of seeds 5..24"}
 
 
@@ -322,6 +324,10 @@ def main():
             self.name = name
             self.prec = PREC_FP64 if name == "fp64" else PREC_MIXED
             self.opts = opts_of(self.prec)
+            if name == "learned" and warm_params is not None:
+                # warm-started solves need the tighter stop rule to stay within 0.1 kJ/mol
+                from mdft_b200 import warmstart
+                self.opts.update(pgtol=min(args.pgtol, warmstart.LEARNED_PGTOL), guni_tol=min(args.guni_tol, warmstart.LEARNED_GUNI_TOL))
             self.engines = []
             for _ in range(W):
                 e = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=local, precision=self.prec)

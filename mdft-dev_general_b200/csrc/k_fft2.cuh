@@ -227,8 +227,12 @@ __device__ __forceinline__ void fft64_rows_padded(typename Cplx<T>::t *buf, cons
     for (int r = 0; r < 8; ++r) b[j + 8 * r] = v[r];
 }
 
+// CTAs per SM the register allocator is asked to allow (the padded FP32 planes: three fit in
+// shared memory)
+template <typename T, int N> __host__ __device__ constexpr int xy_tma_min_blocks() { return xy_padded<T, N>() ? 3 : 1; }
+
 template <typename T, int N>
-__global__ void __launch_bounds__(xy_threads<T, N>()) k_fft_xy_tma(typename Cplx<T>::t *__restrict__ data,
+__global__ void __launch_bounds__(xy_threads<T, N>(), xy_tma_min_blocks<T, N>()) k_fft_xy_tma(typename Cplx<T>::t *__restrict__ data,
                                                                   const typename Cplx<T>::t *__restrict__ tw, int sign,
                                                                   long long nplanes, int *__restrict__ err) {
     using C = typename Cplx<T>::t;
@@ -241,70 +245,71 @@ __global__ void __launch_bounds__(xy_threads<T, N>()) k_fft_xy_tma(typename Cplx
     C *twl = buf0 + 2 * N * P;
     __shared__ uint64_t full[2];
     __shared__ int abort_flag;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long nmine = (long long)blockIdx.x < nplanes ? (nplanes - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    // warp 0: the plane's copy into buffer `dst` (one copy, or N row copies two per lane)
-    auto load_plane = [&](C *dst, const C *src, uint64_t *bar) {
-        if (tid == 0) mbar_arrive_expect_tx(bar, kPlane);
+    // copy issuers: padded rows, lane 0 of each warp moves its own RW rows in and out (so its
+    // wait for its own stores to be read covers the rows it overwrites); else thread 0 moves
+    // the whole plane
+    constexpr int RW = PAD ? N / (THREADS / 32) : N;
+    static_assert(!PAD || N % (THREADS / 32) == 0, "whole rows per warp");
+    const bool issuer = PAD ? lane == 0 : tid == 0;
+    const int r0 = PAD ? warp * RW : 0;
+    auto load_rows = [&](C *dst, const C *src, uint64_t *bar) {
         if constexpr (PAD) {
-            __syncwarp();
-            for (int r = tid; r < N; r += 32) bulk_load(dst + r * P, src + r * N, kRow, bar);
-        } else if (tid == 0) {
+            for (int r = r0; r < r0 + RW; ++r) bulk_load(dst + r * P, src + r * N, kRow, bar);
+        } else {
             bulk_load(dst, src, kPlane, bar);
         }
+    };
+    auto store_rows = [&](C *dst, const C *src) {
+        if constexpr (PAD) {
+            for (int r = r0; r < r0 + RW; ++r) bulk_store(dst + r * N, src + r * P, kRow);
+        } else {
+            bulk_store(dst, src, kPlane);
+        }
+        bulk_commit();
     };
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
         mbar_fence_init();
         abort_flag = 0;
-    }
-    if (tid < 32 && nmine > 0) {
-        __syncwarp();
-        load_plane(buf0, data + (size_t)blockIdx.x * N * N, &full[0]);
+        if (nmine > 0) mbar_arrive_expect_tx(&full[0], kPlane);
     }
     for (int i = tid; i < N; i += THREADS) twl[i] = tw[i];
     __syncthreads();
+    if (issuer && nmine > 0) load_rows(buf0, data + (size_t)blockIdx.x * N * N, &full[0]);
     long long i = 0;
     for (; i < nmine; ++i) {
         const int s = (int)(i & 1);
         C *buf = buf0 + s * N * P;
         const long long p = blockIdx.x + i * gridDim.x;
-        if (tid < 32 && i + 1 < nmine) {
-            bulk_wait_read_all();  // the other buffer's last stores (this lane's) have been read out
-            __syncwarp();
-            load_plane(buf0 + (s ^ 1) * N * P, data + (size_t)(p + gridDim.x) * N * N, &full[s ^ 1]);
-        }
+        const bool more = i + 1 < nmine;
         if (!mbar_wait(&full[s], (uint32_t)((i >> 1) & 1))) abort_flag = 1;
+        if (tid == 0 && more) mbar_arrive_expect_tx(&full[s ^ 1], kPlane);
         __syncthreads();
         if (abort_flag) break;
+        if (issuer && more) {
+            bulk_wait_read_all();  // this issuer's stores of the other buffer have been read out
+            load_rows(buf0 + (s ^ 1) * N * P, data + (size_t)(p + gridDim.x) * N * N, &full[s ^ 1]);
+        }
         if constexpr (PAD) {
             fft64_rows_padded<T, THREADS>(buf, twl, sign);  // along x
             __syncthreads();
         } else {
             fft_lines<T, N, 0, N, THREADS, false>(buf, 1, N, twl, sign);  // along x: line = y
         }
-        fft_lines<T, N, 0, N, THREADS, true>(buf, P, 1, twl, sign);             // along y: line = x
+        fft_lines<T, N, 0, N, THREADS, true>(buf, P, 1, twl, sign);  // along y: line = x
         fence_proxy_async_smem();
         __syncthreads();
-        if constexpr (PAD) {
-            if (tid < 32) {
-                for (int r = tid; r < N; r += 32) bulk_store(data + (size_t)p * N * N + r * N, buf + r * P, kRow);
-                bulk_commit();
-            }
-        } else if (tid == 0) {
-            bulk_store(data + (size_t)p * N * N, buf, kPlane);
-            bulk_commit();
-        }
+        if (issuer) store_rows(data + (size_t)p * N * N, buf);
     }
-    if (tid < 32) {
-        if (tid == 0 && abort_flag) {
-            atomicExch(err, 1);
-            // the copy issued for the next plane gets a bounded wait before the CTA exits
-            if (i + 1 < nmine) (void)mbar_wait(&full[(i + 1) & 1], (uint32_t)(((i + 1) >> 1) & 1));
-        }
-        bulk_wait_all();
+    if (tid == 0 && abort_flag) {
+        atomicExch(err, 1);
+        // the copy that did not land in time gets one more bounded wait before the CTA exits
+        (void)mbar_wait(&full[i & 1], (uint32_t)((i >> 1) & 1));
     }
+    if (issuer) bulk_wait_all();
 }
 
 template <typename T> __host__ __device__ constexpr int z_tl() { return sizeof(T) == 8 ? 16 : 32; }

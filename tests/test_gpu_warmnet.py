@@ -237,25 +237,33 @@ def test_warm_started_solve_reaches_the_cold_result(sys16, precision):
 
 
 @pytest.mark.skipif(not os.path.exists(warmstart.WEIGHTS), reason="no trained parameters in the package")
-def test_trained_network_against_cold_solves(tmp_path):
+def test_trained_network_against_cold_solves(tmp_path, record_property):
     """Held-out 1-30-site solutes at 64^3 (seeds outside the training set): the trained
     network's start is much closer to the converged density than the bulk guess (masked
-    squared error of the m <= 1 log-density projections), and warm-started mixed solves reach
-    max|df| <= 1e-4 at the cold solves' dG; the evaluation counts of both are printed."""
+    squared error of the m <= 1 log-density projections).  Cold mixed solves with the bench's
+    stop rule (max|df| <= 1e-4, |sum w df dv| <= 0.1) and warm-started ones with the learned
+    form's tighter rule (5e-5, 0.05; with the bench's rule one held-out warm solve in twelve
+    stopped 0.133 kJ/mol off) land within 0.1 kJ/mol of an FP64 solve to max|df| <= 1e-6.
+    The warm/cold evaluation ratio is recorded (junit property warm_cold_evaluation_ratio)
+    and bounded."""
     params, meta = warmstart.load_params()
     ck = str(tmp_path / "ck.dat")
     synth.make_ck_file(ck, 3, seed=warmstart.CK_SEED, kmax=12.0)
-    opts = dict(m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=3000, precision=PREC_MIXED)
+    opts = dict(m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=3000, precision=PREC_MIXED, guni_tol=0.1)
+    warm_opts = dict(opts, pgtol=warmstart.LEARNED_PGTOL, guni_tol=warmstart.LEARNED_GUNI_TOL)
+    ref_opts = dict(m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, precision=0, guni_tol=0.01)
     e = Engine(64, 32.0, 3, ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    ref = Engine(64, 32.0, 3, ck, temperature=SV.temperature, n0=SV.n0, precision=0)
     net = warmstart.WarmNet(64, params=params)
     n3 = 64 ** 3
     feat = torch.empty((3, n3), device="cuda")
     tgt = torch.empty((4, n3), device="cuda")
     mask = torch.empty((n3,), device="cuda")
     pred = torch.empty((4, n3), device="cuda")
-    evals = []
+    rows = []
     for sd in (50000000, 50000001, 50000002):
         sol = warmstart.centred(warmstart.config4_solute(sd), e.box)
+        dg_ref = ref.solve(sol, SV, **ref_opts)["dG"]
         e.set_warm_net(None)
         rc = e.solve(sol, SV, **opts)
         e.warm_target(tgt.data_ptr(), mask.data_ptr())
@@ -267,13 +275,24 @@ def test_trained_network_against_cold_solves(tmp_path):
         err_bulk = float(((tgt ** 2).sum(0) * mask).sum())
         assert err_net < 0.1 * err_bulk, (sd, err_net, err_bulk)
         e.set_warm_net(net)
-        rw = e.solve(sol, SV, **opts)
-        assert rw["status"] == 0 and rw["pgnorm"] <= 1e-4
-        assert abs(rw["dG"] - rc["dG"]) <= 0.15, (sd, rw["dG"], rc["dG"])
-        evals.append((rc["evaluations"] + rc["evaluations_mixed"], rw["evaluations"] + rw["evaluations_mixed"],
-                      round(err_net / err_bulk, 4)))
-    print("held-out (cold evaluations, warm evaluations, start error ratio):", evals, "trained:",
-          {k: meta.get(k) for k in ("train", "epochs", "final_val_loss")})
+        rw = e.solve(sol, SV, **warm_opts)
+        assert rw["status"] == 0 and rw["pgnorm"] <= warmstart.LEARNED_PGTOL
+        assert abs(rc["dG"] - dg_ref) <= 0.1, (sd, rc["dG"], dg_ref)
+        assert abs(rw["dG"] - dg_ref) <= 0.1, (sd, rw["dG"], dg_ref)
+        rows.append((rc["evaluations"] + rc["evaluations_mixed"], rw["evaluations"] + rw["evaluations_mixed"],
+                     round(err_net / err_bulk, 4), round(rc["dG"] - dg_ref, 4), round(rw["dG"] - dg_ref, 4)))
+    cold = sum(r[0] for r in rows)
+    warm = sum(r[1] for r in rows)
+    ratio = warm / cold
+    record_property("warm_cold_evaluation_ratio", round(ratio, 4))
+    record_property("held_out_rows", rows)
+    print("held-out (cold evaluations, warm evaluations, start error ratio, cold dG error, warm dG error):", rows,
+          "warm/cold evaluations: %.3f" % ratio, "trained:", {k: meta.get(k) for k in ("train", "epochs", "final_val_loss")})
+    # measured 1.13 on these seeds (warm at the tighter rule against cold at the bench's): the
+    # start gains nothing in evaluations, so the bench keeps the cold start; the bound catches
+    # a start that costs more
+    assert ratio <= 1.25, rows
     e.set_warm_net(None)
-    e.close()
+    for x in (e, ref):
+        x.close()
     net.close()
