@@ -37,6 +37,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return done != 0;
 }
 
+// one arrival on bar (no transaction bytes)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Named barrier `id` over the first `n` threads of the block (n a multiple of 32; id 0 is
+// __syncthreads'): wait, and wait with an OR of `pred` over the n threads.
+__device__ __forceinline__ void named_sync(uint32_t id, uint32_t n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ bool named_sync_or(uint32_t id, uint32_t n, bool pred) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(out)
+        : "r"((uint32_t)pred), "r"(id), "r"(n)
+        : "memory");
+    return out != 0;
+}
+
 // Wait for the phase with the given parity to complete; false after kWaitLimit polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     for (unsigned it = 0; it < kWaitLimit; ++it)

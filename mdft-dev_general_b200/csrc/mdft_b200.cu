@@ -495,7 +495,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
         if (x32 && v84 && h->ring_g) {
             const int rgrid = std::min(ntiles, h->nsm);
             const size_t rs = gather_ring_smem_bytes(h->um_gs, 84);
-            constexpr int rt = gather_ring_threads<84>();
+            constexpr int rt = gather_ring_block<84>();
             k_gather_ring<84><<<rgrid, rt, rs, h->stream>>>(pl, h->um_gimg.p, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
             red_blocks = rgrid;
         } else if (x32 && v84)
