@@ -83,6 +83,8 @@ def parse():
                     help="profiling mode: only N solves of the workload (no timing, no reference solves)")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
+    ap.add_argument("--fft-compare", action="store_true",
+                    help="timing comparison: the engine's FFT stages against cuFFT (torch.fft) on the same planes")
     return ap.parse_args()
 
 
@@ -274,6 +276,45 @@ EVALS_PER_SOLVE_FP64 = {"mean": 190.55, "key": (N_GRID, BOX, MMAX, NSITE, CK_SEE
                         "source": "mean of 20 plain FP64 GPU solves of seeds 5..24"}
 
 
+def fft_compare(n, box, ck, sv, sol, rvdw, device):
+    """The engine's forward and inverse 3-D FFT stages (np planes of n^3 complex, in place,
+    live CUDA-event stage times averaged over one solve) against cuFFT through torch.fft on a
+    tensor of the same shape (out of place, plan cached, the same sign conventions, no
+    scaling).  A timing comparison only: cuFFT is not on the engine's path."""
+    import torch
+    from mdft_b200 import Engine, PREC_FP64, PREC_MIXED
+    res = {"metric": "3-D FFT stage time, %d planes of %d^3" % (0, n), "unit": "ms", "workload": WORKLOAD % (N_GRID, BOX, MMAX, NSITE)}
+    for name, prec, dt in (("fp32", PREC_MIXED, torch.complex64), ("fp64", PREC_FP64, torch.complex128)):
+        e = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=device, precision=prec)
+        np_ = e.np
+        opts = dict(m=5, pgtol=PGTOL, ftol_abs=-1.0, itermax=3000, precision=prec, guni_tol=GUNI_TOL)
+        e.solve(sol, sv, rvdw=rvdw, **opts)
+        e.set_timing(True)
+        e.solve(sol, sv, rvdw=rvdw, **opts)
+        st, cnt = e.stage_times()
+        e.set_timing(False)
+        e.close()
+        x = torch.randn(np_, n, n, n, dtype=dt, device=device)
+        for _ in range(5):  # plans and warm-up
+            torch.fft.fftn(x, dim=(1, 2, 3))
+            torch.fft.ifftn(x, dim=(1, 2, 3), norm="forward")
+        t = {}
+        for key, fn in (("forward", lambda: torch.fft.fftn(x, dim=(1, 2, 3))),
+                        ("inverse", lambda: torch.fft.ifftn(x, dim=(1, 2, 3), norm="forward"))):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            for _ in range(20):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            t[key] = a.elapsed_time(b) / 20
+        res["metric"] = "3-D FFT stage time, %d planes of %d^3" % (np_, n)
+        res[name] = {"engine_forward_ms": st["fft_forward"] / cnt, "engine_inverse_ms": st["fft_inverse"] / cnt,
+                     "cufft_forward_ms": t["forward"], "cufft_inverse_ms": t["inverse"], "engine_evaluations": cnt}
+    print(json.dumps(res))
+
+
 def median(xs):
     return float(np.median(np.asarray(xs, dtype=np.float64)))
 
@@ -372,6 +413,10 @@ def main():
     sols = [solute(sd, box) for sd in replica_seeds(rank, args.warmup + args.steps)]
     warm_idx = list(range(args.warmup))
     steps_idx = list(range(args.warmup, args.warmup + args.steps))
+
+    if args.fft_compare:
+        fft_compare(n, box, ck, sv, sols[0], rvdw, local)
+        return
 
     if args.evals or args.solves:
         # profiling modes: N evaluations at the first solute's guess density, or N solves
