@@ -106,6 +106,18 @@ struct mdft_handle {
     double stage_ms[ST_COUNT] = {0};
     int stage_count = 0;
     long long launches = 0;  // kernels launched by this handle
+    // the evaluation pipeline as CUDA graphs, one per set of buffers and flags (MDFT_GRAPHS=0:
+    // direct launches); never used while stage timing is on
+    struct PipeGraph {
+        const void *x, *dvec, *vext, *vext32;
+        double *g;
+        int do_ideal, df_mode, prec;
+        bool v32, x32;
+        cudaGraphExec_t exec;
+        long long nlaunch;
+    };
+    std::vector<PipeGraph> pipe_graphs;
+    bool graphs_on = true;
     // vector reductions
     DevBuf<double> vpart, vsc;
     double *h_vsc = nullptr;
@@ -560,10 +572,58 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
 // dvec (df_mode 1 only): h_sums[3] = df.dvec, h_sums[4] = max|df| after finish_sums.
 // vec32 (bulk-copy gather only): df and dvec are FP32 vectors (the minimiser's mixed solves);
 // x32 (FP32 evaluations, with vec32): the point is FP32 too and vext is read from h->vext32.
+// The pipeline is a fixed sequence of launches for given buffers and flags: it runs as a CUDA
+// graph captured on first use (one graph launch instead of about a dozen kernel launches per
+// evaluation), falling back to direct launches when capture is not possible.
+constexpr size_t kMaxPipeGraphs = 8;
+void drop_pipe_graphs(mdft_handle *h) {
+    for (auto &pg : h->pipe_graphs) cudaGraphExecDestroy(pg.exec);
+    h->pipe_graphs.clear();
+}
 int run_pipeline(mdft_handle *h, const void *d_xi, double *d_df, int do_ideal, int df_mode, const void *dvec = nullptr,
                  bool vec32 = false, bool x32 = false) {
-    if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32, x32);
-    return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32, x32);
+    auto direct = [&]() {
+        if (h->eval_prec == MDFT_PREC_MIXED) return run_pipeline_t<float>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32, x32);
+        return run_pipeline_t<double>(h, d_xi, d_df, do_ideal, df_mode, dvec, vec32, x32);
+    };
+    if (!h->graphs_on || h->timing) return direct();
+    for (auto &pg : h->pipe_graphs)
+        if (pg.x == d_xi && pg.g == d_df && pg.dvec == dvec && pg.do_ideal == do_ideal && pg.df_mode == df_mode &&
+            pg.prec == h->eval_prec && pg.v32 == vec32 && pg.x32 == x32 && pg.vext == h->vext.p && pg.vext32 == h->vext32.p) {
+            h->launches += pg.nlaunch;
+            return check_cuda(cudaGraphLaunch(pg.exec, h->stream), "pipeline graph launch");
+        }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return direct();  // inside a caller's capture: launch into it
+    }
+    const long long l0 = h->launches;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return direct();
+    }
+    const int rc = direct();
+    const long long nl = h->launches - l0;  // counted during capture; nothing has run yet
+    h->launches = l0;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = rc == 0 && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (rc) return rc;  // a launch was refused (nothing ran)
+    if (!ok) {
+        h->graphs_on = false;  // this handle's pipeline does not capture: launch directly from now on
+        return direct();
+    }
+    if (h->pipe_graphs.size() >= kMaxPipeGraphs) {
+        cudaGraphExecDestroy(h->pipe_graphs.front().exec);
+        h->pipe_graphs.erase(h->pipe_graphs.begin());
+    }
+    h->pipe_graphs.push_back(mdft_handle::PipeGraph{d_xi, dvec, h->vext.p, h->vext32.p, d_df, do_ideal, df_mode, h->eval_prec, vec32, x32, exec, nl});
+    h->launches += nl;
+    return check_cuda(cudaGraphLaunch(exec, h->stream), "pipeline graph launch");
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
@@ -627,6 +687,8 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     {
         const char *tr = std::getenv("MDFT_TRACE");
         h->trace = tr && tr[0] && tr[0] != '0';
+        const char *gr = std::getenv("MDFT_GRAPHS");
+        h->graphs_on = !(gr && std::strcmp(gr, "0") == 0);
     }
     h->precision = d->precision;
     h->device = d->device;
@@ -864,6 +926,7 @@ int mdft_destroy(mdft_handle *h) {
     // an attached warm-start network goes back to its own stream before this one is destroyed
     if (h->warm) mdft_warm_net_set_stream(h->warm, nullptr);
     h->warm = nullptr;
+    drop_pipe_graphs(h);
     h->ozp_cq.free();
     h->um_pimg.free();
     h->um_gimg.free();

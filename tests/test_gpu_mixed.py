@@ -142,3 +142,24 @@ def test_oz_factored_rotations(tmp_path, name, monkeypatch):
     assert np.abs(df1 - dfo).max() <= 1e-4 * np.abs(dfo).max()
     e0.close()
     e1.close()
+
+
+@pytest.mark.parametrize("precision", [0, PREC_MIXED])
+def test_pipeline_graphs_match_direct_launches(tmp_path, precision, monkeypatch):
+    # The evaluation pipeline replayed as CUDA graphs (the default) against direct launches
+    # (MDFT_GRAPHS=0): the same solve, bit for bit (dG, iteration and evaluation counts), and
+    # the same number of kernels counted.
+    c = cases.ALL_CASES["mol24_m3"]
+    ck = cases.case_ck(tmp_path, c)
+    sol = cases.solute_of(c)
+    opts = dict(m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=3000, precision=precision, guni_tol=0.1)
+    res = []
+    for graphs in ("0", "1"):
+        monkeypatch.setenv("MDFT_GRAPHS", graphs)
+        e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=precision)
+        l0 = e.launch_count
+        r = e.solve(sol, SV, rvdw=c["rvdw"], **opts)
+        res.append((r["dG"], r["iterations"], r["evaluations"], r["evaluations_mixed"], e.launch_count - l0))
+        e.close()
+    monkeypatch.delenv("MDFT_GRAPHS")
+    assert res[0] == res[1], res
