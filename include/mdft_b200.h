@@ -234,6 +234,15 @@ int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const 
 /* Number of kernels this handle has launched since creation. */
 int mdft_get_launch_count(const mdft_handle *h, long long *count);
 
+/* The kernel forms of this handle's FP32 evaluations (no counterpart in the reference):
+ * forms[4] = {projection: 0 register / 1 bulk-copy ring, gather: 0 register / 1 ring, OZ:
+ * 0 complex rotations / 1 factored rotations, 1 when the autotuner chose them}.  The
+ * autotuner times two configurations on the handle's first FP32 phase (the default forms,
+ * and the alternatives) stage by stage and keeps the faster form of each stage; ms (may be
+ * NULL) receives 6 doubles {project, oz, gather} x {configuration 0, 1} in ms, -1 when not
+ * measured.  MDFT_AUTOTUNE=0, MDFT_ANGULAR or MDFT_OZ in the environment at create skip it. */
+int mdft_get_kernel_forms(const mdft_handle *h, int *forms, double *ms);
+
 /* ---- The reference's density file (output/density.bin, input/density.bin) ----
  *
  * Write (src/module_postprocessing.f90:45-95): Fortran unformatted sequential records with

@@ -7,7 +7,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <thread>
 
@@ -94,6 +97,12 @@ struct mdft_handle {
     DevBuf<uint16_t> um_pimg, um_gimg;
     int um_grid_p = 0, um_grid_g = 0;
     bool ring_p = false, ring_g = false;  // FP32 phase: the bulk-copy ring forms (one CTA per SM)
+    bool ring_p_ok = false, ring_g_ok = false;  // ... where they fit
+    // autotuning of the FP32 forms (project: register/ring, OZ: factored/unfactored, gather:
+    // ring/register), once per handle on its first FP32 phase; tune_ms[stage][config] are the
+    // measured stage times of the two configurations timed (-1: not measured)
+    bool tune_on = false, tuned = false;
+    double tune_ms[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
     bool ozp_ok = false;  // FP32 evaluations use the thread-per-pair k_ozp
     bool ozd = false;     // ... in its factored-rotation form k_ozd (MDFT_OZ=ozp: the unfactored one)
     OzpParams ozp{};
@@ -664,6 +673,9 @@ double combine(const mdft_handle *h, double fid, double fext, double fexc) {
     return f;
 }
 
+// create-time tuning of the FP32 kernel forms (defined with the solver, solve.cuh)
+int autotune_at_create(mdft_handle *h);
+
 }  // namespace
 
 // -------------------------------------------------------------------------
@@ -840,13 +852,18 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
             h->um_grid_p = h->nsm * std::max(1, bp);
             h->um_grid_g = h->nsm * std::max(1, bg);
             h->um_ok = true;
-            h->ring_p = want_ring_p && project_ring_smem_bytes(h->um_ps, g.no) <= dyn_max;
-            h->ring_g = want_ring && g.no == 84 && gather_ring_smem_bytes(h->um_gs, 84) <= dyn_max;
-            if (h->ring_p) {
+            h->ring_p_ok = project_ring_smem_bytes(h->um_ps, g.no) <= dyn_max;
+            h->ring_g_ok = g.no == 84 && gather_ring_smem_bytes(h->um_gs, 84) <= dyn_max;
+            h->ring_p = want_ring_p && h->ring_p_ok;
+            h->ring_g = want_ring && h->ring_g_ok;
+            if (h->ring_p_ok) {
                 if ((rc = allow_smem((const void *)k_project_ring<4>, maxsmem))) return rc;
                 if ((rc = allow_smem((const void *)k_project_ring<1>, maxsmem))) return rc;
             }
-            if (h->ring_g && (rc = allow_smem((const void *)k_gather_ring<84>, maxsmem))) return rc;
+            if (h->ring_g_ok && (rc = allow_smem((const void *)k_gather_ring<84>, maxsmem))) return rc;
+            // the FP32 forms are measured on the first FP32 phase unless chosen in the environment
+            const char *at = std::getenv("MDFT_AUTOTUNE");
+            h->tune_on = !(at && std::strcmp(at, "0") == 0) && !ang && !std::getenv("MDFT_OZ");
         }
     }
     {
@@ -915,6 +932,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
         }
     }
     h->eval_prec = h->precision;
+    if ((rc = autotune_at_create(h.get()))) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "create"))) return rc;
     *out = h.release();
     return MDFT_OK;
@@ -1046,6 +1064,18 @@ int mdft_set_timing(mdft_handle *h, int on) {
     h->timing = on != 0;
     for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = 0;
     h->stage_count = 0;
+    return MDFT_OK;
+}
+
+int mdft_get_kernel_forms(const mdft_handle *h, int *forms, double *ms) {
+    if (!h || !forms) { set_error("null argument"); return MDFT_E_ARG; }
+    forms[0] = h->ring_p ? 1 : 0;
+    forms[1] = h->ring_g ? 1 : 0;
+    forms[2] = h->ozd;
+    forms[3] = h->tuned && h->tune_ms[0][0] >= 0 ? 1 : 0;
+    if (ms)
+        for (int i = 0; i < 3; ++i)
+            for (int c = 0; c < 2; ++c) ms[2 * i + c] = h->tune_ms[i][c];
     return MDFT_OK;
 }
 

@@ -43,6 +43,118 @@ int eval_fg(mdft_handle *h, const void *x, double *g, const void *dvec, double *
     return eval_finish(h, f, gd, gmax, guni, fscale);
 }
 
+// Autotuner of the FP32 forms: the pipeline at the FP32 point x (gradient into the scratch
+// vector g) under two configurations -- the defaults (register projection, ring gather,
+// factored OZ) and the alternatives (ring projection, register gather, complex-rotation
+// OZ) -- one untimed and three timed evaluations each, stage times by CUDA events; each stage
+// keeps its faster form.
+int autotune_fp32(mdft_handle *h, const void *x, double *g) {
+    if (h->tuned) return 0;
+    h->tuned = true;
+    if (!h->tune_on || !h->um_ok) return 0;
+    const bool timing0 = h->timing;
+    double ms0[ST_COUNT];
+    for (int i = 0; i < ST_COUNT; ++i) ms0[i] = h->stage_ms[i];
+    const int cnt0 = h->stage_count;
+    struct Cfg {
+        bool rp, rg, oz;
+    };
+    const Cfg cfg[2] = {{false, h->ring_g_ok, h->ozp_ok ? true : h->ozd}, {h->ring_p_ok, false, false}};
+    double ms[2][ST_COUNT] = {};
+    int rc = 0;
+    for (int c = 0; c < 2 && !rc; ++c) {
+        h->ring_p = cfg[c].rp;
+        h->ring_g = cfg[c].rg;
+        h->ozd = cfg[c].oz;
+        double fid, fext, fexc;
+        h->timing = false;
+        if ((rc = run_pipeline(h, x, g, 1, 1, nullptr, true, true)) || (rc = finish_sums(h, &fid, &fext, &fexc))) break;
+        h->timing = true;
+        for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = 0;
+        h->stage_count = 0;
+        for (int r = 0; r < 3 && !rc; ++r)
+            if (!(rc = run_pipeline(h, x, g, 1, 1, nullptr, true, true))) rc = finish_sums(h, &fid, &fext, &fexc);
+        for (int i = 0; i < ST_COUNT; ++i) ms[c][i] = h->stage_count ? h->stage_ms[i] / h->stage_count : -1.0;
+    }
+    h->timing = timing0;
+    for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = ms0[i];
+    h->stage_count = cnt0;
+    drop_pipe_graphs(h);  // graphs captured under either configuration are stale
+    if (rc) {  // keep the defaults
+        h->ring_p = cfg[0].rp;
+        h->ring_g = cfg[0].rg;
+        h->ozd = cfg[0].oz;
+        return rc;
+    }
+    const int stage[3] = {ST_PROJECT, ST_OZ, ST_GATHER};
+    for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 2; ++c) h->tune_ms[i][c] = ms[c][stage[i]];
+    const bool diff_p = cfg[0].rp != cfg[1].rp, diff_g = cfg[0].rg != cfg[1].rg, diff_o = cfg[0].oz != cfg[1].oz;
+    h->ring_p = diff_p && ms[1][ST_PROJECT] < ms[0][ST_PROJECT] ? cfg[1].rp : cfg[0].rp;
+    h->ring_g = diff_g && ms[1][ST_GATHER] < ms[0][ST_GATHER] ? cfg[1].rg : cfg[0].rg;
+    h->ozd = diff_o && ms[1][ST_OZ] < ms[0][ST_OZ] ? cfg[1].oz : cfg[0].oz;
+    if (h->trace)
+        std::fprintf(stderr, "mdft-trace autotune: project %s (%.4f / %.4f ms), oz %s (%.4f / %.4f), gather %s (%.4f / %.4f)\n",
+                     h->ring_p ? "ring" : "register", ms[0][ST_PROJECT], ms[1][ST_PROJECT], h->ozd ? "factored" : "complex",
+                     ms[0][ST_OZ], ms[1][ST_OZ], h->ring_g ? "ring" : "register", ms[0][ST_GATHER], ms[1][ST_GATHER]);
+    return 0;
+}
+
+__global__ void k_fill_f32(float *__restrict__ p, float v, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+// Create-time tuning of a mixed handle, shared by every handle of the same shape on the same
+// device in this process (the first one measures, under a lock, at the bulk density with no
+// external potential -- the kernels' times do not depend on the values).
+struct TuneKey {
+    int dev, nx, ny, nz, mmax, mrso, no;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(dev, nx, ny, nz, mmax, mrso, no) < std::tie(o.dev, o.nx, o.ny, o.nz, o.mmax, o.mrso, o.no);
+    }
+};
+struct TuneResult {
+    bool rp, rg, oz;
+    double ms[3][2];
+};
+int autotune_at_create(mdft_handle *h) {
+    if (!h->tune_on || !h->um_ok || !h->pt_ok32 || h->gt_ncol32 <= 0 || h->precision != MDFT_PREC_MIXED) return 0;
+    static std::mutex mu;
+    static std::map<TuneKey, TuneResult> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const Grid &g = h->g;
+    const TuneKey key{dev, g.nx, g.ny, g.nz, g.mmax, g.mrso, g.no};
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        const long long nf = g.N * g.no;
+        int rc;
+        if (!h->vext32.p && (rc = alloc_check(h->vext32.alloc((size_t)nf), "FP32 vext", (size_t)nf * 4))) return rc;
+        cudaMemsetAsync(h->vext32.p, 0, (size_t)nf * 4, h->stream);
+        float *x = reinterpret_cast<float *>(h->xi.p);  // the FP64 buffer holds the FP32 point
+        k_fill_f32<<<vec_grid(), 256, 0, h->stream>>>(x, 1.0f, nf);
+        h->launches += 1;
+        const int ep = h->eval_prec;
+        h->eval_prec = MDFT_PREC_MIXED;
+        rc = autotune_fp32(h, x, h->df.p);
+        h->eval_prec = ep;
+        if (rc) return rc;
+        TuneResult r{h->ring_p, h->ring_g, h->ozd, {}};
+        for (int i = 0; i < 3; ++i)
+            for (int c = 0; c < 2; ++c) r.ms[i][c] = h->tune_ms[i][c];
+        cache[key] = r;
+    } else {
+        h->ring_p = it->second.rp;
+        h->ring_g = it->second.rg;
+        h->ozd = it->second.oz;
+        for (int i = 0; i < 3; ++i)
+            for (int c = 0; c < 2; ++c) h->tune_ms[i][c] = it->second.ms[i][c];
+        h->tuned = true;
+    }
+    return 0;
+}
+
 int lbfgs_alloc(mdft_handle *h, int m) {
     LbfgsState &L = h->lb;
     const long long n = h->g.N * h->g.no;

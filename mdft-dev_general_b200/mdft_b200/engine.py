@@ -87,6 +87,7 @@ SIGNATURES = {
     "mdft_guess_density_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mdft_minimize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_MinOpts), C.POINTER(_MinRes)]),
     "mdft_get_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "mdft_get_kernel_forms": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _DP]),
     "mdft_ideal_external_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double,
                                               C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mdft_pressure_correction": (C.c_int, [C.c_void_p, _DP, C.c_double, C.c_double, _DP]),
@@ -299,6 +300,14 @@ class Engine:
         _check(lib().mdft_minimize_device(self.h, C.c_void_p(d_xi), C.byref(o), C.byref(r)))
         return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
                     evaluations_mixed=r.evaluations_mixed, guni=r.guni)
+
+    def kernel_forms(self) -> dict:
+        """The FP32 kernel forms in use and the autotuner's stage times (ms, -1: not measured)."""
+        f = (C.c_int * 4)()
+        ms = np.zeros(6)
+        _check(lib().mdft_get_kernel_forms(self.h, f, _p(ms)))
+        return dict(project_ring=bool(f[0]), gather_ring=bool(f[1]), oz_factored=bool(f[2]), tuned=bool(f[3]),
+                    stage_ms={"project": ms[0:2].tolist(), "oz": ms[2:4].tolist(), "gather": ms[4:6].tolist()})
 
     @property
     def launch_count(self) -> int:

@@ -163,3 +163,39 @@ def test_pipeline_graphs_match_direct_launches(tmp_path, precision, monkeypatch)
         e.close()
     monkeypatch.delenv("MDFT_GRAPHS")
     assert res[0] == res[1], res
+
+
+@pytest.mark.parametrize("tune", ["1", "0"])
+def test_autotuner_picks_measured_forms(tmp_path, tune, monkeypatch):
+    # The autotuner times the default and the alternative FP32 forms when a mixed handle is
+    # created (once per shape and device in a process) and keeps the faster form of each stage;
+    # with MDFT_AUTOTUNE=0 the defaults stay and nothing is measured.  Either way the solve
+    # lands within 0.1 kJ/mol of the FP64 solve.
+    c = cases.ALL_CASES["mol24_m3"]
+    ck = cases.case_ck(tmp_path, c)
+    sol = cases.solute_of(c)
+    e64 = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0)
+    r64 = e64.solve(sol, SV, rvdw=c["rvdw"], m=5, pgtol=1e-6, ftol_abs=-1.0, itermax=3000, guni_tol=0.01)
+    e64.close()
+    monkeypatch.delenv("MDFT_ANGULAR", raising=False)
+    monkeypatch.delenv("MDFT_OZ", raising=False)
+    monkeypatch.setenv("MDFT_AUTOTUNE", tune)
+    e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=PREC_MIXED)
+    monkeypatch.delenv("MDFT_AUTOTUNE")
+    kf = e.kernel_forms()
+    r = e.solve(sol, SV, rvdw=c["rvdw"], m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=3000, precision=PREC_MIXED, guni_tol=0.1)
+    assert e.kernel_forms() == kf  # chosen at create, kept by the solve
+    print("\nautotune %s: %s" % (tune, kf))
+    if tune == "1":
+        assert kf["tuned"]
+        for stage, (m0, m1) in kf["stage_ms"].items():
+            assert m0 > 0 and m1 > 0, (stage, m0, m1)
+        ms = kf["stage_ms"]
+        assert kf["project_ring"] == (ms["project"][1] < ms["project"][0])
+        assert kf["gather_ring"] == (ms["gather"][0] <= ms["gather"][1])
+        assert kf["oz_factored"] == (ms["oz"][0] <= ms["oz"][1])
+    else:
+        assert not kf["tuned"] and kf["gather_ring"] and not kf["project_ring"] and kf["oz_factored"]
+        assert kf["stage_ms"] == {"project": [-1.0, -1.0], "oz": [-1.0, -1.0], "gather": [-1.0, -1.0]}
+    assert abs(r["dG"] - r64["dG"]) <= 0.1, (r["dG"], r64["dG"])
+    e.close()
