@@ -77,7 +77,7 @@ def parse():
     ap.add_argument("--polish", type=int, default=1, help="mixed: 1 = FP64 iterations until pgtol, 0 = one FP64 evaluation")
     ap.add_argument("--guni-tol", type=float, default=GUNI_TOL,
                     help="also stop only when |sum w df dv| <= this (kJ/mol); <= 0: off")
-    ap.add_argument("--regions", type=int, default=3, help="timed regions per form (the median is reported)")
+    ap.add_argument("--regions", type=int, default=5, help="timed regions per form (the median is reported)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 form's timing")
     ap.add_argument("--solves", type=int, default=0,
                     help="profiling mode: only N solves of the workload (no timing, no reference solves)")

@@ -234,6 +234,13 @@ int mdft_ideal_external_noalloc(const double *d_xi, const double *d_vext, const 
 /* Number of kernels this handle has launched since creation. */
 int mdft_get_launch_count(const mdft_handle *h, long long *count);
 
+/* Error-path test switch (no counterpart in the reference): with on != 0, this handle's
+ * bulk-copy and tensor-core gather kernels behave as if their first mbarrier wait had run
+ * out -- they set the device error flag and return before issuing any copy or allocating
+ * tensor memory -- so every evaluation fails with MDFT_E_CUDA and the bounded-wait message.
+ * Off again, the handle evaluates as before. */
+int mdft_set_wait_failure(mdft_handle *h, int on);
+
 /* The kernel forms of this handle's FP32 evaluations (no counterpart in the reference):
  * forms[4] = {projection: 0 register / 1 bulk-copy ring, gather: 0 register / 1 ring, OZ:
  * 0 complex rotations / 1 factored rotations, 1 when the autotuner chose them}.  The

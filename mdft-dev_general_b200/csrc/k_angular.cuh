@@ -41,6 +41,8 @@ struct GatherArgs {
     int df_mode;                          // 0 none, 1 store (id + exc), 2 accumulate exc
     const void *dvec;                     // df_mode 1: also df.dvec (null: df.df is not wanted -> 0);
                                           // FP64, or the type of df in k_gather_tma
+    int fail_wait;                        // the bulk-copy gathers report a timed-out wait at once,
+                                          // before any copy or tensor-memory allocation (tests)
 };
 
 template <typename T> struct Vec4;

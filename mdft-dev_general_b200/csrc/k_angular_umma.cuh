@@ -342,6 +342,10 @@ __global__ void __launch_bounds__(kUmThreads, 2) k_gather_umma(const float2 *__r
                                                                const double *__restrict__ w, TD *__restrict__ df,
                                                                double *__restrict__ partial, int *__restrict__ err,
                                                                GatherArgs a, UmmaShape s, int ntiles) {
+    if (a.fail_wait) {  // the error path of a timed-out wait, with nothing issued yet
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
     extern __shared__ __align__(128) unsigned char um_smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_slot;
@@ -733,6 +737,10 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
                                                                double *__restrict__ partial, int *__restrict__ err,
                                                                GatherArgs a, UmmaShape s, int ntiles) {
     static_assert(NO % 4 == 0, "vector epilogue needs no % 4 == 0");
+    if (a.fail_wait) {  // the error path of a timed-out wait, with nothing issued yet
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
     constexpr int NT = gather_ring_threads<NO>();  // epilogue threads
     static_assert(NT % 32 == 0, "whole warps");
     static_assert(NT + 32 <= 1024, "one CTA of at most 1024 threads");

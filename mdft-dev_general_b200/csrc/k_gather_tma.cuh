@@ -68,6 +68,10 @@ __global__ void __launch_bounds__(kGtThreads, sizeof(T) == 8 ? 1 : 2) k_gather_t
                                                               TD *__restrict__ df, double *__restrict__ partial,
                                                               int *__restrict__ err, GatherArgs a, int ntiles) {
     using C = typename Cplx<T>::t;
+    if (a.fail_wait) {  // the error path of a timed-out wait, with nothing issued yet
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
     constexpr int NC = 32 * NCOL;
     constexpr int BM = gt_bm<T>();   // points per tile
     constexpr int PW = BM / 8;       // points per warp

@@ -127,6 +127,7 @@ struct mdft_handle {
     };
     std::vector<PipeGraph> pipe_graphs;
     bool graphs_on = true;
+    bool wait_fail = false;  // mdft_set_wait_failure: gathers report a timed-out wait (tests)
     // vector reductions
     DevBuf<double> vpart, vsc;
     double *h_vsc = nullptr;
@@ -482,6 +483,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     if ((rc = launch_fft_t<T>(h, planes, tw, -1))) return rc;
     stage_mark(h, 4);
     GatherArgs ga;
+    ga.fail_wait = h->wait_fail ? 1 : 0;
     ga.N = g.N;
     ga.no = g.no;
     ga.np = g.np;
@@ -1064,6 +1066,13 @@ int mdft_set_timing(mdft_handle *h, int on) {
     h->timing = on != 0;
     for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = 0;
     h->stage_count = 0;
+    return MDFT_OK;
+}
+
+int mdft_set_wait_failure(mdft_handle *h, int on) {
+    if (!h) { set_error("null argument"); return MDFT_E_ARG; }
+    h->wait_fail = on != 0;
+    drop_pipe_graphs(h);  // the captured launches carry the flag
     return MDFT_OK;
 }
 

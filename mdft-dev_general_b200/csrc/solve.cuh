@@ -46,8 +46,10 @@ int eval_fg(mdft_handle *h, const void *x, double *g, const void *dvec, double *
 // Autotuner of the FP32 forms: the pipeline at the FP32 point x (gradient into the scratch
 // vector g) under two configurations -- the defaults (register projection, ring gather,
 // factored OZ) and the alternatives (ring projection, register gather, complex-rotation
-// OZ) -- one untimed and three timed evaluations each, stage times by CUDA events; each stage
-// keeps its faster form.
+// OZ) -- one untimed and three timed evaluations each, stage times by CUDA events (the
+// fastest of the three); each stage keeps its default form unless the alternative is more
+// than 5 % faster.
+constexpr double kTuneMargin = 0.05;
 int autotune_fp32(mdft_handle *h, const void *x, double *g) {
     if (h->tuned) return 0;
     h->tuned = true;
@@ -70,11 +72,14 @@ int autotune_fp32(mdft_handle *h, const void *x, double *g) {
         h->timing = false;
         if ((rc = run_pipeline(h, x, g, 1, 1, nullptr, true, true)) || (rc = finish_sums(h, &fid, &fext, &fexc))) break;
         h->timing = true;
-        for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = 0;
-        h->stage_count = 0;
-        for (int r = 0; r < 3 && !rc; ++r)
+        for (int i = 0; i < ST_COUNT; ++i) ms[c][i] = -1.0;
+        for (int r = 0; r < 3 && !rc; ++r) {  // the fastest of three evaluations, stage by stage
+            for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = 0;
+            h->stage_count = 0;
             if (!(rc = run_pipeline(h, x, g, 1, 1, nullptr, true, true))) rc = finish_sums(h, &fid, &fext, &fexc);
-        for (int i = 0; i < ST_COUNT; ++i) ms[c][i] = h->stage_count ? h->stage_ms[i] / h->stage_count : -1.0;
+            for (int i = 0; i < ST_COUNT && !rc; ++i)
+                if (ms[c][i] < 0.0 || h->stage_ms[i] < ms[c][i]) ms[c][i] = h->stage_ms[i];
+        }
     }
     h->timing = timing0;
     for (int i = 0; i < ST_COUNT; ++i) h->stage_ms[i] = ms0[i];
@@ -90,9 +95,12 @@ int autotune_fp32(mdft_handle *h, const void *x, double *g) {
     for (int i = 0; i < 3; ++i)
         for (int c = 0; c < 2; ++c) h->tune_ms[i][c] = ms[c][stage[i]];
     const bool diff_p = cfg[0].rp != cfg[1].rp, diff_g = cfg[0].rg != cfg[1].rg, diff_o = cfg[0].oz != cfg[1].oz;
-    h->ring_p = diff_p && ms[1][ST_PROJECT] < ms[0][ST_PROJECT] ? cfg[1].rp : cfg[0].rp;
-    h->ring_g = diff_g && ms[1][ST_GATHER] < ms[0][ST_GATHER] ? cfg[1].rg : cfg[0].rg;
-    h->ozd = diff_o && ms[1][ST_OZ] < ms[0][ST_OZ] ? cfg[1].oz : cfg[0].oz;
+    // an alternative replaces a default only when it is faster by more than kTuneMargin, so
+    // that timing noise does not flip a choice
+    auto better = [](double alt, double def) { return alt < (1.0 - kTuneMargin) * def; };
+    h->ring_p = diff_p && better(ms[1][ST_PROJECT], ms[0][ST_PROJECT]) ? cfg[1].rp : cfg[0].rp;
+    h->ring_g = diff_g && better(ms[1][ST_GATHER], ms[0][ST_GATHER]) ? cfg[1].rg : cfg[0].rg;
+    h->ozd = diff_o && better(ms[1][ST_OZ], ms[0][ST_OZ]) ? cfg[1].oz : cfg[0].oz;
     if (h->trace)
         std::fprintf(stderr, "mdft-trace autotune: project %s (%.4f / %.4f ms), oz %s (%.4f / %.4f), gather %s (%.4f / %.4f)\n",
                      h->ring_p ? "ring" : "register", ms[0][ST_PROJECT], ms[1][ST_PROJECT], h->ozd ? "factored" : "complex",

@@ -88,6 +88,7 @@ SIGNATURES = {
     "mdft_minimize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_MinOpts), C.POINTER(_MinRes)]),
     "mdft_get_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "mdft_get_kernel_forms": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _DP]),
+    "mdft_set_wait_failure": (C.c_int, [C.c_void_p, C.c_int]),
     "mdft_ideal_external_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_double,
                                               C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mdft_pressure_correction": (C.c_int, [C.c_void_p, _DP, C.c_double, C.c_double, _DP]),
@@ -300,6 +301,10 @@ class Engine:
         _check(lib().mdft_minimize_device(self.h, C.c_void_p(d_xi), C.byref(o), C.byref(r)))
         return dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
                     evaluations_mixed=r.evaluations_mixed, guni=r.guni)
+
+    def set_wait_failure(self, on: bool):
+        """Make the gathers report a timed-out wait before issuing any copy (error-path tests)."""
+        _check(lib().mdft_set_wait_failure(self.h, 1 if on else 0))
 
     def kernel_forms(self) -> dict:
         """The FP32 kernel forms in use and the autotuner's stage times (ms, -1: not measured)."""

@@ -168,7 +168,8 @@ def test_pipeline_graphs_match_direct_launches(tmp_path, precision, monkeypatch)
 @pytest.mark.parametrize("tune", ["1", "0"])
 def test_autotuner_picks_measured_forms(tmp_path, tune, monkeypatch):
     # The autotuner times the default and the alternative FP32 forms when a mixed handle is
-    # created (once per shape and device in a process) and keeps the faster form of each stage;
+    # created (once per shape and device in a process) and keeps, stage by stage, the default
+    # unless the alternative is more than 5 % faster;
     # with MDFT_AUTOTUNE=0 the defaults stay and nothing is measured.  Either way the solve
     # lands within 0.1 kJ/mol of the FP64 solve.
     c = cases.ALL_CASES["mol24_m3"]
@@ -191,9 +192,10 @@ def test_autotuner_picks_measured_forms(tmp_path, tune, monkeypatch):
         for stage, (m0, m1) in kf["stage_ms"].items():
             assert m0 > 0 and m1 > 0, (stage, m0, m1)
         ms = kf["stage_ms"]
-        assert kf["project_ring"] == (ms["project"][1] < ms["project"][0])
-        assert kf["gather_ring"] == (ms["gather"][0] <= ms["gather"][1])
-        assert kf["oz_factored"] == (ms["oz"][0] <= ms["oz"][1])
+        # the alternative (configuration 1) wins only when more than 5 % faster
+        assert kf["project_ring"] == (ms["project"][1] < 0.95 * ms["project"][0])
+        assert kf["gather_ring"] == (not ms["gather"][1] < 0.95 * ms["gather"][0])
+        assert kf["oz_factored"] == (not ms["oz"][1] < 0.95 * ms["oz"][0])
     else:
         assert not kf["tuned"] and kf["gather_ring"] and not kf["project_ring"] and kf["oz_factored"]
         assert kf["stage_ms"] == {"project": [-1.0, -1.0], "oz": [-1.0, -1.0], "gather": [-1.0, -1.0]}

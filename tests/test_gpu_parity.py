@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from mdft_b200 import Engine
+from mdft_b200 import Engine, MdftError, PREC_MIXED
 import cases
 
 pytestmark = pytest.mark.gpu
@@ -179,3 +179,31 @@ def test_solve_entry_point(tmp_path):
     np.testing.assert_array_equal(xi, x2)
     e.close()
     e2.close()
+
+
+@pytest.mark.parametrize("precision", [0, PREC_MIXED])
+def test_timed_out_wait_is_reported(tmp_path, precision):
+    # The bounded-wait error path of the bulk-copy and tensor-core gathers, provoked with nothing
+    # in flight: the kernels report a timed-out wait before issuing any copy, the evaluation
+    # fails with the bounded-wait message, and the handle evaluates as before once the switch is
+    # off (the same F and gradient, bit for bit); a mixed solve (the ring gather) fails the same way.
+    c = cases.ALL_CASES["mol24_m3"]
+    ck = cases.case_ck(tmp_path, c)
+    o = O.Oracle(c["n"], c["L"], c["mmax"], ck, SV.kT, SV.n0)
+    o.compute_vext(cases.solute_of(c), SV, rvdw=c["rvdw"])
+    xi = o.guess_density()
+    e = Engine(c["n"], c["L"], c["mmax"], ck, temperature=SV.temperature, n0=SV.n0, precision=precision)
+    e.set_vext(o.get_vext())
+    f0, g0, _ = e.energy_and_gradient(xi)
+    e.set_wait_failure(True)
+    with pytest.raises(MdftError, match="timed out"):
+        e.energy_and_gradient(xi)
+    if precision == PREC_MIXED:
+        with pytest.raises(MdftError, match="timed out"):
+            e.solve(cases.solute_of(c), SV, rvdw=c["rvdw"], m=5, pgtol=1e-4, ftol_abs=-1.0, itermax=50,
+                    precision=PREC_MIXED, guni_tol=0.1)
+        e.set_vext(o.get_vext())
+    e.set_wait_failure(False)
+    f1, g1, _ = e.energy_and_gradient(xi)
+    assert f1 == f0 and np.array_equal(g1, g0)
+    e.close()
