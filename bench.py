@@ -83,6 +83,9 @@ def parse():
                     help="profiling mode: only N solves of the workload (no timing, no reference solves)")
     ap.add_argument("--evals", type=int, default=0,
                     help="profiling mode: only N energy_and_gradient evaluations of the workload (no solve)")
+    ap.add_argument("--prof-grid", type=int, default=0,
+                    help="with --evals: evaluations of a config-2-style cluster on this grid (0.375 A spacing) instead")
+    ap.add_argument("--prof-mmax", type=int, default=5, help="with --prof-grid: the angular order")
     ap.add_argument("--fft-compare", action="store_true",
                     help="timing comparison: the engine's FFT stages against cuFFT (torch.fft) on the same planes")
     return ap.parse_args()
@@ -416,6 +419,24 @@ def main():
 
     if args.fft_compare:
         fft_compare(n, box, ck, sv, sols[0], rvdw, local)
+        return
+
+    if args.evals and args.prof_grid:
+        # profiling mode: the general kernels (np = 88, no = 330 at mmax 5) on a packed cluster
+        # (600 sites in a 48 A box, proportionally fewer in a smaller one), mixed precision, N
+        # evaluations at its guess density
+        pn, pbox = args.prof_grid, 0.375 * args.prof_grid
+        eng = Engine(pn, pbox, args.prof_mmax, ck_file(args.prof_mmax, kmax=15.0), temperature=sv.temperature, n0=sv.n0,
+                     device=local, precision=PREC_MIXED)
+        rad = min(20.0, 0.4 * pbox)  # 600 sites at >= 3 A fill a 20 A sphere; fewer in a smaller box
+        cl = synth.packed_cluster_solute(max(20, int(540 * (rad / 20.0) ** 3)), seed=2026, radius=rad)
+        cl.xyz = synth.center_solute(cl.xyz, (pbox,) * 3)
+        eng.compute_vext(cl, sv, rvdw=min(RVDW, 0.45 * pbox))
+        xi0 = eng.guess_density()
+        for _ in range(args.evals):
+            f, _, terms = eng.energy_and_gradient(xi0)
+        print(json.dumps({"evals": args.evals, "grid": pn, "mmax": args.prof_mmax, "np": eng.np, "no": eng.no, "f": f}))
+        eng.close()
         return
 
     if args.evals or args.solves:
