@@ -55,8 +55,9 @@ GUNI_TOL = 0.1
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, by (form, stage), from one ncu
 # capture of each FP32-phase kernel in a mixed solve of this workload (k_gather_ring<84>,
-# k_project_umma<float,4>, k_ozp<3,2>); absent: null
-NCU_TRAFFIC_BYTES = {("mixed", "oz"): 65.1e6, ("mixed", "gather"): 393.2e6, ("mixed", "project"): 112.1e6}
+# k_project_umma<float,4>, k_ozd<3,2>), and of the FP64 form's kernels; absent: null
+NCU_TRAFFIC_BYTES = {("mixed", "oz"): 69.2e6, ("mixed", "gather"): 397.8e6, ("mixed", "project"): 113.1e6,
+                     ("fp64", "oz"): 186.6e6, ("fp64", "gather"): 803.4e6, ("fp64", "project"): 256.1e6}
 
 
 def parse():
