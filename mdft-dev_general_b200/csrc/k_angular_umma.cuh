@@ -703,7 +703,8 @@ template <int NO> __host__ __device__ constexpr int gather_ring_threads() { retu
 // the block: those threads plus one copy warp
 template <int NO> __host__ __device__ constexpr int gather_ring_block() { return gather_ring_threads<NO>() + 32; }
 inline size_t gather_ring_smem_bytes(const UmmaShape &s, int no) {
-    return umma_smem_bytes(s) + (size_t)kUmBM * no * 4 + (size_t)kGrStages * 3 * kGrSub * no * 4;
+    // + the projections of one tile, [Kp / 2 complex][128 points]
+    return umma_smem_bytes(s) + (size_t)kUmBM * no * 4 + (size_t)kGrStages * 3 * kGrSub * no * 4 + (size_t)(s.Kp / 2) * kUmBM * 8;
 }
 
 // log(v) for the ring epilogue: the hardware base-2 logarithm (lg2.approx; absolute error
@@ -747,7 +748,7 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
     constexpr int kWarps = NT / 32 + 1, kGroupWarps = (NT / 32) / 4;  // epilogue warps per tensor-memory lane quarter
     constexpr uint32_t kEpiBar = 1;                                   // named barrier of the epilogue threads
     extern __shared__ __align__(128) unsigned char um_smem[];
-    __shared__ uint64_t bar, sfull[kGrStages], sempty[kGrStages];
+    __shared__ uint64_t bar, sfull[kGrStages], sempty[kGrStages], pfull, pempty;
     __shared__ uint32_t tmem_slot;
     __shared__ double red[kGatherSums][kWarps];
     __shared__ double wsum_s;
@@ -761,6 +762,8 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
             mbar_init(&sfull[k], 1);
             mbar_init(&sempty[k], NT / 32);
         }
+        mbar_init(&pfull, 1);
+        mbar_init(&pempty, NT / 32);
         double ws = 0.0;
         for (int io = 0; io < NO; ++io) ws += w[io];
         wsum_s = ws;
@@ -771,6 +774,7 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
     float *vt = reinterpret_cast<float *>(um_smem + umma_smem_bytes(s));  // [128][NO]
     float *ring = vt + (size_t)kUmBM * NO;  // stage k: x, vext, d of kGrSub points each
     constexpr int SUB = kGrSub * NO;        // floats per array per sub-tile
+    float2 *pst = reinterpret_cast<float2 *>(ring + (size_t)kGrStages * 3 * SUB);  // [np][128] of the next tile
     const bool want_v = a.do_ideal != 0, want_d = a.dvec != nullptr, store = a.df_mode == 1;
     const float *dvec = static_cast<const float *>(a.dvec);
     const int nmine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -782,9 +786,23 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
         // ---- the copy warp: sub-tile G into stage G % kGrStages once the stage is empty ----
         const uint32_t sb = (uint32_t)(SUB * 4);
         const uint32_t tx = sb * (1u + (want_v ? 1u : 0u) + (want_d ? 1u : 0u));
-        int issued[kGrStages] = {};
+        const uint32_t pb = (uint32_t)(kUmBM * sizeof(float2));  // one projection of a tile
+        int issued[kGrStages] = {}, pissued = 0;
         for (int G = 0; G < nsub; ++G) {
             const int st = G % kGrStages;
+            if (G % kGrPer == 0) {
+                // tile G / kGrPer's projections, once the previous tile's are in the A tile
+                const int i = G / kGrPer;
+                if (i > 0 && !mbar_wait(&pempty, (uint32_t)((i - 1) & 1))) {
+                    aborted = true;
+                    break;
+                }
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&pfull, pb * (uint32_t)np);
+                    for (int ip = 0; ip < np; ++ip) bulk_load(pst + (size_t)ip * kUmBM, planes + (size_t)ip * a.N + tile0(i), pb, &pfull);
+                }
+                ++pissued;
+            }
             if (G >= kGrStages && !mbar_wait(&sempty[st], (uint32_t)((G / kGrStages - 1) & 1))) {
                 aborted = true;  // the epilogue warps stopped (or stalled): copy nothing more
                 break;
@@ -800,9 +818,11 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
             ++issued[st];
         }
         // every copy issued has landed (or had its bounded wait) before the block ends
-        if (lane == 0)
+        if (lane == 0) {
             for (int st = 0; st < kGrStages; ++st)
                 if (issued[st] > 0) (void)mbar_wait(&sfull[st], (uint32_t)((issued[st] - 1) & 1));
+            if (pissued > 0) (void)mbar_wait(&pfull, (uint32_t)((pissued - 1) & 1));
+        }
         if (aborted && lane == 0) atomicExch(err, 1);
     } else {
         // ---- the epilogue warps ----
@@ -818,16 +838,29 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
         const double cid = a.kT * a.dv * a.rho0, cext = a.dv * a.rho0, cexc = (double)pre * a.rho0;
         const double tile_id = want_v ? cid * (double)kUmBM * wsum_s : 0.0;  // constant part of F_id per tile
         int miss = 0, mdone = 0;  // thread 0's MMA bookkeeping
-        float pv[kTasks][8];
-        if (nmine > 0) gather_load<NT, kTasks>(planes, a.N, tile0(0), np, KC, pv);
         bool lost = false;  // this thread saw a copy that did not land in time
         for (int i = 0; i < nmine; ++i) {
+            // the tile's projections (staged by the copy warp) split into the A tile
+            const bool okp = !lost && umma::wait_phase(&pfull, (uint32_t)(i & 1));
+            if (!okp) lost = true;
 #pragma unroll
             for (int q = 0; q < kTasks; ++q) {
                 const int t = tid + q * NT;
                 const int m = t % kUmBM, kc = t / kUmBM;
-                if (kc < KC) store_split8(c, s.Kp, m, 8 * kc, pv[q]);
+                if (kc < KC) {
+                    float v[8];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int ip = 4 * kc + j;
+                        const float2 p = (okp && ip < np) ? pst[(size_t)ip * kUmBM + m] : make_float2(0.f, 0.f);
+                        v[2 * j] = p.x;
+                        v[2 * j + 1] = p.y;
+                    }
+                    store_split8(c, s.Kp, m, 8 * kc, v);
+                }
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&pempty);  // this warp is done with the staged projections
             fence_proxy_async_smem();
             umma::fence_before_sync();
             named_sync(kEpiBar, NT);
@@ -835,7 +868,6 @@ __global__ void __launch_bounds__(gather_ring_block<NO>(), 1) k_gather_ring(cons
                 umma_issue(c, s, &bar);
                 ++miss;
             }
-            if (i + 1 < nmine) gather_load<NT, kTasks>(planes, a.N, tile0(i + 1), np, KC, pv);
             const bool ok = umma::wait_phase(&bar, (uint32_t)(i & 1));
             if (tid == 0 && ok) ++mdone;
             // one agreement per tile: an MMA or a copy that did not complete stops every epilogue warp
