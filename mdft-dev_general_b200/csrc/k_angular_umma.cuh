@@ -116,7 +116,8 @@ __device__ __forceinline__ void store_split8(const UmmaCta &c, int Kp, int r, in
 // VW: values per vector load of xi (4 when no % 4 == 0 and xi is 16-byte aligned, else 1).
 // bimg: the packed hi and lo images of A^T ([Np][Kp]: row 2ip + {0: re, 1: im}, column io).
 // The next tile's xi is loaded into registers while the current tile's MMAs and stores run.
-constexpr int kPjTasks = 6;  // 128 points x (96 / 8) chunks over 256 threads
+constexpr int kPjThreads = 384;  // 12 warps, three per tensor-memory lane quarter; two CTAs per SM
+constexpr int kPjTasks = (kUmBM * 12 + kPjThreads - 1) / kPjThreads;  // 128 points x (96 / 8) chunks
 
 // v = x (FP32 xi) or x^2 - 1 formed in FP64 (FP64 xi) for the 8 orientations of each chunk
 template <typename TX, int VW>
@@ -124,7 +125,7 @@ __device__ __forceinline__ void project_load(const TX *__restrict__ xi, long lon
     const int tid = threadIdx.x;
 #pragma unroll
     for (int q = 0; q < kPjTasks; ++q) {
-        const int t = tid + q * kUmThreads;
+        const int t = tid + q * kPjThreads;
         const int m = t % kUmBM, kc = t / kUmBM;
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[q][j] = 0.0f;
@@ -161,7 +162,7 @@ __device__ __forceinline__ void project_store(const UmmaCta &c, int Kp, int no, 
     const int tid = threadIdx.x;
 #pragma unroll
     for (int q = 0; q < kPjTasks; ++q) {
-        const int t = tid + q * kUmThreads;
+        const int t = tid + q * kPjThreads;
         const int m = t % kUmBM, kc = t / kUmBM;
         if (kc >= KC) continue;
         float d[8];
@@ -176,7 +177,7 @@ __device__ __forceinline__ void project_store(const UmmaCta &c, int Kp, int no, 
 }
 
 template <typename TX, int VW>
-__global__ void __launch_bounds__(kUmThreads, 2) k_project_umma(const TX *__restrict__ xi, const uint16_t *__restrict__ bimg,
+__global__ void __launch_bounds__(kPjThreads, 2) k_project_umma(const TX *__restrict__ xi, const uint16_t *__restrict__ bimg,
                                                                 float2 *__restrict__ planes, int *__restrict__ err,
                                                                 AngularArgs a, UmmaShape s, int ntiles) {
     extern __shared__ __align__(128) unsigned char um_smem[];
@@ -206,10 +207,10 @@ __global__ void __launch_bounds__(kUmThreads, 2) k_project_umma(const TX *__rest
         __syncthreads();  // every thread's wait result is in abort_flag: the branch below is uniform
         if (abort_flag) break;
         umma::fence_after_sync();
-        // ---- epilogue: warp (quarter q4, half h) stores columns 16 cc .. 16 cc + 15, cc = h, h+2, ... ----
+        // ---- epilogue: warp (quarter q4, third h) stores columns 16 cc .. 16 cc + 15, cc = h, h+3, ... ----
         const int q4 = warp & 3, h = warp >> 2;
         const long long pt = pt0 + 32 * q4 + lane;
-        for (int cc = h; cc < s.Np / 16; cc += 2) {
+        for (int cc = h; cc < s.Np / 16; cc += kPjThreads / 128) {
             float acc[16];
             umma::ld16(c.tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(16 * cc), acc);
             umma::ld_wait();

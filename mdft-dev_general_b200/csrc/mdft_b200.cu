@@ -447,11 +447,11 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
             if (vec) k_project_ring<4><<<rgrid, kRingThreads, rsmem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
             else k_project_ring<1><<<rgrid, kRingThreads, rsmem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
         } else if (x32) {
-            if (vec) k_project_umma<float, 4><<<grid, kUmThreads, smem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
-            else k_project_umma<float, 1><<<grid, kUmThreads, smem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            if (vec) k_project_umma<float, 4><<<grid, kPjThreads, smem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            else k_project_umma<float, 1><<<grid, kPjThreads, smem, h->stream>>>(static_cast<const float *>(xin), h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
         } else {
-            if (vec) k_project_umma<double, 4><<<grid, kUmThreads, smem, h->stream>>>(d_xi, h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
-            else k_project_umma<double, 1><<<grid, kUmThreads, smem, h->stream>>>(d_xi, h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            if (vec) k_project_umma<double, 4><<<grid, kPjThreads, smem, h->stream>>>(d_xi, h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
+            else k_project_umma<double, 1><<<grid, kPjThreads, smem, h->stream>>>(d_xi, h->um_pimg.p, (float2 *)planes, h->kerr.p, aa, h->um_ps, ntiles);
         }
     } else if (x32) {
         const int ntiles = (int)(g.N / kPtBM);
@@ -848,7 +848,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
             for (const void *fn : gf)
                 if ((rc = allow_smem(fn, maxsmem))) return rc;
             int bp = 0, bg = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_project_umma<float, 4>, kUmThreads, umma_smem_bytes(h->um_ps));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_project_umma<float, 4>, kPjThreads, umma_smem_bytes(h->um_ps));
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bg, k_gather_umma<float, float, 84>, kUmThreads,
                                                           gather_umma_smem_bytes(h->um_gs, g.no));
             h->um_grid_p = h->nsm * std::max(1, bp);
