@@ -375,6 +375,37 @@ int mdft_set_warm_net(mdft_handle *h, mdft_warm_net *net);
 /* stats[0]: warm-started solves, stats[1]: of which redone from the bulk guess. */
 int mdft_get_warm_stats(const mdft_handle *h, long long *stats);
 
+/* ---- Multi-species solvent (nb_solvent > 1) ----
+ *
+ * energy_and_gradient of a solvent of nspec >= 2 species: replaces the excess pointer
+ * set to energy_cproj_mrso_mixture (src/module_init_simu.f90:67-71,
+ * src/module_energy_cproj_mrso_mixture.f90:67-850) with the ideal and external terms summed
+ * over species (src/module_energy_ideal_and_external.f90:46-72).
+ *
+ * Each species is an FP64 handle on one grid, mmax, mrso, temperature and device, created
+ * with that species' n0 already multiplied by its mole fraction (as the reference stores
+ * it, src/module_solvent.f90:221-222) and its own c(k) file, with its vext set
+ * (mdft_set_vext or mdft_compute_vext with its own sites).  mole_fraction[s] must lie in
+ * (0, 1] and the fractions must sum to exactly 1 (src/module_solvent.f90:476-485; a zero
+ * fraction would give n0 = 0, which mdft_create refuses).  The mixture uses the species
+ * handles' buffers and streams: while it is in use, do not evaluate on those handles
+ * directly, and destroy it before them.  The reference takes the mixture routine only for
+ * nspec > 1, so nspec = 1 is refused; that routine differs from the single-species one in
+ * two ways, kept here: -q is rotated with R(m,mup,khi) (single species: R(m,mup,-khi)) and
+ * at self-conjugate k-points the q result is kept.  As in the reference, species s2's
+ * excess field is gamma_{s2} = sum_s c(s2) (x) drho_s (c_{s2,s} taken as c_{s2}).
+ *
+ * xi, df: [nspec][nz][ny][nx][no] doubles (each species' block in the single-species layout,
+ * df as the reference's df(no,nx,ny,nz,nspec)); terms = {F_id, F_ext, F_exc, constant
+ * corrections}, F_id and F_ext summed over species, the corrections species 0's
+ * (mdft_set_constant_correction). */
+typedef struct mdft_mixture mdft_mixture;
+int mdft_mixture_create(mdft_handle *const *species, int nspec, const double *mole_fraction, mdft_mixture **out);
+int mdft_mixture_destroy(mdft_mixture *m);
+int mdft_mixture_energy_and_gradient(mdft_mixture *m, const double *xi, double *f, double *df, double *terms);
+/* Device arrays (d_df may be NULL: energy only). */
+int mdft_mixture_energy_and_gradient_device(mdft_mixture *m, const double *d_xi, double *d_df, double *f, double *terms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,7 +39,10 @@ struct OzTables {
 // value = sum_t c_t X_t (x) U_t with X a level-1 entry and U a level l-1 entry (or the zero
 // slot); R[dest] = value and R[fill] = (s Re, -s Im), except at (l,0,0) where the
 // reference's symmetric fill negates Im in place.
-inline bool build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
+// mix: the rotations of -q as the multi-species routine writes them, with R(m,mup,khi)
+// (src/module_energy_cproj_mrso_mixture.f90:519,638) where the single-species routine uses
+// R(m,mup,-khi) (src/module_energy_cproj_mrso.f90:517,644).  Only the r2 indices change.
+inline bool build_oz_tables(const Grid &g, const CTable &ct, OzTables &T, bool mix = false) {
     const int M = g.mmax, mrso = g.mrso, np = g.np;
     if (np >= 256 || rot_off(M + 1) + 1 >= 2048 || ct.ncoef >= 4096) return false;  // term encodings
     auto pidx = [&](int m, int mup, int mu2) { return g.pidx(m, mup, mu2); };
@@ -47,10 +50,11 @@ inline bool build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
     T.nrot = rot_off(M + 1);
     const int zero = T.nrot;
     std::vector<int> fwd_off{0}, fwd, oz_off{0}, ozt, bwd_off{0}, bwd, sign;
+    const int ks = mix ? 1 : -1;  // khi of the -q rotations is ks * khi
     for (int o = 0; o < np; ++o) {
         const int m = g.pm[o], khi = g.pmup[o], mu2 = g.pmu[o] / mrso;
         // forward rotation of output (m, khi, mu2): sum over mup (:505-523)
-        for (int mup = -m; mup <= m; ++mup) fwd.push_back(pack_rot_term(pidx(m, mup, mu2), ridx(m, mup, khi), ridx(m, mup, -khi)));
+        for (int mup = -m; mup <= m; ++mup) fwd.push_back(pack_rot_term(pidx(m, mup, mu2), ridx(m, mup, khi), ridx(m, mup, ks * khi)));
         fwd_off.push_back((int)fwd.size());
         // OZ sum of output (m, khi, mu2) (:561-606)
         int ia = ct.ia_start[o];
@@ -58,7 +62,7 @@ inline bool build_oz_tables(const Grid &g, const CTable &ct, OzTables &T) {
             for (int nu2 = -n / mrso; nu2 <= n / mrso; ++nu2, ++ia) ozt.push_back(pack_oz_term(ia, pidx(n, khi, std::abs(nu2)), nu2 < 0 ? 1 : 0));
         oz_off.push_back((int)ozt.size());
         // back rotation of output (m, mup, mu2): sum over khi (:626-641)
-        for (int k = -m; k <= m; ++k) bwd.push_back(pack_rot_term(pidx(m, k, mu2), ridx(m, khi, k), ridx(m, khi, -k)));
+        for (int k = -m; k <= m; ++k) bwd.push_back(pack_rot_term(pidx(m, k, mu2), ridx(m, khi, k), ridx(m, khi, ks * k)));
         bwd_off.push_back((int)bwd.size());
         sign.push_back(neg1pow(m));
     }
@@ -133,6 +137,7 @@ struct Oz2Args {
     int mmax, np, ncoef, nq;
     double dq, twopi_lx, twopi_ly, twopi_lz;
     int quirks;  // FP64 path: FP32 rounding of the flushed entries and the gamma flush, as the reference
+    int accumulate;  // Mode 1: add the results to out instead of storing them
     int n_ints, n_dbls, nrot;
     int fwd_off, fwd_terms, oz_off, oz_terms, bwd_off, bwd_terms, sign, lvl_off, rec_int;
 };
@@ -158,10 +163,15 @@ inline size_t oz2_smem_bytes(const Oz2Args &a, int W) {
 }
 
 // smem: ints | coefficients (T) | flags[2W] | per warp: R[nrot+1], ceff[ncoef], dq, dmq, rq, rmq, gq, gmq
-template <typename T>
+// Mode 0: the single-species step, in place on planes (out unused).  Mode 1: the
+// multi-species step (src/module_energy_cproj_mrso_mixture.f90:478-664) of one (s, s2) pair:
+// reads species s's planes, stores (a.accumulate: adds) gamma_{s2} to out; at self-conjugate
+// points it keeps the q result (:648-660); with tables built with mix = true.
+template <typename T, int Mode = 0>
 __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ planes,
                                              const typename Cplx<T>::t *__restrict__ ctab, const int *__restrict__ gints,
-                                             const double *__restrict__ gdbls, Oz2Args a) {
+                                             const double *__restrict__ gdbls, Oz2Args a,
+                                             typename Cplx<T>::t *__restrict__ out) {
     using C = typename Cplx<T>::t;
     extern __shared__ __align__(16) unsigned char oz2_smem[];
     const int W = blockDim.x >> 5;
@@ -385,13 +395,23 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
     for (int e = threadIdx.x; e < 2 * np * W; e += blockDim.x) {
         const int side = e / (np * W), rem = e % (np * W), ip = rem / W, j = rem % W;
         if (!flags[j]) continue;
-        if (side == 0 && flags[W + j]) continue;
+        if (flags[W + j] && side == (Mode == 0 ? 0 : 1)) continue;
         const long long kj = k0 + j;
         const int jx = (int)(kj % a.nx), jy = (int)((kj / a.nx) % a.ny), jz = (int)(kj / ((long long)a.nx * a.ny));
         long long kidx;
         if (side == 0) kidx = ((long long)jz * a.ny + jy) * a.nx + jx;
         else kidx = ((long long)((a.nz - jz) % a.nz) * a.ny + (a.ny - jy) % a.ny) * a.nx + (a.nx - jx) % a.nx;
-        planes[(size_t)ip * a.N + kidx] = wbase[(size_t)j * per_warp + (a.nrot + 1) + a.ncoef + side * np + ip];
+        const C v = wbase[(size_t)j * per_warp + (a.nrot + 1) + a.ncoef + side * np + ip];
+        if (Mode == 0) {
+            planes[(size_t)ip * a.N + kidx] = v;
+        } else if (a.accumulate) {
+            C o = out[(size_t)ip * a.N + kidx];
+            o.x += v.x;
+            o.y += v.y;
+            out[(size_t)ip * a.N + kidx] = o;
+        } else {
+            out[(size_t)ip * a.N + kidx] = v;
+        }
     }
     }  // group loop
 }

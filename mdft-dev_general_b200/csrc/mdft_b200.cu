@@ -413,6 +413,72 @@ void stage_mark(mdft_handle *h, int i) {
     if (h->timing) cudaEventRecord(h->ev[i], h->stream);
 }
 
+// Arguments of the S7 gather.  The excess prefactor -kT 2 (4 pi^2) / mrso / n0
+// (src/module_energy_cproj_mrso.f90:728) carries a species' mole fraction as `scale` in a
+// multi-species evaluation (src/module_energy_cproj_mrso_mixture.f90:791).
+GatherArgs gather_args(const mdft_handle *h, int df_mode, int do_ideal, const void *dvec, double scale) {
+    const Grid &g = h->g;
+    GatherArgs ga;
+    ga.fail_wait = h->wait_fail ? 1 : 0;
+    ga.N = g.N;
+    ga.no = g.no;
+    ga.np = g.np;
+    ga.rho0 = g.rho0;
+    ga.kT = g.kT;
+    ga.dv = g.dv;
+    const double fourpisq = 4.0 * kPi * kPi;
+    ga.prefactor = -g.kT * 2.0 * fourpisq / g.mrso / g.n0;
+    if (scale != 1.0) ga.prefactor *= scale;
+    ga.cst = 1.0 / (double)(g.nx * g.ny * g.nz);
+    ga.do_ideal = do_ideal;
+    ga.df_mode = df_mode;
+    ga.dvec = dvec;
+    return ga;
+}
+
+// S1 on CUDA cores, FP64 point: the bulk-copy projection where it fits and xi is 16-byte
+// aligned, else the tiled one.
+template <typename T>
+void launch_project_cc(mdft_handle *h, const double *d_xi, const T *A, typename Cplx<T>::t *planes, const AngularArgs &aa) {
+    const Grid &g = h->g;
+    if ((sizeof(T) == 8 ? h->pt_ok64 : h->pt_ok32) && ((uintptr_t)d_xi & 15u) == 0) {
+        const int ntiles = (int)(g.N / kPtBM);
+        k_project_tma<T><<<std::min(ntiles, h->nsm), 256, project_tma_smem_bytes<T>(g.np, g.no), h->stream>>>(d_xi, A, planes,
+                                                                                                             h->kerr.p, aa, ntiles);
+    } else if (h->bm_project == 64)
+        k_project<T, 64><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(64, g.no), h->stream>>>(d_xi, A, planes, aa);
+    else
+        k_project<T, 32><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(32, g.no), h->stream>>>(d_xi, A, planes, aa);
+}
+
+// S7 + ideal/external on CUDA cores, FP64 point and gradient: the bulk-copy gather with
+// gt_ncol column groups (gt_ncol > 0), else the tiled one.  Returns the number of partial
+// rows k_reduce_sums folds.
+template <typename T>
+long long launch_gather_cc(mdft_handle *h, const typename Cplx<T>::t *planes, const T *B, const double *d_xi, double *d_df,
+                           const GatherArgs &ga, int gt_ncol) {
+    const Grid &g = h->g;
+    if (gt_ncol > 0) {
+        const int ntiles = (int)(g.N / gt_bm<T>());
+        const int grid = std::min(ntiles, h->nsm * (sizeof(T) == 8 ? 1 : 2));
+        const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
+        if (gt_ncol == 1)
+            k_gather_tma<T, 1, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        else if (gt_ncol == 2)
+            k_gather_tma<T, 2, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        else
+            k_gather_tma<T, 3, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
+        return grid;
+    }
+    if (h->bm_gather == 64)
+        k_gather<T, 64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(64, g.np), h->stream>>>(
+            planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+    else
+        k_gather<T, 32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(32, g.np), h->stream>>>(
+            planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+    return h->nblk_gather;
+}
+
 // The excess-term pipeline plus (optionally) the ideal/external term on device
 // arrays, in precision T; leaves {F_id, F_ext, sum_exc, df.dvec, max|df|} in h->sums.
 template <typename T>
@@ -457,14 +523,9 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
         const int ntiles = (int)(g.N / kPtBM);
         k_project_tma<float, float><<<std::min(ntiles, h->pt_grid_x32), 256, project_tma_smem_bytes<float, float>(g.np, g.no), h->stream>>>(
             static_cast<const float *>(xin), (const float *)A, (float2 *)planes, h->kerr.p, aa, ntiles);
-    } else if ((dbl ? h->pt_ok64 : h->pt_ok32) && ((uintptr_t)d_xi & 15u) == 0) {
-        const int ntiles = (int)(g.N / kPtBM);
-        k_project_tma<T><<<std::min(ntiles, h->nsm), 256, project_tma_smem_bytes<T>(g.np, g.no), h->stream>>>(d_xi, A, planes,
-                                                                                                             h->kerr.p, aa, ntiles);
-    } else if (h->bm_project == 64)
-        k_project<T, 64><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(64, g.no), h->stream>>>(d_xi, A, planes, aa);
-    else
-        k_project<T, 32><<<(unsigned)h->nblk_project, kAngThreads, project_smem_bytes<T>(32, g.no), h->stream>>>(d_xi, A, planes, aa);
+    } else {
+        launch_project_cc<T>(h, d_xi, A, planes, aa);
+    }
     int rc = check_cuda(cudaGetLastError(), "project launch");
     if (rc) return rc;
     stage_mark(h, 1);
@@ -477,25 +538,12 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
         launch_ozp(h, (float2 *)planes, (const float2 *)ctab, oz);
     else
         k_oz2<T><<<dbl ? h->oz_grid : h->oz_grid32, 32 * ozw, dbl ? h->oz_smem : h->oz_smem32, h->stream>>>(planes, ctab, h->oz_ints.p,
-                                                                                                           h->oz_dbls.p, oz);
+                                                                                                           h->oz_dbls.p, oz, nullptr);
     if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
     stage_mark(h, 3);
     if ((rc = launch_fft_t<T>(h, planes, tw, -1))) return rc;
     stage_mark(h, 4);
-    GatherArgs ga;
-    ga.fail_wait = h->wait_fail ? 1 : 0;
-    ga.N = g.N;
-    ga.no = g.no;
-    ga.np = g.np;
-    ga.rho0 = g.rho0;
-    ga.kT = g.kT;
-    ga.dv = g.dv;
-    const double fourpisq = 4.0 * kPi * kPi;
-    ga.prefactor = -g.kT * 2.0 * fourpisq / g.mrso / g.n0;
-    ga.cst = 1.0 / (double)(g.nx * g.ny * g.nz);
-    ga.do_ideal = do_ideal;
-    ga.df_mode = d_df ? df_mode : 0;
-    ga.dvec = dvec;
+    const GatherArgs ga = gather_args(h, d_df ? df_mode : 0, do_ideal, dvec, 1.0);
     const int gt_ncol = dbl ? h->gt_ncol64 : h->gt_ncol32;
     auto al16 = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
     long long red_blocks = h->nblk_gather;
@@ -534,7 +582,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
         else
             k_gather_umma<double, double, 0><<<grid, kUmThreads, smem, h->stream>>>(pl, h->um_gimg.p, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, h->um_gs, ntiles);
         if (!(x32 && v84 && h->ring_g)) red_blocks = grid;
-    } else if (tma_gather) {
+    } else if (tma_gather && (x32 || vec32)) {
         const int ntiles = (int)(g.N / gt_bm<T>());
         const int grid = std::min(ntiles, h->nsm * (dbl ? 1 : 2));
         const size_t smem = gather_tma_smem_bytes<T>(g.np, g.no, gt_ncol);
@@ -550,7 +598,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
                 k_gather_tma<float, 2, float, float><<<grid, kGtThreads, smem, h->stream>>>(pl, B32, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
             else
                 k_gather_tma<float, 3, float, float><<<grid, kGtThreads, smem, h->stream>>>(pl, B32, x32p, h->vext32.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
-        } else if (vec32) {
+        } else {
             float *df32 = reinterpret_cast<float *>(d_df);
             if (gt_ncol == 1)
                 k_gather_tma<T, 1, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
@@ -558,21 +606,11 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
                 k_gather_tma<T, 2, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
             else
                 k_gather_tma<T, 3, float><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, df32, h->partial.p, h->kerr.p, ga, ntiles);
-        } else {
-            if (gt_ncol == 1)
-                k_gather_tma<T, 1, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
-            else if (gt_ncol == 2)
-                k_gather_tma<T, 2, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
-            else
-                k_gather_tma<T, 3, double><<<grid, kGtThreads, smem, h->stream>>>(planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, h->kerr.p, ga, ntiles);
         }
         red_blocks = grid;
-    } else if (h->bm_gather == 64)
-        k_gather<T, 64><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(64, g.np), h->stream>>>(
-            planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
-    else
-        k_gather<T, 32><<<(unsigned)h->nblk_gather, kAngThreads, gather_smem_bytes<T>(32, g.np), h->stream>>>(
-            planes, B, d_xi, h->vext.p, h->w.p, d_df, h->partial.p, ga);
+    } else {
+        red_blocks = launch_gather_cc<T>(h, planes, B, d_xi, d_df, ga, tma_gather ? gt_ncol : 0);
+    }
     if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
     k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, red_blocks, h->sums.p);
     h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft_t)
@@ -1104,3 +1142,4 @@ int mdft_get_stage_times(const mdft_handle *h, double *ms5, int *count) {
 }  // extern "C"
 
 #include "solve.cuh"
+#include "mixture.cuh"

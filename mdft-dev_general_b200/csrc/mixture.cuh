@@ -1,0 +1,222 @@
+// Multi-species solvent: energy_and_gradient with nspec > 1 species
+// (src/module_energy_and_gradient.f90:86-217, excess_energy => energy_cproj_mrso_mixture by
+// src/module_init_simu.f90:67-71).
+//
+// A mixture binds nspec species handles on one grid, angular order, symmetry order,
+// temperature and device, all FP64.  Each handle holds one species: its n0 (the pure
+// fluid's times the mole fraction, src/module_solvent.f90:221-222), its c(k) table and its
+// vext.  One evaluation:
+//   * species s, on its handle's stream: the S1 projection of rho0_s (xi_s^2 - 1) into the
+//     handle's planes and their forward FFT (src/module_energy_cproj_mrso_mixture.f90:283-335);
+//   * species s2, on its stream once every forward FFT is done:
+//     gamma_{s2} = sum_s OZ_{c(s2)}(drho_s) by nspec launches of k_oz2<double, 1> (the first
+//     stores, the others add, in the reference's order over s, :483-664), the inverse FFT of
+//     gamma_{s2} (:690-719), then the gather of species s2 with its ideal and external terms
+//     and the excess prefactor times x_{s2} (:788-810,
+//     src/module_energy_ideal_and_external.f90:46-72).
+// The mixture owns the gamma planes (nspec x np x N complex) and the OZ term tables of the
+// multi-species rotation form (build_oz_tables with mix = true).
+#pragma once
+
+#include <vector>
+
+struct mdft_mixture {
+    std::vector<mdft_handle *> sp;
+    std::vector<double> x;
+    int device = 0;
+    DevBuf<double2> gam;  // [nspec][np][N]
+    DevBuf<int> oz_ints;
+    DevBuf<double> oz_dbls;
+    int oz_grid = 0;
+    DevBuf<double> xi, df;  // staging of the host entry point, [nspec][N][no]
+    std::vector<cudaEvent_t> ev_fwd;
+};
+
+namespace {
+
+int mixture_check(const mdft_mixture *m) {
+    if (!m) { set_error("null mixture"); return MDFT_E_ARG; }
+    return check_cuda(cudaSetDevice(m->device), "cudaSetDevice");
+}
+
+// Launches one evaluation; leaves each species' sums on its handle (finish_sums reads them).
+int mixture_launch(mdft_mixture *m, const double *d_xi, double *d_df) {
+    const int ns = (int)m->sp.size();
+    const Grid &g = m->sp[0]->g;
+    const size_t n = (size_t)g.N * g.no;
+    int rc;
+    for (int s = 0; s < ns; ++s) {
+        mdft_handle *h = m->sp[s];
+        const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
+        const AngularArgs aa{g.N, g.no, g.np, h->g.rho0};
+        launch_project_cc<double>(h, d_xi + s * n, h->A.p, h->planes.p, aa);
+        if ((rc = check_cuda(cudaGetLastError(), "project launch"))) return rc;
+        if ((rc = launch_fft_t<double>(h, h->planes.p, tw, +1))) return rc;
+        if ((rc = check_cuda(cudaEventRecord(m->ev_fwd[s], h->stream), "event record"))) return rc;
+        h->launches += 1;
+    }
+    for (int s2 = 0; s2 < ns; ++s2) {
+        mdft_handle *h = m->sp[s2];
+        double2 *gam = m->gam.p + (size_t)s2 * g.np * g.N;
+        for (int s = 0; s < ns; ++s)
+            if ((rc = check_cuda(cudaStreamWaitEvent(h->stream, m->ev_fwd[s], 0), "stream wait"))) return rc;
+        Oz2Args oz = h->oz;  // this species' c table: nq, dq
+        oz.quirks = 1;
+        for (int s = 0; s < ns; ++s) {
+            oz.accumulate = s > 0 ? 1 : 0;
+            k_oz2<double, 1><<<m->oz_grid, 32 * h->oz_warps, h->oz_smem, h->stream>>>(m->sp[s]->planes.p, h->ctab.p, m->oz_ints.p,
+                                                                                     m->oz_dbls.p, oz, gam);
+            if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
+        }
+        const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
+        if ((rc = launch_fft_t<double>(h, gam, tw, -1))) return rc;
+        const GatherArgs ga = gather_args(h, d_df ? 1 : 0, 1, nullptr, m->x[s2]);
+        const bool tma = h->gt_ncol64 > 0 && ((uintptr_t)(d_xi + s2 * n) & 15u) == 0;
+        const long long rows = launch_gather_cc<double>(h, gam, h->B.p, d_xi + s2 * n, d_df ? d_df + s2 * n : nullptr, ga,
+                                                        tma ? h->gt_ncol64 : 0);
+        if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
+        k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, rows, h->sums.p);
+        if ((rc = check_cuda(cudaGetLastError(), "reduce launch"))) return rc;
+        h->launches += ns + 2;
+    }
+    return MDFT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdft_mixture_create(mdft_handle *const *species, int nspec, const double *mole_fraction, mdft_mixture **out) {
+    if (!species || !mole_fraction || !out) { set_error("null argument"); return MDFT_E_ARG; }
+    *out = nullptr;
+    if (nspec < 2) {
+        set_error("a mixture needs at least two species (one species uses the handle itself)");
+        return MDFT_E_ARG;
+    }
+    const mdft_handle *h0 = species[0];
+    if (!h0) { set_error("null species handle"); return MDFT_E_ARG; }
+    const Grid &g0 = h0->g;
+    double xsum = 0.0;
+    for (int s = 0; s < nspec; ++s) {
+        const mdft_handle *h = species[s];
+        if (!h) { set_error("null species handle"); return MDFT_E_ARG; }
+        for (int t = 0; t < s; ++t)
+            if (species[t] == h) { set_error("species %d and %d are the same handle", t, s); return MDFT_E_ARG; }
+        const Grid &g = h->g;
+        if (g.nx != g0.nx || g.ny != g0.ny || g.nz != g0.nz || g.lx != g0.lx || g.ly != g0.ly || g.lz != g0.lz ||
+            g.mmax != g0.mmax || g.mrso != g0.mrso || g.kT != g0.kT || h->device != h0->device) {
+            set_error("species %d differs from species 0 in grid, angular order, symmetry order, temperature or device", s);
+            return MDFT_E_ARG;
+        }
+        if (h->precision != MDFT_PREC_FP64) { set_error("mixtures are evaluated in FP64: species %d is not", s); return MDFT_E_ARG; }
+        if (h->ct.ncoef != h0->ct.ncoef) { set_error("species %d has another c(k) coefficient count", s); return MDFT_E_ARG; }
+        const double x = mole_fraction[s];
+        if (!(x > 0.0 && x <= 1.0)) { set_error("mole fraction of species %d is %g, outside (0, 1]", s, x); return MDFT_E_ARG; }
+        xsum += x;
+    }
+    // src/module_solvent.f90:476-480: the fractions must sum to exactly one
+    if (xsum != 1.0) { set_error("mole fractions sum to %.17g, not 1", xsum); return MDFT_E_ARG; }
+    std::unique_ptr<mdft_mixture> m(new mdft_mixture());
+    m->sp.assign(species, species + nspec);
+    m->x.assign(mole_fraction, mole_fraction + nspec);
+    m->device = h0->device;
+    int rc;
+    if ((rc = mixture_check(m.get()))) return rc;
+    OzTables tb;
+    if (!build_oz_tables(g0, h0->ct, tb, true)) { set_error("OZ term tables exceed their index encoding"); return MDFT_E_ARG; }
+    if ((int)tb.ints.size() != h0->oz.n_ints || (int)tb.dbls.size() != h0->oz.n_dbls) {
+        set_error("multi-species OZ tables differ in layout from the species tables");
+        return MDFT_E_STATE;
+    }
+    const size_t planes = (size_t)nspec * g0.np * g0.N;
+    if ((rc = alloc_check(m->gam.alloc(planes), "mixture gamma planes", planes * sizeof(double2)))) return rc;
+    if ((rc = alloc_check(m->oz_ints.alloc(tb.ints.size()), "OZ tables", tb.ints.size() * 4))) return rc;
+    if ((rc = alloc_check(m->oz_dbls.alloc(std::max<size_t>(1, tb.dbls.size())), "OZ tables", tb.dbls.size() * 8))) return rc;
+    if ((rc = check_cuda(cudaMemcpy(m->oz_ints.p, tb.ints.data(), tb.ints.size() * 4, cudaMemcpyHostToDevice), "OZ tables"))) return rc;
+    if (!tb.dbls.empty() &&
+        (rc = check_cuda(cudaMemcpy(m->oz_dbls.p, tb.dbls.data(), tb.dbls.size() * 8, cudaMemcpyHostToDevice), "OZ tables")))
+        return rc;
+    int maxsmem = 0;
+    if ((rc = check_cuda(cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, m->device), "device attribute")))
+        return rc;
+    if ((rc = allow_smem((const void *)k_oz2<double, 1>, maxsmem))) return rc;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oz2<double, 1>, 32 * h0->oz_warps, h0->oz_smem);
+    const long long nk = (long long)g0.nx * g0.ny * (g0.nz / 2 + 1);
+    const long long groups = (nk + h0->oz_warps - 1) / h0->oz_warps;
+    m->oz_grid = (int)std::min<long long>(groups, (long long)std::max(1, per_sm) * h0->nsm);
+    m->ev_fwd.assign(nspec, nullptr);
+    for (int s = 0; s < nspec; ++s)
+        if ((rc = check_cuda(cudaEventCreateWithFlags(&m->ev_fwd[s], cudaEventDisableTiming), "event create"))) {
+            for (cudaEvent_t e : m->ev_fwd)
+                if (e) cudaEventDestroy(e);
+            return rc;
+        }
+    *out = m.release();
+    return MDFT_OK;
+}
+
+int mdft_mixture_destroy(mdft_mixture *m) {
+    if (!m) return MDFT_OK;
+    cudaSetDevice(m->device);
+    for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : m->ev_fwd)
+        if (e) cudaEventDestroy(e);
+    m->gam.free(); m->oz_ints.free(); m->oz_dbls.free(); m->xi.free(); m->df.free();
+    delete m;
+    return MDFT_OK;
+}
+
+int mdft_mixture_energy_and_gradient_device(mdft_mixture *m, const double *d_xi, double *d_df, double *f, double *terms) {
+    int rc = mixture_check(m);
+    if (rc) return rc;
+    if (!d_xi || !f) { set_error("null argument"); return MDFT_E_ARG; }
+    if ((rc = mixture_launch(m, d_xi, d_df))) {
+        for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
+        return rc;
+    }
+    // src/module_energy_ideal_and_external.f90:46-72 sums F_id and F_ext over species in
+    // order; F_exc = 0.5 dv sum_{s2} (...) (src/module_energy_cproj_mrso_mixture.f90:810)
+    double fid = 0.0, fext = 0.0, sexc = 0.0;
+    int first = 0;
+    for (mdft_handle *h : m->sp) {
+        double a = 0, b = 0, c = 0;
+        const int r = finish_sums(h, &a, &b, &c);  // synchronises the species' stream
+        if (r && !first) first = r;
+        fid += a;
+        fext += b;
+        sexc += h->h_sums[2];
+    }
+    if (first) return first;
+    const mdft_handle *h0 = m->sp[0];
+    const double fexc = sexc * 0.5 * h0->g.dv;
+    *f = combine(h0, fid, fext, fexc);
+    if (terms) {
+        terms[0] = fid;
+        terms[1] = fext;
+        terms[2] = fexc;
+        terms[3] = h0->const_corr;
+    }
+    return MDFT_OK;
+}
+
+int mdft_mixture_energy_and_gradient(mdft_mixture *m, const double *xi, double *f, double *df, double *terms) {
+    int rc = mixture_check(m);
+    if (rc) return rc;
+    if (!xi || !f) { set_error("null argument"); return MDFT_E_ARG; }
+    const Grid &g = m->sp[0]->g;
+    const size_t n = (size_t)m->sp.size() * g.N * g.no;
+    if (!m->xi.p && (rc = alloc_check(m->xi.alloc(n), "mixture xi", n * 8))) return rc;
+    if (df && !m->df.p && (rc = alloc_check(m->df.alloc(n), "mixture df", n * 8))) return rc;
+    cudaStream_t st = m->sp[0]->stream;
+    if ((rc = check_cuda(cudaMemcpyAsync(m->xi.p, xi, n * 8, cudaMemcpyHostToDevice, st), "xi upload"))) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(st), "xi upload"))) return rc;
+    if ((rc = mdft_mixture_energy_and_gradient_device(m, m->xi.p, df ? m->df.p : nullptr, f, terms))) return rc;
+    if (df) {
+        if ((rc = check_cuda(cudaMemcpyAsync(df, m->df.p, n * 8, cudaMemcpyDeviceToHost, st), "df download"))) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(st), "df download"))) return rc;
+    }
+    return MDFT_OK;
+}
+
+}  // extern "C"

@@ -142,6 +142,11 @@ SIGNATURES = {
     "mdft_warm_expand_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "mdft_set_warm_net": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mdft_get_warm_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    # multi-species solvent
+    "mdft_mixture_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, _DP, C.POINTER(C.c_void_p)]),
+    "mdft_mixture_destroy": (C.c_int, [C.c_void_p]),
+    "mdft_mixture_energy_and_gradient": (C.c_int, [C.c_void_p, _DP, _DP, _DP, _DP]),
+    "mdft_mixture_energy_and_gradient_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _DP, _DP]),
 }
 
 
@@ -404,6 +409,60 @@ class Engine:
         cnt = C.c_int()
         _check(lib().mdft_get_stage_times(self.h, _p(ms), C.byref(cnt)))
         return dict(zip(("project", "fft_forward", "oz", "fft_inverse", "gather"), ms)), cnt.value
+
+
+class Mixture:
+    """A solvent of several species (energy_cproj_mrso_mixture), each an FP64 Engine on one grid.
+
+    Create every species' Engine with n0 = (pure fluid n0) * (its mole fraction), its own
+    c(k) file and its vext; the Mixture borrows their buffers and streams, so close it before
+    them and do not evaluate on them while it is open.
+    """
+
+    def __init__(self, engines, mole_fractions):
+        self.engines = list(engines)
+        ns = len(self.engines)
+        x = np.ascontiguousarray(mole_fractions, dtype=np.float64)
+        if x.shape != (ns,):
+            raise MdftError("one mole fraction per species")
+        hs = (C.c_void_p * ns)(*[e.h for e in self.engines])
+        h = C.c_void_p()
+        _check(lib().mdft_mixture_create(hs, ns, _p(x), C.byref(h)))
+        self.h = h
+        self.shape = (ns,) + tuple(self.engines[0].shape)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mdft_mixture_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def energy_and_gradient(self, xi, want_grad=True):
+        """Return (f, df, terms): xi and df of shape (nspec, nz, ny, nx, no), terms as Engine's."""
+        x = np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        f = np.zeros(1)
+        terms = np.zeros(4)
+        df = np.empty(self.shape) if want_grad else None
+        _check(lib().mdft_mixture_energy_and_gradient(self.h, _p(x), _p(f), _p(df), _p(terms)))
+        return float(f[0]), df, terms
+
+    def energy_and_gradient_device(self, xi_ptr: int, df_ptr: int | None):
+        f = np.zeros(1)
+        terms = np.zeros(4)
+        _check(lib().mdft_mixture_energy_and_gradient_device(self.h, C.c_void_p(xi_ptr),
+                                                             C.c_void_p(df_ptr) if df_ptr else None, _p(f), _p(terms)))
+        return float(f[0]), terms
 
 
 def solve_batch(engines, solutes, solvent, rvdw=10.0, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, precision=PREC_FP64,

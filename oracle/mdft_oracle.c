@@ -751,9 +751,13 @@ static int g_quirks = 3;
 void orc_set_quirks(int q) { g_quirks = q; }
 static inline double q_sp(double x, int bit) { return (g_quirks & bit) ? to_sp(x) : x; }
 
-static void oz_pair(const orc *o, const double q[3], cplx *dq_, cplx *dmq_, int q_eq_mq, int nyq_flag,
+/* mix = 1: the multi-species routine's form (module_energy_cproj_mrso_mixture.f90:509-523,
+   :630-640), which rotates -q with R(m,mup,khi) where the single-species routine uses
+   R(m,mup,-khi) (module_energy_cproj_mrso.f90:517,644). */
+static void oz_pair(const orc *o, const double q[3], cplx *dq_, cplx *dmq_, int q_eq_mq, int nyq_flag, int mix,
                     cplx *outq, cplx *outmq, double *R, cplx *ceff, cplx *drq, cplx *drmq, cplx *gq, cplx *gmq)
 {
+    const int ks = mix ? 1 : -1; /* khi of the -q rotation is ks*khi */
     const int M = o->mmax, W = 2 * M + 1, np = o->np, mrso = o->mrso;
     orc_rotation_matrix(M, q, R);
     const int sz = (M + 1) * W * W;
@@ -772,7 +776,7 @@ static void oz_pair(const orc *o, const double q[3], cplx *dq_, cplx *dmq_, int 
                 for (int mup = -m; mup <= m; ++mup) {
                     int jp = o->p3p[p3idx(o, m, mup, mu2)];
                     a = a + gq[jp] * RR(m, mup, khi);
-                    b = b + gmq[jp] * RR(m, mup, -khi);
+                    b = b + gmq[jp] * RR(m, mup, ks * khi);
                 }
                 drq[ip] = a;
                 drmq[ip] = b * ((m % 2 == 0) ? 1.0 : -1.0);
@@ -825,7 +829,7 @@ static void oz_pair(const orc *o, const double q[3], cplx *dq_, cplx *dmq_, int 
                 for (int khi = -m; khi <= m; ++khi) {
                     int jp = o->p3p[p3idx(o, m, khi, mu2)];
                     a = a + gq[jp] * conj(RR(m, mup, khi));
-                    b = b + gmq[jp] * conj(RR(m, mup, -khi));
+                    b = b + gmq[jp] * conj(RR(m, mup, ks * khi));
                 }
                 outq[ip] = a;
                 outmq[ip] = b * ((m % 2 == 0) ? 1.0 : -1.0);
@@ -836,15 +840,15 @@ static void oz_pair(const orc *o, const double q[3], cplx *dq_, cplx *dmq_, int 
 }
 
 /* ------------------------------------------------------------------------- */
-/* energy_cproj_mrso: module_energy_cproj_mrso.f90:61-782.                   */
-static int excess(orc *o, const double *xi, double *fexc, double *df)
+/* The stages of energy_cproj_mrso (module_energy_cproj_mrso.f90:61-782),    */
+/* shared with energy_cproj_mrso_mixture.                                    */
+
+/* S1 projection of rho0 (xi^2 - 1) (:276-290) and S2 forward FFT, sign +1 (:306-329). */
+static void project_forward(const orc *o, const double *xi, cplx *drho /* [N][np] ip fastest */)
 {
     const int nx = o->nx, ny = o->ny, nz = o->nz, np = o->np, no = o->no;
     const long N = o->N;
     const double rho0 = o->rho0;
-    if (!o->c) { set_err("c(k) table not loaded"); return -1; }
-    cplx *drho = o->drho; /* [N][np] ip fastest */
-    /* S1 projection :276-290 */
 #pragma omp parallel
     {
         double *ov = malloc(sizeof(double) * no);
@@ -860,58 +864,87 @@ static int excess(orc *o, const double *xi, double *fexc, double *df)
         free(ov);
         free(ft);
     }
-    /* S2 forward FFT, sign +1 :306-329 */
     cplx *buf = malloc(sizeof(cplx) * N);
     for (int ip = 0; ip < np; ++ip) {
         for (long r = 0; r < N; ++r) buf[r] = drho[r * np + ip];
         fft3d(buf, nx, ny, nz, +1);
         for (long r = 0; r < N; ++r) drho[r * np + ip] = buf[r];
     }
-    /* S3-S5 rotation + OZ + back rotation, serial reference order :462-665 */
-    {
-        char *isok = calloc(N, 1);
-        const int M = o->mmax, W = 2 * M + 1;
-        double *R = malloc(sizeof(double) * 2 * (M + 1) * W * W);
-        cplx *ceff = malloc(sizeof(cplx) * o->ncoef);
-        cplx *tmp = malloc(sizeof(cplx) * 8 * np);
-        cplx *drq = tmp, *drmq = tmp + np, *gq = tmp + 2 * np, *gmq = tmp + 3 * np;
-        cplx *oq = tmp + 4 * np, *omq = tmp + 5 * np, *inq = tmp + 6 * np, *inmq = tmp + 7 * np;
-        for (int izq = 1; izq <= nz / 2 + 1; ++izq) {
-            int izmq = (izq == 1) ? 1 : nz - izq + 2;
-            for (int iyq = 1; iyq <= ny; ++iyq) {
-                int iymq = (iyq == 1) ? 1 : ny - iyq + 2;
-                for (int ixq = 1; ixq <= nx; ++ixq) {
-                    int ixmq = (ixq == 1) ? 1 : nx - ixq + 2;
-                    long rq = ((long)(izq - 1) * ny + (iyq - 1)) * nx + (ixq - 1);
-                    long rmq = ((long)(izmq - 1) * ny + (iymq - 1)) * nx + (ixmq - 1);
-                    if (isok[rq] && isok[rmq]) continue;
-                    int q_eq_mq = (ixmq == ixq && iymq == iyq && izmq == izq);
-                    int nyq = (ixq == nx / 2 + 1 || iyq == ny / 2 + 1 || izq == nz / 2 + 1);
-                    double q[3] = {o->kx[ixq - 1], o->ky[iyq - 1], o->kz[izq - 1]};
-                    for (int i = 0; i < np; ++i) { inq[i] = drho[rq * np + i]; inmq[i] = drho[rmq * np + i]; }
-                    oz_pair(o, q, inq, inmq, q_eq_mq, nyq, oq, omq, R, ceff, drq, drmq, gq, gmq);
-                    for (int i = 0; i < np; ++i) drho[rq * np + i] = oq[i];
-                    for (int i = 0; i < np; ++i) drho[rmq * np + i] = omq[i];
-                    isok[rq] = 1;
-                    isok[rmq] = 1;
+    free(buf);
+}
+
+/* S3-S5, every (q, -q) pair once, in the reference's serial order, with oc's c table.
+   mix = 0 (module_energy_cproj_mrso.f90:462-665): in place (out == in); the -q result
+   replaces the q result at self-conjugate points, conjugated where a Nyquist index is set.
+   mix = 1 (module_energy_cproj_mrso_mixture.f90:478-664): out += the results; at
+   self-conjugate points only the q result is added. */
+static int oz_sweep(const orc *oc, const cplx *in, cplx *out, int mix)
+{
+    const int nx = oc->nx, ny = oc->ny, nz = oc->nz, np = oc->np;
+    const long N = oc->N;
+    char *isok = calloc(N, 1);
+    const int M = oc->mmax, W = 2 * M + 1;
+    double *R = malloc(sizeof(double) * 2 * (M + 1) * W * W);
+    cplx *ceff = malloc(sizeof(cplx) * oc->ncoef);
+    cplx *tmp = malloc(sizeof(cplx) * 8 * np);
+    cplx *drq = tmp, *drmq = tmp + np, *gq = tmp + 2 * np, *gmq = tmp + 3 * np;
+    cplx *oq = tmp + 4 * np, *omq = tmp + 5 * np, *inq = tmp + 6 * np, *inmq = tmp + 7 * np;
+    for (int izq = 1; izq <= nz / 2 + 1; ++izq) {
+        int izmq = (izq == 1) ? 1 : nz - izq + 2;
+        for (int iyq = 1; iyq <= ny; ++iyq) {
+            int iymq = (iyq == 1) ? 1 : ny - iyq + 2;
+            for (int ixq = 1; ixq <= nx; ++ixq) {
+                int ixmq = (ixq == 1) ? 1 : nx - ixq + 2;
+                long rq = ((long)(izq - 1) * ny + (iyq - 1)) * nx + (ixq - 1);
+                long rmq = ((long)(izmq - 1) * ny + (iymq - 1)) * nx + (ixmq - 1);
+                if (isok[rq] && isok[rmq]) continue;
+                int q_eq_mq = (ixmq == ixq && iymq == iyq && izmq == izq);
+                int nyq = (ixq == nx / 2 + 1 || iyq == ny / 2 + 1 || izq == nz / 2 + 1);
+                double q[3] = {oc->kx[ixq - 1], oc->ky[iyq - 1], oc->kz[izq - 1]};
+                for (int i = 0; i < np; ++i) { inq[i] = in[rq * np + i]; inmq[i] = in[rmq * np + i]; }
+                oz_pair(oc, q, inq, inmq, q_eq_mq, mix ? 0 : nyq, mix, oq, omq, R, ceff, drq, drmq, gq, gmq);
+                if (mix) {
+                    for (int i = 0; i < np; ++i) out[rq * np + i] += oq[i];
+                    if (!q_eq_mq)
+                        for (int i = 0; i < np; ++i) out[rmq * np + i] += omq[i];
+                } else {
+                    for (int i = 0; i < np; ++i) out[rq * np + i] = oq[i];
+                    for (int i = 0; i < np; ++i) out[rmq * np + i] = omq[i];
                 }
+                isok[rq] = 1;
+                isok[rmq] = 1;
             }
         }
-        for (long r = 0; r < N; ++r)
-            if (!isok[r]) { set_err("not all gamma_p computed"); free(isok); free(R); free(ceff); free(tmp); free(buf); return -1; }
-        free(isok); free(R); free(ceff); free(tmp);
     }
-    /* S6 inverse FFT, sign -1, times 1/N :690-719 */
+    int rc = 0;
+    for (long r = 0; r < N; ++r)
+        if (!isok[r]) { set_err("not all gamma_p computed"); rc = -1; break; }
+    free(isok); free(R); free(ceff); free(tmp);
+    return rc;
+}
+
+/* S6 inverse FFT, sign -1, times 1/N (:690-719). */
+static void inverse_fft(const orc *o, cplx *drho)
+{
+    const int nx = o->nx, ny = o->ny, nz = o->nz, np = o->np;
+    const long N = o->N;
     const double cst = 1.0 / (double)(nx * ny * nz);
+    cplx *buf = malloc(sizeof(cplx) * N);
     for (int ip = 0; ip < np; ++ip) {
         for (long r = 0; r < N; ++r) buf[r] = drho[r * np + ip];
         fft3d(buf, nx, ny, nz, -1);
         for (long r = 0; r < N; ++r) drho[r * np + ip] = buf[r] * cst;
     }
     free(buf);
-    /* S7 gather + energy + gradient :728-762 */
-    const double fourpisq = 4.0 * ORC_PI * ORC_PI;
-    const double prefactor = -o->kT * 2.0 * fourpisq / o->mrso / o->n0;
+}
+
+/* S7 gather (:728-762): returns sum (xi^2 rho0 - rho0) v with v = prefactor w proj2angl(gamma),
+   and adds 2 rho0 xi v to df. */
+static double gather_excess(const orc *o, const cplx *drho, const double *xi, double prefactor, double *df)
+{
+    const int np = o->np, no = o->no;
+    const long N = o->N;
+    const double rho0 = o->rho0;
     double pff[ORC_NCHUNK];
 #pragma omp parallel
     {
@@ -938,6 +971,47 @@ static int excess(orc *o, const double *xi, double *fexc, double *df)
     }
     double ff = 0.0;
     for (int ch = 0; ch < ORC_NCHUNK; ++ch) ff += pff[ch];
+    return ff;
+}
+
+/* energy_cproj_mrso: module_energy_cproj_mrso.f90:61-782. */
+static int excess(orc *o, const double *xi, double *fexc, double *df)
+{
+    if (!o->c) { set_err("c(k) table not loaded"); return -1; }
+    project_forward(o, xi, o->drho);
+    if (oz_sweep(o, o->drho, o->drho, 0)) return -1;
+    inverse_fft(o, o->drho);
+    const double fourpisq = 4.0 * ORC_PI * ORC_PI;
+    const double prefactor = -o->kT * 2.0 * fourpisq / o->mrso / o->n0;
+    *fexc = gather_excess(o, o->drho, xi, prefactor, df) * 0.5 * o->dv;
+    return 0;
+}
+
+/* energy_cproj_mrso_mixture: module_energy_cproj_mrso_mixture.f90:67-850.  sp[s] holds species
+   s (its n0 already times its mole fraction, module_solvent.f90:221-222, its c table and
+   vext); xi and df are [ns][N][no].  gamma_{s2} = sum_s OZ_{c(s2)}(drho_s), summed in the
+   reference's order (s outer, s2 inner, :483-664), then gathered per s2 with the prefactor
+   -kT 2 (4 pi^2) / mrso / n0(s2) x(s2) (:728-760). */
+static int excess_mixture(orc *const *sp, int ns, const double *xfrac, const double *xi, double *fexc, double *df)
+{
+    const orc *o = sp[0];
+    const long N = o->N, no = o->no, np = o->np;
+    for (int s = 0; s < ns; ++s)
+        if (!sp[s]->c) { set_err("c(k) table not loaded"); return -1; }
+    cplx *gam = calloc((size_t)ns * N * np, sizeof(cplx));
+    if (!gam) { set_err("out of memory"); return -1; }
+    for (int s = 0; s < ns; ++s) project_forward(sp[s], xi + s * N * no, sp[s]->drho);
+    for (int s = 0; s < ns; ++s)
+        for (int s2 = 0; s2 < ns; ++s2)
+            if (oz_sweep(sp[s2], sp[s]->drho, gam + s2 * N * np, 1)) { free(gam); return -1; }
+    const double fourpisq = 4.0 * ORC_PI * ORC_PI;
+    double ff = 0.0;
+    for (int s2 = 0; s2 < ns; ++s2) {
+        inverse_fft(o, gam + s2 * N * np);
+        const double prefactor = -sp[s2]->kT * 2.0 * fourpisq / sp[s2]->mrso / sp[s2]->n0 * xfrac[s2];
+        ff += gather_excess(sp[s2], gam + s2 * N * np, xi + s2 * N * no, prefactor, df ? df + s2 * N * no : NULL);
+    }
+    free(gam);
     *fexc = ff * 0.5 * o->dv;
     return 0;
 }
@@ -980,6 +1054,48 @@ int orc_energy_grad(orc *o, const double *xi, double *f, double *df, double *ter
     double fid, fext, fexc;
     ideal_and_external(o, xi, &fid, &fext, df);
     if (excess(o, xi, &fexc, df)) return -1;
+    double ff = 0.0;
+    ff = ff + fid + fext;
+    ff = ff + fexc;
+    ff = ff + 0.0; /* bridge "no" */
+    ff = ff + o->const_corr;
+    *f = ff;
+    if (terms) { terms[0] = fid; terms[1] = fext; terms[2] = fexc; terms[3] = o->const_corr; }
+    return 0;
+}
+
+/* energy_and_gradient with nspec > 1 species (module_energy_and_gradient.f90:86-217 with the
+   excess pointer on energy_cproj_mrso_mixture, module_init_simu.f90:67-71): the ideal and
+   external terms summed over species (module_energy_ideal_and_external.f90:46-72), then the
+   mixture excess.  xi, df: [ns][N][no]; the constant corrections are sp[0]'s.  The oracle
+   accepts ns = 1 too (the mixture routine's own form of one species). */
+int orc_mixture_energy_grad(orc *const *sp, int ns, const double *xfrac, const double *xi, double *f, double *df,
+                            double *terms)
+{
+    if (ns < 1 || !sp || !xfrac) { set_err("bad species list"); return -1; }
+    const orc *o = sp[0];
+    double xs = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        const orc *p = sp[s];
+        if (!p || p->nx != o->nx || p->ny != o->ny || p->nz != o->nz || p->lx != o->lx || p->ly != o->ly ||
+            p->lz != o->lz || p->mmax != o->mmax || p->mrso != o->mrso || p->kT != o->kT) {
+            set_err("species differ in grid, angular order or temperature");
+            return -1;
+        }
+        if (!(xfrac[s] > 0.0 && xfrac[s] <= 1.0)) { set_err("mole fraction outside (0, 1]"); return -1; }
+        xs += xfrac[s];
+    }
+    if (xs != 1.0) { set_err("mole fractions do not sum to 1"); return -1; }
+    const long n = o->N * o->no;
+    if (df) memset(df, 0, sizeof(double) * n * ns);
+    double fid = 0.0, fext = 0.0, fexc;
+    for (int s = 0; s < ns; ++s) {
+        double a, b;
+        ideal_and_external(sp[s], xi + s * n, &a, &b, df ? df + s * n : NULL);
+        fid += a;
+        fext += b;
+    }
+    if (excess_mixture(sp, ns, xfrac, xi, &fexc, df)) return -1;
     double ff = 0.0;
     ff = ff + fid + fext;
     ff = ff + fexc;

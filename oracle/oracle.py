@@ -62,6 +62,7 @@ def lib():
                                    C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_set_quirks.argtypes = [C.c_int]
         L.orc_pressure_correction.argtypes = [C.c_void_p, dp, C.c_double, C.c_double, dp]
+        L.orc_mixture_energy_grad.argtypes = [C.POINTER(C.c_void_p), C.c_int, dp, dp, dp, dp, dp]
     return _LIB
 
 
@@ -217,3 +218,23 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(lib().orc_last_error().decode())
         return dict(dG=out[0], pmv=out[1], pbulk=out[2], deltaN=out[3])
+
+
+def mixture_energy_grad(species, mole_fractions, xi, want_grad=True):
+    """energy_and_gradient of a multi-species solvent (energy_cproj_mrso_mixture).
+
+    species: Oracle objects on one grid, each created with its n0 times its mole fraction,
+    with its own c(k) table and vext; xi: (nspec, *shape).  Returns (F, df, terms) with
+    df of xi's shape and terms {F_id, F_ext, F_exc, corrections}.
+    """
+    ns = len(species)
+    shape = (ns,) + tuple(species[0].shape)
+    xi = np.ascontiguousarray(xi, dtype=np.float64).reshape(shape)
+    x = np.ascontiguousarray(mole_fractions, dtype=np.float64)
+    hs = (C.c_void_p * ns)(*[o.h for o in species])
+    f = np.zeros(1); terms = np.zeros(4)
+    df = np.zeros(shape) if want_grad else None
+    rc = lib().orc_mixture_energy_grad(hs, ns, _p(x), _p(xi), _p(f), _p(df) if want_grad else None, _p(terms))
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return float(f[0]), df, terms
