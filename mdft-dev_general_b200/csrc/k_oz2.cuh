@@ -40,8 +40,8 @@ struct OzTables {
 // slot); R[dest] = value and R[fill] = (s Re, -s Im), except at (l,0,0) where the
 // reference's symmetric fill negates Im in place.
 // mix: the rotations of -q as the multi-species routine writes them, with R(m,mup,khi)
-// (src/module_energy_cproj_mrso_mixture.f90:519,638) where the single-species routine uses
-// R(m,mup,-khi) (src/module_energy_cproj_mrso.f90:517,644).  Only the r2 indices change.
+// (src/module_energy_cproj_mrso_mixture.f90:551,672) where the single-species routine uses
+// R(m,mup,-khi) (src/module_energy_cproj_mrso.f90:517,636).  Only the r2 indices change.
 inline bool build_oz_tables(const Grid &g, const CTable &ct, OzTables &T, bool mix = false) {
     const int M = g.mmax, mrso = g.mrso, np = g.np;
     if (np >= 256 || rot_off(M + 1) + 1 >= 2048 || ct.ncoef >= 4096) return false;  // term encodings
@@ -164,9 +164,9 @@ inline size_t oz2_smem_bytes(const Oz2Args &a, int W) {
 
 // smem: ints | coefficients (T) | flags[2W] | per warp: R[nrot+1], ceff[ncoef], dq, dmq, rq, rmq, gq, gmq
 // Mode 0: the single-species step, in place on planes (out unused).  Mode 1: the
-// multi-species step (src/module_energy_cproj_mrso_mixture.f90:478-664) of one (s, s2) pair:
+// multi-species step (src/module_energy_cproj_mrso_mixture.f90:491-721) of one (s, s2) pair:
 // reads species s's planes, stores (a.accumulate: adds) gamma_{s2} to out; at self-conjugate
-// points it keeps the q result (:648-660); with tables built with mix = true.
+// points it keeps the q result (:685-709); with tables built with mix = true.
 template <typename T, int Mode = 0>
 __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ planes,
                                              const typename Cplx<T>::t *__restrict__ ctab, const int *__restrict__ gints,

@@ -7,12 +7,12 @@
 // fluid's times the mole fraction, src/module_solvent.f90:221-222), its c(k) table and its
 // vext.  One evaluation:
 //   * species s, on its handle's stream: the S1 projection of rho0_s (xi_s^2 - 1) into the
-//     handle's planes and their forward FFT (src/module_energy_cproj_mrso_mixture.f90:283-335);
+//     handle's planes and their forward FFT (src/module_energy_cproj_mrso_mixture.f90:283-344);
 //   * species s2, on its stream once every forward FFT is done:
 //     gamma_{s2} = sum_s OZ_{c(s2)}(drho_s) by nspec launches of k_oz2<double, 1> (the first
-//     stores, the others add, in the reference's order over s, :483-664), the inverse FFT of
-//     gamma_{s2} (:690-719), then the gather of species s2 with its ideal and external terms
-//     and the excess prefactor times x_{s2} (:788-810,
+//     stores, the others add, in the reference's order over s, :491-721), the inverse FFT of
+//     gamma_{s2} (:746-779), then the gather of species s2 with its ideal and external terms
+//     and the excess prefactor times x_{s2} (:788-809,
 //     src/module_energy_ideal_and_external.f90:46-72).
 // The mixture owns the gamma planes (nspec x np x N complex) and the OZ term tables of the
 // multi-species rotation form (build_oz_tables with mix = true).
@@ -176,7 +176,7 @@ int mdft_mixture_energy_and_gradient_device(mdft_mixture *m, const double *d_xi,
         return rc;
     }
     // src/module_energy_ideal_and_external.f90:46-72 sums F_id and F_ext over species in
-    // order; F_exc = 0.5 dv sum_{s2} (...) (src/module_energy_cproj_mrso_mixture.f90:810)
+    // order; F_exc = 0.5 dv sum_{s2} (...) (src/module_energy_cproj_mrso_mixture.f90:788-809)
     double fid = 0.0, fext = 0.0, sexc = 0.0;
     int first = 0;
     for (mdft_handle *h : m->sp) {

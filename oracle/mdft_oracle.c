@@ -751,9 +751,9 @@ static int g_quirks = 3;
 void orc_set_quirks(int q) { g_quirks = q; }
 static inline double q_sp(double x, int bit) { return (g_quirks & bit) ? to_sp(x) : x; }
 
-/* mix = 1: the multi-species routine's form (module_energy_cproj_mrso_mixture.f90:509-523,
-   :630-640), which rotates -q with R(m,mup,khi) where the single-species routine uses
-   R(m,mup,-khi) (module_energy_cproj_mrso.f90:517,644). */
+/* mix = 1: the multi-species routine's form (module_energy_cproj_mrso_mixture.f90:541-557,
+   :664-677), which rotates -q with R(m,mup,khi) where the single-species routine uses
+   R(m,mup,-khi) (module_energy_cproj_mrso.f90:517,636). */
 static void oz_pair(const orc *o, const double q[3], cplx *dq_, cplx *dmq_, int q_eq_mq, int nyq_flag, int mix,
                     cplx *outq, cplx *outmq, double *R, cplx *ceff, cplx *drq, cplx *drmq, cplx *gq, cplx *gmq)
 {
@@ -876,7 +876,7 @@ static void project_forward(const orc *o, const double *xi, cplx *drho /* [N][np
 /* S3-S5, every (q, -q) pair once, in the reference's serial order, with oc's c table.
    mix = 0 (module_energy_cproj_mrso.f90:462-665): in place (out == in); the -q result
    replaces the q result at self-conjugate points, conjugated where a Nyquist index is set.
-   mix = 1 (module_energy_cproj_mrso_mixture.f90:478-664): out += the results; at
+   mix = 1 (module_energy_cproj_mrso_mixture.f90:491-721): out += the results; at
    self-conjugate points only the q result is added. */
 static int oz_sweep(const orc *oc, const cplx *in, cplx *out, int mix)
 {
@@ -990,8 +990,8 @@ static int excess(orc *o, const double *xi, double *fexc, double *df)
 /* energy_cproj_mrso_mixture: module_energy_cproj_mrso_mixture.f90:67-850.  sp[s] holds species
    s (its n0 already times its mole fraction, module_solvent.f90:221-222, its c table and
    vext); xi and df are [ns][N][no].  gamma_{s2} = sum_s OZ_{c(s2)}(drho_s), summed in the
-   reference's order (s outer, s2 inner, :483-664), then gathered per s2 with the prefactor
-   -kT 2 (4 pi^2) / mrso / n0(s2) x(s2) (:728-760). */
+   reference's order (s outer, s2 inner, :491-721), then gathered per s2 with the prefactor
+   -kT 2 (4 pi^2) / mrso / n0(s2) x(s2) (:788-809). */
 static int excess_mixture(orc *const *sp, int ns, const double *xfrac, const double *xi, double *fexc, double *df)
 {
     const orc *o = sp[0];

@@ -2,8 +2,8 @@
 reference's algorithm implies, on the CPU.
 
 * mmax 0: the rotations are the identity, so the mixture routine of one species equals the
-  single-species routine exactly (src/module_energy_cproj_mrso_mixture.f90:509-523 against
-  src/module_energy_cproj_mrso.f90:505-523).
+  single-species routine exactly (src/module_energy_cproj_mrso_mixture.f90:541-557 against
+  src/module_energy_cproj_mrso.f90:508-522).
 * mmax >= 1: the two routines differ -- the mixture rotates -q with R(m,mup,khi) where the
   single-species routine uses R(m,mup,-khi) -- and the oracle keeps that difference.
 * Splitting one species into two identical halves (n0 and mole fraction halved, the same c,
