@@ -375,6 +375,31 @@ int mdft_set_warm_net(mdft_handle *h, mdft_warm_net *net);
 /* stats[0]: warm-started solves, stats[1]: of which redone from the bulk guess. */
 int mdft_get_warm_stats(const mdft_handle *h, long long *stats);
 
+/* ---- Bridge term, bridge = "cgb" (src/module_energy_and_gradient.f90:166-175, 246-275) ----
+ *
+ * The coarse-grained bridge of src/module_coarse_grained_gageat_bridge.f90:216-482 (one
+ * species, FP64 handles only): n(r) = sum_io xi^2 rho0 w / n0, n_cg its convolution with a
+ * normalised Gaussian of width sigma on the periodic grid, and F_b = sum kT dv n0 Phi(n_cg)
+ * ('sla') or sum kT dv n0 (n - 1) Phi(n_cg) ('wda', cgb_version) with A3 = 1 - c00/2 and B6.
+ * Once set, every full evaluation of the handle (mdft_energy_and_gradient*, the FP64
+ * minimiser, mdft_solve, the batch) adds F_b to F and its gradient to df, and the stopping
+ * quantities (max|df|, sum w df) include it; F = terms[0] + terms[1] + terms[2] + F_b +
+ * terms[3].  FP32 evaluations (mixed solves) are refused while it is set; mdft_excess_energy
+ * leaves it out, as the reference's excess seam does.  As in the reference, the 'wda'
+ * gradient convolves Phi' before multiplying by (n - 1) (:349-419); it is not the
+ * derivative of that F_b.  version MDFT_BRIDGE_NONE removes the term. */
+#define MDFT_BRIDGE_NONE 0     /* bridge = "no"              */
+#define MDFT_BRIDGE_CGB_SLA 1  /* bridge = "cgb", cgb_version 'sla' (the default) */
+#define MDFT_BRIDGE_CGB_WDA 2  /* bridge = "cgb", cgb_version 'wda' */
+/* B6, sigma: cgb_B6 (default 0) and cgb_sigma (default 1 A); c00: c00_000 (mdft_cgb_c00). */
+int mdft_set_bridge_cgb(mdft_handle *h, int version, double B6, double sigma, double c00);
+/* c00_000 for the reference's solvent names: spce -14.64872 at mmax 0, -13.665 above;
+ * tip3p -11.9078 (:260-263).  Other names: MDFT_E_ARG (the reference leaves it unset). */
+int mdft_cgb_c00(const char *solvent, int mmax, double *c00);
+/* energy_bridge(fb, df) alone: fb, and df (host array, may be NULL) += the bridge
+ * gradient; fb = 0 and df unchanged without a bridge. */
+int mdft_bridge_energy(mdft_handle *h, const double *xi, double *fb, double *df);
+
 /* ---- Multi-species solvent (nb_solvent > 1) ----
  *
  * energy_and_gradient of a solvent of nspec >= 2 species: replaces the excess pointer

@@ -28,6 +28,7 @@
 #include "k_project_tma.cuh"
 #include "k_angular_umma.cuh"
 #include "k_vext.cuh"
+#include "k_bridge.cuh"
 
 namespace mdft {
 
@@ -140,6 +141,12 @@ struct mdft_handle {
     DevBuf<double4> wdir;
     DevBuf<double> wsite;
     long long warm_starts = 0, warm_fallbacks = 0;
+    // bridge = "cgb" (mdft_set_bridge_cgb): 0 none, 1 'sla', 2 'wda'; the transformed kernel,
+    // two work planes, n(r) and the block partials
+    int cgb = 0;
+    CgbArgs cgb_args{};
+    DevBuf<double2> cgb_kk, cgb_a, cgb_b;
+    DevBuf<double> cgb_dens, cgb_part;
 };
 
 namespace {
@@ -436,6 +443,36 @@ GatherArgs gather_args(const mdft_handle *h, int df_mode, int do_ideal, const vo
     return ga;
 }
 
+// batched FFT over planes (defined with the solver, solve.cuh)
+int launch_fft_planes(mdft_handle *h, double2 *data, int nplanes, int sign);
+
+// The bridge term after the pipeline of a full FP64 evaluation: F_b into sums[6]; with d_df,
+// the bridge gradient added to d_df and sums[3..5] recomputed over the final gradient.
+int launch_bridge(mdft_handle *h, const double *d_xi, double *d_df, const double *dvec) {
+    const Grid &g = h->g;
+    const CgbArgs &a = h->cgb_args;
+    const unsigned nb = kRedBlocks;
+    int rc;
+    k_cgb_density<<<nb, kBrThreads, 0, h->stream>>>(d_xi, h->w.p, a, h->cgb_dens.p, h->cgb_a.p);
+    if ((rc = launch_fft_planes(h, h->cgb_a.p, 1, -1))) return rc;
+    k_cgb_cmul<<<nb, kBrThreads, 0, h->stream>>>(h->cgb_a.p, h->cgb_kk.p, g.N);
+    if ((rc = launch_fft_planes(h, h->cgb_a.p, 1, +1))) return rc;
+    k_cgb_phi<<<nb, kBrThreads, 0, h->stream>>>(h->cgb_a.p, h->cgb_dens.p, a, d_df ? 1 : 0, h->cgb_b.p, h->cgb_part.p);
+    h->launches += 4;
+    if (d_df) {
+        if ((rc = launch_fft_planes(h, h->cgb_b.p, 1, -1))) return rc;
+        k_cgb_cmul<<<nb, kBrThreads, 0, h->stream>>>(h->cgb_b.p, h->cgb_kk.p, g.N);
+        if ((rc = launch_fft_planes(h, h->cgb_b.p, 1, +1))) return rc;
+        k_cgb_grad<<<nb, kBrThreads, 0, h->stream>>>(d_xi, h->w.p, a, h->cgb_a.p, h->cgb_b.p, h->cgb_dens.p, d_df, dvec,
+                                                     h->cgb_part.p + kRedBlocks);
+        h->launches += 2;
+    }
+    k_cgb_finish<<<1, kBrThreads, 0, h->stream>>>(h->cgb_part.p, kRedBlocks, h->cgb_part.p + kRedBlocks, d_df ? kRedBlocks : 0,
+                                                  h->sums.p);
+    h->launches += 1;
+    return check_cuda(cudaGetLastError(), "bridge launch");
+}
+
 // S1 on CUDA cores, FP64 point: the bulk-copy projection where it fits and xi is 16-byte
 // aligned, else the tiled one.
 template <typename T>
@@ -488,6 +525,10 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     const double *d_xi = static_cast<const double *>(xin);  // FP64 point unless x32
     const Grid &g = h->g;
     const bool dbl = sizeof(T) == 8;
+    if (h->cgb && do_ideal && (!dbl || vec32 || x32)) {
+        set_error("the bridge term is evaluated in FP64 only (an FP64 handle and FP64 solves)");
+        return MDFT_E_STATE;
+    }
     C *planes = dbl ? (C *)h->planes.p : (C *)h->planes32.p;
     const T *A = dbl ? (const T *)h->A.p : (const T *)h->A32.p;
     const T *B = dbl ? (const T *)h->B.p : (const T *)h->B32.p;
@@ -614,8 +655,11 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
     k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, red_blocks, h->sums.p);
     h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft_t)
+    if ((rc = check_cuda(cudaGetLastError(), "reduce launch"))) return rc;
+    if (h->cgb && do_ideal && (rc = launch_bridge(h, d_xi, ga.df_mode == 1 ? d_df : nullptr, static_cast<const double *>(dvec))))
+        return rc;
     stage_mark(h, 5);
-    return check_cuda(cudaGetLastError(), "reduce launch");
+    return MDFT_OK;
 }
 
 // dvec (df_mode 1 only): h_sums[3] = df.dvec, h_sums[4] = max|df| after finish_sums.
@@ -676,7 +720,8 @@ int run_pipeline(mdft_handle *h, const void *d_xi, double *d_df, int do_ideal, i
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
-    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, kGatherSums * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
+    // {F_id, F_ext, sum_exc, df.dvec, max|df|, sum w df, F_b}
+    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, (kGatherSums + 1) * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
     if (rc) return rc;
     if ((rc = check_cuda(cudaMemcpyAsync(h->h_kerr, h->kerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "flag copy"))) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "evaluation"))) return rc;
@@ -708,7 +753,7 @@ double combine(const mdft_handle *h, double fid, double fext, double fexc) {
     double f = 0.0;
     f = f + fid + fext;
     f = f + fexc;
-    f = f + 0.0;  // bridge "no"
+    f = f + (h->cgb ? h->h_sums[6] : 0.0);  // bridge: F_b of this evaluation ("no": 0)
     f = f + h->const_corr;
     return f;
 }
@@ -914,6 +959,7 @@ int mdft_create(const mdft_desc *d, mdft_handle **out) {
     cudaMemset(h->kerr.p, 0, sizeof(int));
     if ((rc = check_cuda(cudaMallocHost(&h->h_kerr, sizeof(int)), "pinned flag"))) return rc;
     if ((rc = alloc_check(h->sums.alloc(8), "sums", 64))) return rc;
+    cudaMemset(h->sums.p, 0, 8 * sizeof(double));
     if ((rc = check_cuda(cudaMallocHost(&h->h_sums, 8 * sizeof(double)), "pinned sums"))) return rc;
     if ((rc = alloc_check(h->vpart.alloc((size_t)kMaxRows * kRedBlocks), "reduction partials", 8 * kMaxRows * kRedBlocks))) return rc;
     if ((rc = alloc_check(h->vsc.alloc(kScalarSlots), "reduction scalars", 8 * kScalarSlots))) return rc;
@@ -1051,6 +1097,89 @@ int mdft_get_vext(const mdft_handle *h, double *v) {
 int mdft_set_constant_correction(mdft_handle *h, double c) {
     if (!h) { set_error("null argument"); return MDFT_E_ARG; }
     h->const_corr = c;
+    return MDFT_OK;
+}
+
+// c00_000 by solvent(1)%name and grid%mmax (src/module_coarse_grained_gageat_bridge.f90:260-263)
+int mdft_cgb_c00(const char *solvent, int mmax, double *c00) {
+    if (!solvent || !c00) { set_error("null argument"); return MDFT_E_ARG; }
+    if (std::strcmp(solvent, "spce") == 0) *c00 = mmax == 0 ? -14.64872 : -13.665;
+    else if (std::strcmp(solvent, "tip3p") == 0) *c00 = -11.9078;
+    else {
+        set_error("no c00_000 for solvent '%s' (the reference has values for spce and tip3p only)", solvent);
+        return MDFT_E_ARG;
+    }
+    return MDFT_OK;
+}
+
+int mdft_set_bridge_cgb(mdft_handle *h, int version, double B6, double sigma, double c00) {
+    if (!h) { set_error("null argument"); return MDFT_E_ARG; }
+    if (version < MDFT_BRIDGE_NONE || version > MDFT_BRIDGE_CGB_WDA) { set_error("unknown cgb version %d", version); return MDFT_E_ARG; }
+    if (version != MDFT_BRIDGE_NONE && h->precision != MDFT_PREC_FP64) {
+        set_error("the bridge term needs an FP64 handle");
+        return MDFT_E_ARG;
+    }
+    if (version != MDFT_BRIDGE_NONE && !(sigma > 0.0 && std::isfinite(sigma) && std::isfinite(B6) && std::isfinite(c00))) {
+        set_error("cgb parameters must be finite, sigma > 0");
+        return MDFT_E_ARG;
+    }
+    drop_pipe_graphs(h);  // the captured pipelines carry the bridge's launches
+    int rc;
+    if (version == MDFT_BRIDGE_NONE) {
+        h->cgb = 0;
+        h->cgb_kk.free(); h->cgb_a.free(); h->cgb_b.free(); h->cgb_dens.free(); h->cgb_part.free();
+        return check_cuda(cudaMemsetAsync(h->sums.p + 6, 0, sizeof(double), h->stream), "sums reset");
+    }
+    const Grid &g = h->g;
+    if (!h->cgb_kk.p) {
+        if ((rc = alloc_check(h->cgb_kk.alloc(g.N), "bridge kernel", g.N * 16))) return rc;
+        if ((rc = alloc_check(h->cgb_a.alloc(g.N), "bridge plane", g.N * 16))) return rc;
+        if ((rc = alloc_check(h->cgb_b.alloc(g.N), "bridge plane", g.N * 16))) return rc;
+        if ((rc = alloc_check(h->cgb_dens.alloc(g.N), "bridge density", g.N * 8))) return rc;
+        if ((rc = alloc_check(h->cgb_part.alloc(4 * kRedBlocks), "bridge partials", 32 * kRedBlocks))) return rc;
+    }
+    // fill_kernel (src/module_coarse_grained_gageat_bridge.f90:123-210)
+    const double pi = std::acos(-1.0);
+    const double sp = sigma * std::sqrt(2.0 * pi);
+    const double gp = 1.0 / (sp * sp * sp), oo = 1.0 / (2.0 * sigma * sigma);
+    const double cut = -1.0 / oo * std::log(1.0e-10 / gp);
+    const double nf = (double)(float)(g.nx * g.ny * g.nz);  // real(nx*ny*nz): single precision
+    k_cgb_kernel<<<kRedBlocks, kBrThreads, 0, h->stream>>>(h->cgb_kk.p, g.nx, g.ny, g.nz, g.lx / g.nx, g.ly / g.ny, g.lz / g.nz,
+                                                           gp, oo, cut);
+    if ((rc = launch_fft_planes(h, h->cgb_kk.p, 1, -1))) return rc;
+    k_cgb_scale<<<kRedBlocks, kBrThreads, 0, h->stream>>>(h->cgb_kk.p, g.N, nf, g.lx * g.ly * g.lz);
+    h->launches += 2;
+    if ((rc = check_cuda(cudaGetLastError(), "bridge kernel"))) return rc;
+    CgbArgs &a = h->cgb_args;
+    a.N = g.N;
+    a.no = g.no;
+    a.version = version;
+    a.rho0 = g.rho0;
+    a.n0 = g.n0;
+    a.kT = g.kT;
+    a.vvox = (g.lx / g.nx) * (g.ly / g.ny) * (g.lz / g.nz);
+    a.nf = nf;
+    a.A3 = 1.0 - c00 / 2.0;
+    a.B6 = B6;
+    h->cgb = version;
+    return check_cuda(cudaStreamSynchronize(h->stream), "bridge set-up");
+}
+
+int mdft_bridge_energy(mdft_handle *h, const double *xi, double *fb, double *df) {
+    if (!h || !xi || !fb) { set_error("null argument"); return MDFT_E_ARG; }
+    *fb = 0.0;
+    if (!h->cgb) return MDFT_OK;  // bridge "no"
+    const size_t n = (size_t)h->g.N * h->g.no;
+    int rc = check_cuda(cudaMemcpyAsync(h->xi.p, xi, n * 8, cudaMemcpyHostToDevice, h->stream), "xi upload");
+    if (rc) return rc;
+    if (df && (rc = check_cuda(cudaMemcpyAsync(h->df.p, df, n * 8, cudaMemcpyHostToDevice, h->stream), "df upload"))) return rc;
+    if ((rc = launch_bridge(h, h->xi.p, df ? h->df.p : nullptr, nullptr))) return rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(h->h_sums + 6, h->sums.p + 6, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy")))
+        return rc;
+    if (df && (rc = check_cuda(cudaMemcpyAsync(df, h->df.p, n * 8, cudaMemcpyDeviceToHost, h->stream), "df download"))) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "bridge"))) return rc;
+    *fb = h->h_sums[6];
+    if (!std::isfinite(*fb)) { set_error("non-finite bridge energy"); return MDFT_E_NUMERIC; }
     return MDFT_OK;
 }
 

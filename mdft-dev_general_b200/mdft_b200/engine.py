@@ -142,6 +142,10 @@ SIGNATURES = {
     "mdft_warm_expand_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "mdft_set_warm_net": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mdft_get_warm_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    # bridge term
+    "mdft_set_bridge_cgb": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]),
+    "mdft_cgb_c00": (C.c_int, [C.c_char_p, C.c_int, _DP]),
+    "mdft_bridge_energy": (C.c_int, [C.c_void_p, _DP, _DP, _DP]),
     # multi-species solvent
     "mdft_mixture_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, _DP, C.POINTER(C.c_void_p)]),
     "mdft_mixture_destroy": (C.c_int, [C.c_void_p]),
@@ -281,6 +285,24 @@ class Engine:
                                        _p(ve), _p(vx), float(rvdw), _p(lj)))
         self.lj_tail = float(lj[0])
         return self.lj_tail
+
+    def set_bridge_cgb(self, version, B6=0.0, sigma=1.0, c00=None, solvent="spce", mmax=None):
+        """bridge = "cgb": version 1 'sla', 2 'wda', 0 removes it.  c00 defaults to the
+        reference's value for `solvent` at this handle's mmax."""
+        if c00 is None and version:
+            v = np.zeros(1)
+            _check(lib().mdft_cgb_c00(solvent.encode(), int(self.sizes.ntheta - 1 if mmax is None else mmax), _p(v)))
+            c00 = float(v[0])
+        _check(lib().mdft_set_bridge_cgb(self.h, int(version), float(B6), float(sigma), float(c00 or 0.0)))
+
+    def bridge_energy(self, xi, df=None):
+        """energy_bridge(fb, df): returns F_b; adds the bridge gradient to df (in place) when given."""
+        x = np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        fb = np.zeros(1)
+        if df is not None and not (df.flags.c_contiguous and df.dtype == np.float64 and df.size == x.size):
+            raise MdftError("df must be a contiguous float64 array of xi's size")
+        _check(lib().mdft_bridge_energy(self.h, _p(x), _p(fb), _p(df)))
+        return float(fb[0])
 
     def guess_density(self):
         xi = np.empty(self.shape)

@@ -371,6 +371,9 @@ typedef struct orc {
     cplx *c; /* [nq][ncoef] */
     double *vext; /* [N][no], owned */
     double const_corr; /* charged-solute corrections added to F (constant in xi) */
+    /* bridge = "cgb" (0: none, 1: 'sla', 2: 'wda') and its parameters */
+    int cgb;
+    double cgb_B6, cgb_sigma, cgb_c00;
     cplx *drho; /* [N][np] */
 } orc;
 
@@ -1048,16 +1051,19 @@ static void ideal_and_external(const orc *o, const double *xi, double *fid, doub
 
 /* energy_and_gradient: module_energy_and_gradient.f90:36-240.               */
 /* terms = {F_id, F_ext, F_exc, corrections}                                  */
+static int bridge_cgb(const orc *o, const double *xi, double *fb, double *df);
+
 int orc_energy_grad(orc *o, const double *xi, double *f, double *df, double *terms)
 {
     if (df) memset(df, 0, sizeof(double) * o->N * o->no);
-    double fid, fext, fexc;
+    double fid, fext, fexc, fb = 0.0;
     ideal_and_external(o, xi, &fid, &fext, df);
     if (excess(o, xi, &fexc, df)) return -1;
+    if (o->cgb && bridge_cgb(o, xi, &fb, df)) return -1; /* energy_bridge :166-175, :246-275 */
     double ff = 0.0;
     ff = ff + fid + fext;
     ff = ff + fexc;
-    ff = ff + 0.0; /* bridge "no" */
+    ff = ff + fb;
     ff = ff + o->const_corr;
     *f = ff;
     if (terms) { terms[0] = fid; terms[1] = fext; terms[2] = fexc; terms[3] = o->const_corr; }
@@ -1104,6 +1110,133 @@ int orc_mixture_energy_grad(orc *const *sp, int ns, const double *xfrac, const d
     *f = ff;
     if (terms) { terms[0] = fid; terms[1] = fext; terms[2] = fexc; terms[3] = o->const_corr; }
     return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Coarse-grained bridge, bridge = "cgb":                                     */
+/* module_coarse_grained_gageat_bridge.f90:50-482 (one species).             */
+
+/* fill_kernel (:123-210): the normalised Gaussian of width sigma on the periodic grid,
+   cut where it falls below 1e-10, forward transformed (r2c, sign -1) and scaled by
+   V / real(N) -- `real(nx*ny*nz)` is single precision. */
+static void cgb_kernel_k(const orc *o, double sigma, cplx *kk)
+{
+    const double pi = acos(-1.0);
+    const double sp = sigma * sqrt(2.0 * pi);
+    const double gp = 1.0 / (sp * sp * sp);
+    const double oo = 1.0 / (2.0 * sigma * sigma);
+    const double cut = -1.0 / oo * log(1.0e-10 / gp);
+    const int nx = o->nx, ny = o->ny, nz = o->nz;
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                const double xp = o->dx * (ix < nx - ix ? ix : nx - ix);
+                const double yp = o->dy * (iy < ny - iy ? iy : ny - iy);
+                const double zp = o->dz * (iz < nz - iz ? iz : nz - iz);
+                const double d2 = xp * xp + yp * yp + zp * zp;
+                kk[((long)iz * ny + iy) * nx + ix] = d2 < cut ? gp * exp(-d2 * oo) : 0.0;
+            }
+    fft3d(kk, nx, ny, nz, -1);
+    const double nf = (double)(float)(nx * ny * nz), vol = o->lx * o->ly * o->lz;
+    for (long r = 0; r < o->N; ++r) kk[r] = kk[r] / nf * vol;
+}
+
+/* out = c2r(r2c(in) * kernel_k) / real(N) (:424-451), as a complex FFT of real data. */
+static void cgb_convolve(const orc *o, const cplx *kk, const double *in, double *out, cplx *buf)
+{
+    for (long r = 0; r < o->N; ++r) buf[r] = in[r];
+    fft3d(buf, o->nx, o->ny, o->nz, -1);
+    for (long r = 0; r < o->N; ++r) buf[r] *= kk[r];
+    fft3d(buf, o->nx, o->ny, o->nz, +1);
+    const double nf = (double)(float)(o->nx * o->ny * o->nz);
+    for (long r = 0; r < o->N; ++r) out[r] = creal(buf[r]) / nf;
+}
+
+/* coarse_grained_bridge (:216-421); df (may be NULL) accumulates 2 xi rho0 dfb w (:455-482). */
+static int bridge_cgb(const orc *o, const double *xi, double *fb_out, double *df)
+{
+    const long N = o->N;
+    const int no = o->no;
+    const double kT = o->kT, n0 = o->n0, rho0 = o->rho0;
+    const double vvox = o->dx * o->dy * o->dz, facteur = kT * vvox;
+    const double A3 = 1.0 - o->cgb_c00 / 2.0, B6 = o->cgb_B6;
+    cplx *kk = malloc(sizeof(cplx) * N), *buf = malloc(sizeof(cplx) * N);
+    double *dens = calloc(N, sizeof(double)), *dcg = calloc(N, sizeof(double));
+    double *t = calloc(N, sizeof(double)), *dfb = calloc(N, sizeof(double));
+    if (!kk || !buf || !dens || !dcg || !t || !dfb) {
+        free(kk); free(buf); free(dens); free(dcg); free(t); free(dfb);
+        set_err("out of memory");
+        return -1;
+    }
+    cgb_kernel_k(o, o->cgb_sigma, kk);
+    /* integrate_over_orientations(xi**2 * rho0) / n0 (module_grid.f90:354-380) */
+    for (long r = 0; r < N; ++r) {
+        double a = 0.0;
+        for (int io = 0; io < no; ++io) {
+            const double x = xi[r * no + io];
+            a += x * x * rho0 * o->w[io];
+        }
+        dens[r] = a / n0;
+    }
+    cgb_convolve(o, kk, dens, dcg, buf);
+    double fb = 0.0;
+    if (o->cgb == 1) { /* 'sla' (:274-347) */
+        for (long r = 0; r < N; ++r) {
+            const double ncg = dcg[r], dn = ncg - 1.0;
+            double phib, d;
+            if (ncg < 1.0) {
+                phib = A3 * (dn * dn * dn) + B6 * (ncg * ncg) * ((dn * dn) * (dn * dn));
+                d = kT * A3 * 3.0 * (dn * dn) + kT * B6 * (2.0 * ncg * ((dn * dn) * (dn * dn)) + 4.0 * (ncg * ncg) * (dn * dn * dn));
+            } else {
+                phib = A3 * (dn * dn * dn);
+                d = kT * A3 * 3.0 * (dn * dn);
+            }
+            fb = fb + facteur * n0 * phib;
+            t[r] = d;
+        }
+        if (df) cgb_convolve(o, kk, t, dfb, buf);
+    } else { /* 'wda' (:349-419) */
+        if (df) {
+            for (long r = 0; r < N; ++r) {
+                const double ncg = dcg[r], dn = ncg - 1.0;
+                t[r] = ncg < 1.0 ? A3 * 2.0 * dn + B6 * (2.0 * ncg * (dn * dn * dn) + 3.0 * (ncg * ncg) * (dn * dn))
+                                 : A3 * 2.0 * dn;
+            }
+            cgb_convolve(o, kk, t, dfb, buf);
+        }
+        for (long r = 0; r < N; ++r) {
+            const double ncg = dcg[r], dN = dens[r] - 1.0, dn = ncg - 1.0;
+            const double phib = ncg < 1.0 ? A3 * (dn * dn) + B6 * (ncg * ncg) * (dn * dn * dn) : A3 * (dn * dn);
+            fb = fb + kT * vvox * n0 * dN * phib;
+            if (df) t[r] = kT * (dN * dfb[r] + phib);
+        }
+        if (df) memcpy(dfb, t, sizeof(double) * N);
+    }
+    if (df)
+        for (long r = 0; r < N; ++r)
+            for (int io = 0; io < no; ++io) df[r * no + io] = df[r * no + io] + 2.0 * xi[r * no + io] * rho0 * dfb[r] * o->w[io];
+    free(kk); free(buf); free(dens); free(dcg); free(t); free(dfb);
+    *fb_out = fb;
+    return 0;
+}
+
+/* version 0 removes the bridge (bridge = "no"), 1 'sla', 2 'wda' (cgb_version, :72). */
+int orc_set_bridge_cgb(orc *o, int version, double B6, double sigma, double c00)
+{
+    if (version < 0 || version > 2 || !(sigma > 0.0)) { set_err("bad cgb parameters"); return -1; }
+    o->cgb = version;
+    o->cgb_B6 = B6;
+    o->cgb_sigma = sigma;
+    o->cgb_c00 = c00;
+    return 0;
+}
+
+/* energy_bridge(fb, df) alone: fb and df += the bridge's gradient (df may be NULL). */
+int orc_bridge_energy(orc *o, const double *xi, double *fb, double *df)
+{
+    *fb = 0.0;
+    if (!o->cgb) return 0;
+    return bridge_cgb(o, xi, fb, df);
 }
 
 /* Charged-solute corrections: module_energy_and_gradient.f90:281-344.        */

@@ -63,6 +63,8 @@ def lib():
         L.orc_set_quirks.argtypes = [C.c_int]
         L.orc_pressure_correction.argtypes = [C.c_void_p, dp, C.c_double, C.c_double, dp]
         L.orc_mixture_energy_grad.argtypes = [C.POINTER(C.c_void_p), C.c_int, dp, dp, dp, dp, dp]
+        L.orc_set_bridge_cgb.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.orc_bridge_energy.argtypes = [C.c_void_p, dp, dp, dp]
     return _LIB
 
 
@@ -174,6 +176,21 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(lib().orc_last_error().decode())
         return float(f[0]), df, terms
+
+    def set_bridge_cgb(self, version, B6=0.0, sigma=1.0, c00=-13.665):
+        """bridge = "cgb": version 0 none, 1 'sla', 2 'wda'; c00 the solvent's c(k=0)."""
+        if lib().orc_set_bridge_cgb(self.h, version, B6, sigma, c00) != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def bridge_energy(self, xi, df=None):
+        """energy_bridge(fb, df): returns fb; adds the bridge gradient to df when given."""
+        xi = np.ascontiguousarray(xi, dtype=np.float64).reshape(self.shape)
+        fb = np.zeros(1)
+        if df is not None:
+            assert df.flags.c_contiguous and df.dtype == np.float64
+        if lib().orc_bridge_energy(self.h, _p(xi), _p(fb), _p(df) if df is not None else None) != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return float(fb[0])
 
     def angl2proj(self, o):
         o = np.ascontiguousarray(o, dtype=np.float64)

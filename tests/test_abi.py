@@ -105,3 +105,23 @@ def test_ck_table_checks_without_gpu(tmp_path):
     d = engine._Desc(16, 16, 16, 8.0, 8.0, 8.0, 1, 2, 298.0, 0.0333, bad.encode(), 0, 0)
     assert L.mdft_create(ctypes.byref(d), ctypes.byref(h)) == -2
     assert b"uniform" in L.mdft_last_error()
+
+
+def test_bridge_and_mixture_host_checks_without_gpu():
+    L = engine.lib()
+    v = ctypes.c_double()
+    # c00_000 of src/module_coarse_grained_gageat_bridge.f90:260-263
+    assert L.mdft_cgb_c00(b"spce", 0, ctypes.byref(v)) == 0 and v.value == -14.64872
+    assert L.mdft_cgb_c00(b"spce", 3, ctypes.byref(v)) == 0 and v.value == -13.665
+    assert L.mdft_cgb_c00(b"tip3p", 1, ctypes.byref(v)) == 0 and v.value == -11.9078
+    assert L.mdft_cgb_c00(b"acetonitrile", 1, ctypes.byref(v)) == -1
+    assert b"acetonitrile" in L.mdft_last_error()
+    assert L.mdft_set_bridge_cgb(None, 1, 0.0, 1.0, -13.665) == -1
+    m = ctypes.c_void_p()
+    x = (ctypes.c_double * 2)(0.5, 0.5)
+    hs = (ctypes.c_void_p * 2)(None, None)
+    assert L.mdft_mixture_create(hs, 1, x, ctypes.byref(m)) == -1
+    assert b"at least two" in L.mdft_last_error()
+    assert L.mdft_mixture_create(hs, 2, x, ctypes.byref(m)) == -1
+    assert b"null species" in L.mdft_last_error()
+    assert L.mdft_mixture_destroy(None) == 0
