@@ -387,7 +387,7 @@ int mdft_get_warm_stats(const mdft_handle *h, long long *stats);
  * terms[3].  FP32 evaluations (mixed solves) are refused while it is set; mdft_excess_energy
  * leaves it out, as the reference's excess seam does.  As in the reference, the 'wda'
  * gradient convolves Phi' before multiplying by (n - 1) (:349-419); it is not the
- * derivative of that F_b.  version MDFT_BRIDGE_NONE removes the term. */
+ * derivative of that F_b.  version MDFT_BRIDGE_NONE removes any bridge term. */
 #define MDFT_BRIDGE_NONE 0     /* bridge = "no"              */
 #define MDFT_BRIDGE_CGB_SLA 1  /* bridge = "cgb", cgb_version 'sla' (the default) */
 #define MDFT_BRIDGE_CGB_WDA 2  /* bridge = "cgb", cgb_version 'wda' */
@@ -396,6 +396,21 @@ int mdft_set_bridge_cgb(mdft_handle *h, int version, double B6, double sigma, do
 /* c00_000 for the reference's solvent names: spce -14.64872 at mmax 0, -13.665 above;
  * tip3p -11.9078 (:260-263).  Other names: MDFT_E_ARG (the reference leaves it unset). */
 int mdft_cgb_c00(const char *solvent, int mmax, double *c00);
+/* bridge = "hard_sphere" (src/module_fmt.f90:5-317, one species, FP64 handles only): the
+ * Kierlik-Rosinberg FMT functional (PY or CS, hs_functional) of the orientation-summed
+ * density with hard spheres of radius R (hs_radius), minus the bulk excess chemical
+ * potential and grand potential (src/module_hardspheres.f90:83-189) and minus the quadratic
+ * part of the hard-sphere c(k) (src/cs_of_k_hard_sphere.f90, tabulated on the c(k) file's
+ * step).  It enters evaluations as the "cgb" term does; setting one bridge replaces the
+ * other.  An empty box (every |xi| <= epsilon) gives F_b = -Fexc0 and no gradient
+ * (:46-49).  A weighted density n3 outside (0, 1) fails the evaluation with MDFT_E_NUMERIC
+ * (the reference stops).  The reference computes the bulk parameters only with a
+ * hard-sphere solute (src/compute_vext_hard_sphere.f90:46-53); here they are computed at set. */
+#define MDFT_BRIDGE_HS_PY 1  /* hs_functional PY */
+#define MDFT_BRIDGE_HS_CS 2  /* hs_functional CS */
+int mdft_set_bridge_fmt(mdft_handle *h, int functional, double radius);
+/* out[4] = {radius, excess chemical potential mu_exc0, bulk grand potential Fexc0, nb_k}. */
+int mdft_get_bridge_fmt_params(const mdft_handle *h, double *out);
 /* energy_bridge(fb, df) alone: fb, and df (host array, may be NULL) += the bridge
  * gradient; fb = 0 and df unchanged without a bridge. */
 int mdft_bridge_energy(mdft_handle *h, const double *xi, double *fb, double *df);

@@ -147,7 +147,17 @@ struct mdft_handle {
     CgbArgs cgb_args{};
     DevBuf<double2> cgb_kk, cgb_a, cgb_b;
     DevBuf<double> cgb_dens, cgb_part;
+    // bridge = "hard_sphere" (mdft_set_bridge_fmt): 0 none, 1 PY, 2 CS; seven work planes,
+    // the hard-sphere c(k) and the partials {density 2B | stats 2 | Phi 4B | gradient 4B}
+    int fmt = 0;
+    FmtArgs fmt_args{};
+    DevBuf<double2> fmt_pl;
+    DevBuf<double> fmt_cs, fmt_part;
 };
+
+namespace {
+bool has_bridge(const mdft_handle *h) { return h->cgb || h->fmt; }
+}
 
 namespace {
 
@@ -448,7 +458,34 @@ int launch_fft_planes(mdft_handle *h, double2 *data, int nplanes, int sign);
 
 // The bridge term after the pipeline of a full FP64 evaluation: F_b into sums[6]; with d_df,
 // the bridge gradient added to d_df and sums[3..5] recomputed over the final gradient.
+int launch_fmt(mdft_handle *h, const double *d_xi, double *d_df, const double *dvec) {
+    const FmtArgs &a = h->fmt_args;
+    const unsigned nb = kRedBlocks;
+    const long long N = h->g.N;
+    double2 *pl = h->fmt_pl.p;
+    double *pd = h->fmt_part.p, *stats = pd + 2 * nb, *pphi = stats + 2, *pgr = pphi + 4 * nb;
+    int rc;
+    k_fmt_density<<<nb, kBrThreads, 0, h->stream>>>(d_xi, h->w.p, a, pl, pd);
+    k_fmt_stats<<<1, kBrThreads, 0, h->stream>>>(pd, (int)nb, stats);
+    if ((rc = launch_fft_planes(h, pl, 2, -1))) return rc;
+    k_fmt_weigh<<<nb, kBrThreads, 0, h->stream>>>(pl, h->fmt_cs.p, a);
+    if ((rc = launch_fft_planes(h, pl + N, 5, +1))) return rc;
+    k_fmt_phi<<<nb, kBrThreads, 0, h->stream>>>(pl, a, d_df ? 1 : 0, pphi);
+    h->launches += 4;
+    if (d_df) {
+        if ((rc = launch_fft_planes(h, pl + 2 * N, 4, -1))) return rc;
+        k_fmt_combine<<<nb, kBrThreads, 0, h->stream>>>(pl, a);
+        if ((rc = launch_fft_planes(h, pl + 6 * N, 1, +1))) return rc;
+        h->launches += 1;
+    }
+    k_fmt_grad<<<nb, kBrThreads, 0, h->stream>>>(d_xi, h->w.p, a, pl, stats, d_df, dvec, pgr);
+    k_fmt_finish<<<1, kBrThreads, 0, h->stream>>>(pphi, pgr, (int)nb, stats, a, d_df ? 1 : 0, h->sums.p);
+    h->launches += 2;
+    return check_cuda(cudaGetLastError(), "bridge launch");
+}
+
 int launch_bridge(mdft_handle *h, const double *d_xi, double *d_df, const double *dvec) {
+    if (h->fmt) return launch_fmt(h, d_xi, d_df, dvec);
     const Grid &g = h->g;
     const CgbArgs &a = h->cgb_args;
     const unsigned nb = kRedBlocks;
@@ -525,7 +562,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     const double *d_xi = static_cast<const double *>(xin);  // FP64 point unless x32
     const Grid &g = h->g;
     const bool dbl = sizeof(T) == 8;
-    if (h->cgb && do_ideal && (!dbl || vec32 || x32)) {
+    if (has_bridge(h) && do_ideal && (!dbl || vec32 || x32)) {
         set_error("the bridge term is evaluated in FP64 only (an FP64 handle and FP64 solves)");
         return MDFT_E_STATE;
     }
@@ -656,7 +693,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
     k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, red_blocks, h->sums.p);
     h->launches += 4;  // project, oz, gather, reduce (the FFT launches are counted in launch_fft_t)
     if ((rc = check_cuda(cudaGetLastError(), "reduce launch"))) return rc;
-    if (h->cgb && do_ideal && (rc = launch_bridge(h, d_xi, ga.df_mode == 1 ? d_df : nullptr, static_cast<const double *>(dvec))))
+    if (has_bridge(h) && do_ideal && (rc = launch_bridge(h, d_xi, ga.df_mode == 1 ? d_df : nullptr, static_cast<const double *>(dvec))))
         return rc;
     stage_mark(h, 5);
     return MDFT_OK;
@@ -720,8 +757,8 @@ int run_pipeline(mdft_handle *h, const void *d_xi, double *d_df, int do_ideal, i
 }
 
 int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
-    // {F_id, F_ext, sum_exc, df.dvec, max|df|, sum w df, F_b}
-    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, (kGatherSums + 1) * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
+    // {F_id, F_ext, sum_exc, df.dvec, max|df|, sum w df, F_b, bridge error}
+    int rc = check_cuda(cudaMemcpyAsync(h->h_sums, h->sums.p, (kGatherSums + 2) * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy");
     if (rc) return rc;
     if ((rc = check_cuda(cudaMemcpyAsync(h->h_kerr, h->kerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "flag copy"))) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "evaluation"))) return rc;
@@ -729,6 +766,14 @@ int finish_sums(mdft_handle *h, double *fid, double *fext, double *fexc) {
         cudaMemsetAsync(h->kerr.p, 0, sizeof(int), h->stream);
         set_error("a pipeline wait in the projection or gather timed out (bulk copy never completed)");
         return MDFT_E_CUDA;
+    }
+    if (h->fmt && h->h_sums[7] != 0.0) {
+        const int code = (int)h->h_sums[7];
+        cudaMemsetAsync(h->sums.p + 7, 0, sizeof(double), h->stream);
+        set_error(code == 1 ? "hard-sphere bridge: a weighted density n3 >= 1 (log(1 - n3) undefined)"
+                  : code == 2 ? "hard-sphere bridge (CS): a weighted density n3 <= 0"
+                              : "hard-sphere bridge: 1 - n3 or n3 at zero in the gradient");
+        return MDFT_E_NUMERIC;
     }
     if (h->timing) {
         for (int i = 0; i < ST_COUNT; ++i) {
@@ -753,7 +798,7 @@ double combine(const mdft_handle *h, double fid, double fext, double fexc) {
     double f = 0.0;
     f = f + fid + fext;
     f = f + fexc;
-    f = f + (h->cgb ? h->h_sums[6] : 0.0);  // bridge: F_b of this evaluation ("no": 0)
+    f = f + (has_bridge(h) ? h->h_sums[6] : 0.0);  // bridge: F_b of this evaluation ("no": 0)
     f = f + h->const_corr;
     return f;
 }
@@ -1112,6 +1157,22 @@ int mdft_cgb_c00(const char *solvent, int mmax, double *c00) {
     return MDFT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// bridge = "no": drop both terms and their buffers
+int clear_bridges(mdft_handle *h) {
+    drop_pipe_graphs(h);  // the captured pipelines carry the bridge's launches
+    h->cgb = 0;
+    h->fmt = 0;
+    h->cgb_kk.free(); h->cgb_a.free(); h->cgb_b.free(); h->cgb_dens.free(); h->cgb_part.free();
+    h->fmt_pl.free(); h->fmt_cs.free(); h->fmt_part.free();
+    return check_cuda(cudaMemsetAsync(h->sums.p + 6, 0, 2 * sizeof(double), h->stream), "sums reset");
+}
+}  // namespace
+
+extern "C" {
+
 int mdft_set_bridge_cgb(mdft_handle *h, int version, double B6, double sigma, double c00) {
     if (!h) { set_error("null argument"); return MDFT_E_ARG; }
     if (version < MDFT_BRIDGE_NONE || version > MDFT_BRIDGE_CGB_WDA) { set_error("unknown cgb version %d", version); return MDFT_E_ARG; }
@@ -1123,21 +1184,14 @@ int mdft_set_bridge_cgb(mdft_handle *h, int version, double B6, double sigma, do
         set_error("cgb parameters must be finite, sigma > 0");
         return MDFT_E_ARG;
     }
-    drop_pipe_graphs(h);  // the captured pipelines carry the bridge's launches
-    int rc;
-    if (version == MDFT_BRIDGE_NONE) {
-        h->cgb = 0;
-        h->cgb_kk.free(); h->cgb_a.free(); h->cgb_b.free(); h->cgb_dens.free(); h->cgb_part.free();
-        return check_cuda(cudaMemsetAsync(h->sums.p + 6, 0, sizeof(double), h->stream), "sums reset");
-    }
+    int rc = clear_bridges(h);
+    if (rc || version == MDFT_BRIDGE_NONE) return rc;
     const Grid &g = h->g;
-    if (!h->cgb_kk.p) {
-        if ((rc = alloc_check(h->cgb_kk.alloc(g.N), "bridge kernel", g.N * 16))) return rc;
-        if ((rc = alloc_check(h->cgb_a.alloc(g.N), "bridge plane", g.N * 16))) return rc;
-        if ((rc = alloc_check(h->cgb_b.alloc(g.N), "bridge plane", g.N * 16))) return rc;
-        if ((rc = alloc_check(h->cgb_dens.alloc(g.N), "bridge density", g.N * 8))) return rc;
-        if ((rc = alloc_check(h->cgb_part.alloc(4 * kRedBlocks), "bridge partials", 32 * kRedBlocks))) return rc;
-    }
+    if ((rc = alloc_check(h->cgb_kk.alloc(g.N), "bridge kernel", g.N * 16))) return rc;
+    if ((rc = alloc_check(h->cgb_a.alloc(g.N), "bridge plane", g.N * 16))) return rc;
+    if ((rc = alloc_check(h->cgb_b.alloc(g.N), "bridge plane", g.N * 16))) return rc;
+    if ((rc = alloc_check(h->cgb_dens.alloc(g.N), "bridge density", g.N * 8))) return rc;
+    if ((rc = alloc_check(h->cgb_part.alloc(4 * kRedBlocks), "bridge partials", 32 * kRedBlocks))) return rc;
     // fill_kernel (src/module_coarse_grained_gageat_bridge.f90:123-210)
     const double pi = std::acos(-1.0);
     const double sp = sigma * std::sqrt(2.0 * pi);
@@ -1165,19 +1219,155 @@ int mdft_set_bridge_cgb(mdft_handle *h, int version, double B6, double sigma, do
     return check_cuda(cudaStreamSynchronize(h->stream), "bridge set-up");
 }
 
+// The bulk hard-sphere parameters (src/module_hardspheres.f90:83-189) and the hard-sphere
+// c(k) (src/cs_of_k_hard_sphere.f90:56-157) on nb_k points of the c(k) file's step.
+int mdft_set_bridge_fmt(mdft_handle *h, int functional, double R) {
+    if (!h) { set_error("null argument"); return MDFT_E_ARG; }
+    if (functional < MDFT_BRIDGE_NONE || functional > MDFT_BRIDGE_HS_CS) { set_error("unknown hard-sphere functional %d", functional); return MDFT_E_ARG; }
+    if (functional != MDFT_BRIDGE_NONE && h->precision != MDFT_PREC_FP64) {
+        set_error("the bridge term needs an FP64 handle");
+        return MDFT_E_ARG;
+    }
+    if (functional != MDFT_BRIDGE_NONE && !(R > 0.0 && std::isfinite(R))) { set_error("the hard-sphere radius must be positive"); return MDFT_E_ARG; }
+    int rc = clear_bridges(h);
+    if (rc || functional == MDFT_BRIDGE_NONE) return rc;
+    const Grid &g = h->g;
+    const double pi = kPi, kT = g.kT, n0 = g.n0;
+    const double pf = (double)(4.0f / 3.0f) * pi * n0 * (R * R * R);  // fourthird = 4./3. (single)
+    if (pf >= 0.74) { set_error("hard-sphere packing fraction %g is above 0.74", pf); return MDFT_E_ARG; }
+    // excess chemical potential and bulk grand potential
+    const double b1 = n0 * R, b2 = n0 * 4 * pi * (R * R), b3 = n0 * 4 * pi * (R * R * R) / 3;
+    double dp[4];
+    dp[0] = -std::log(1 - b3);
+    dp[1] = b2 / (1 - b3);
+    if (functional == MDFT_BRIDGE_HS_PY) {
+        dp[2] = b1 / (1 - b3) + (b2 * b2) / (8 * pi * ((1 - b3) * (1 - b3)));
+        dp[3] = n0 / (1 - b3) + b1 * b2 / ((1 - b3) * (1 - b3)) + (b2 * b2 * b2) / (12 * pi * ((1 - b3) * (1 - b3) * (1 - b3)));
+    } else {
+        const double m = b3 - 1;
+        dp[2] = (b3 * ((b2 * b2) - 12 * b1 * m * b3 * pi) + (b2 * b2) * (m * m) * std::log(1 - b3)) / (12 * pi * (m * m) * (b3 * b3));
+        dp[3] = (b3 * ((b2 * b2 * b2) * (2 - 5 * b3 + (b3 * b3)) + 36 * b1 * b2 * m * (b3 * b3) * pi - 36 * n0 * (m * m) * (b3 * b3) * pi) -
+                 2 * (b2 * b2 * b2) * (m * m * m) * std::log(1 - b3)) /
+                (36 * pi * (m * m * m) * (b3 * b3 * b3));
+    }
+    const double dn[4] = {1, R, 4 * pi * (R * R), 4 * pi * (R * R * R) / 3.0};
+    double acc = 0.0;
+    for (int i = 0; i < 4; ++i) acc += dp[i] * dn[i];
+    const double mu = kT * acc;
+    double f0 = functional == MDFT_BRIDGE_HS_PY
+                    ? kT * (-n0 * std::log(1 - b3) + b1 * b2 / (1 - b3) + (b2 * b2 * b2) / (24 * pi * ((1 - b3) * (1 - b3))))
+                    : kT * (((1.0 / (36 * pi)) * (b2 * b2 * b2) / (b3 * b3) - n0) * std::log(1 - b3) + b1 * b2 / (1 - b3) +
+                            (1.0 / (36 * pi)) * (b2 * b2 * b2) / (((1 - b3) * (1 - b3)) * b3));
+    f0 = (f0 - mu * n0) * (g.lx * g.ly * g.lz);
+    // c_hs(k) at k = (i-1) dq with the bulk weighted densities
+    const double twopi = 2.0 * pi;
+    const double kxm = (double)(g.nx / 2) * twopi / g.lx, kym = (double)(g.ny / 2) * twopi / g.ly, kzm = (double)(g.nz / 2) * twopi / g.lz;
+    const double dq = h->ct.dq;
+    const int nbk = (int)(std::sqrt(kxm * kxm + kym * kym + kzm * kzm) / dq) + 1;
+    std::vector<double> cs(nbk);
+    // the bulk weighted densities as cs_of_k_hard_sphere forms them: n0 times w_a(k = 0)
+    const double c0 = n0 * 1.0, c1 = n0 * R, c2 = n0 * (4.0 * pi * (R * R)), c3 = n0 * (4.0 * pi / 3.0 * (R * R * R));
+    const double u = 1.0 - c3, m1 = -1.0 + c3;
+    if (std::fabs(c3 - 1) <= kEpsDp) { set_error("n3 = 1 in the hard-sphere c(k)"); return MDFT_E_ARG; }
+    double d[4][4] = {{0}};
+    if (functional == MDFT_BRIDGE_HS_PY) {
+        d[0][3] = 1.0 / u;
+        d[1][2] = 1.0 / u;
+        d[1][3] = c2 / (u * u);
+        d[2][2] = c2 / (4 * pi * (u * u));
+        d[2][3] = c1 / (u * u) + (c2 * c2) / (4 * pi * (u * u * u));
+        d[3][3] = (2.0 * c1 * c2) / (u * u * u) + c0 / (u * u) + (c2 * c2 * c2) / (4.0 * pi * ((u * u) * (u * u)));
+    } else {
+        d[0][3] = 1.0 / (1 - c3);
+        d[1][2] = 1.0 / (1.0 - c3);
+        d[1][3] = c2 / ((1.0 - c3) * (1.0 - c3));
+        d[2][2] = c2 / (6.0 * ((1.0 - c3) * (1.0 - c3)) * c3 * pi) + (c2 * std::log(1.0 - c3)) / (6.0 * (c3 * c3) * pi);
+        d[2][3] = (c3 * ((c2 * c2) * (2.0 - 5.0 * c3 + (c3 * c3)) + 12.0 * c1 * m1 * (c3 * c3) * pi) -
+                   2.0 * (c2 * c2) * (m1 * m1 * m1) * std::log(1 - c3)) /
+                  (12.0 * (m1 * m1 * m1) * (c3 * c3 * c3) * pi);
+        d[3][3] = (c3 * ((c2 * c2 * c2) * (6.0 - 21.0 * c3 + 26.0 * (c3 * c3) - 5.0 * (c3 * c3 * c3)) -
+                         72.0 * c1 * c2 * m1 * (c3 * c3 * c3) * pi + 36.0 * c0 * (m1 * m1) * (c3 * c3 * c3) * pi) +
+                   6.0 * (c2 * c2 * c2) * ((m1 * m1) * (m1 * m1)) * std::log(1.0 - c3)) /
+                  (36.0 * ((m1 * m1) * (m1 * m1)) * ((c3 * c3) * (c3 * c3)) * pi);
+    }
+    d[2][1] = d[1][2];
+    d[3][0] = d[0][3];
+    d[3][1] = d[1][3];
+    d[3][2] = d[2][3];
+    for (int i = 0; i < nbk; ++i) {
+        const double k = i * dq;
+        double w[4];
+        if (std::fabs(k) <= kEpsDp) {
+            w[0] = 1.0; w[1] = R; w[2] = 4.0 * pi * (R * R); w[3] = 4.0 * pi / 3.0 * (R * R * R);
+        } else {
+            const double kR = k * R, sk = std::sin(kR), ck = std::cos(kR);
+            w[0] = ck + kR * sk / 2.0;
+            w[1] = (sk + kR * ck) / (2.0 * k);
+            w[2] = (4.0 * pi * R * sk) / k;
+            w[3] = 4.0 * pi * (sk - kR * ck) / (k * k * k);
+        }
+        double sum = 0.0;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) sum += d[a][b] * w[a] * w[b];
+        cs[i] = -sum;
+    }
+    const size_t nb = kRedBlocks;
+    if ((rc = alloc_check(h->fmt_pl.alloc(7 * (size_t)g.N), "bridge planes", 7 * 16 * (size_t)g.N))) return rc;
+    if ((rc = alloc_check(h->fmt_cs.alloc(nbk), "hard-sphere c(k)", 8 * (size_t)nbk))) return rc;
+    if ((rc = alloc_check(h->fmt_part.alloc(10 * nb + 2), "bridge partials", 8 * (10 * nb + 2)))) return rc;
+    if ((rc = check_cuda(cudaMemcpy(h->fmt_cs.p, cs.data(), 8 * (size_t)nbk, cudaMemcpyHostToDevice), "hard-sphere c(k)"))) return rc;
+    FmtArgs &a = h->fmt_args;
+    a.N = g.N;
+    a.no = g.no;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.version = functional;
+    a.rho0 = g.rho0;
+    a.kT = kT;
+    a.dv = g.dv;
+    a.R = R;
+    a.mu = mu;
+    a.fexc0 = f0;
+    a.shift = (twopi * (4.0 * pi)) / (double)g.mrso;
+    a.nd = (double)(g.nx * g.ny * g.nz);
+    a.dq = dq;
+    a.lx = g.lx;
+    a.ly = g.ly;
+    a.lz = g.lz;
+    a.nbk = nbk;
+    h->fmt = functional;
+    return MDFT_OK;
+}
+
+int mdft_get_bridge_fmt_params(const mdft_handle *h, double *out) {
+    if (!h || !out) { set_error("null argument"); return MDFT_E_ARG; }
+    if (!h->fmt) { set_error("no hard-sphere bridge set"); return MDFT_E_STATE; }
+    out[0] = h->fmt_args.R;
+    out[1] = h->fmt_args.mu;
+    out[2] = h->fmt_args.fexc0;
+    out[3] = h->fmt_args.nbk;
+    return MDFT_OK;
+}
+
 int mdft_bridge_energy(mdft_handle *h, const double *xi, double *fb, double *df) {
     if (!h || !xi || !fb) { set_error("null argument"); return MDFT_E_ARG; }
     *fb = 0.0;
-    if (!h->cgb) return MDFT_OK;  // bridge "no"
+    if (!has_bridge(h)) return MDFT_OK;  // bridge "no"
     const size_t n = (size_t)h->g.N * h->g.no;
     int rc = check_cuda(cudaMemcpyAsync(h->xi.p, xi, n * 8, cudaMemcpyHostToDevice, h->stream), "xi upload");
     if (rc) return rc;
     if (df && (rc = check_cuda(cudaMemcpyAsync(h->df.p, df, n * 8, cudaMemcpyHostToDevice, h->stream), "df upload"))) return rc;
     if ((rc = launch_bridge(h, h->xi.p, df ? h->df.p : nullptr, nullptr))) return rc;
-    if ((rc = check_cuda(cudaMemcpyAsync(h->h_sums + 6, h->sums.p + 6, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy")))
+    if ((rc = check_cuda(cudaMemcpyAsync(h->h_sums + 6, h->sums.p + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sums copy")))
         return rc;
     if (df && (rc = check_cuda(cudaMemcpyAsync(df, h->df.p, n * 8, cudaMemcpyDeviceToHost, h->stream), "df download"))) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(h->stream), "bridge"))) return rc;
+    if (h->fmt && h->h_sums[7] != 0.0) {
+        cudaMemsetAsync(h->sums.p + 7, 0, sizeof(double), h->stream);
+        set_error("hard-sphere bridge: a weighted density left (0, 1) (code %d)", (int)h->h_sums[7]);
+        return MDFT_E_NUMERIC;
+    }
     *fb = h->h_sums[6];
     if (!std::isfinite(*fb)) { set_error("non-finite bridge energy"); return MDFT_E_NUMERIC; }
     return MDFT_OK;

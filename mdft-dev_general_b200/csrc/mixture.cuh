@@ -109,7 +109,7 @@ int mdft_mixture_create(mdft_handle *const *species, int nspec, const double *mo
             return MDFT_E_ARG;
         }
         if (h->precision != MDFT_PREC_FP64) { set_error("mixtures are evaluated in FP64: species %d is not", s); return MDFT_E_ARG; }
-        if (h->cgb) { set_error("species %d has a bridge term; the reference's bridges take one species", s); return MDFT_E_ARG; }
+        if (has_bridge(h)) { set_error("species %d has a bridge term; the reference's bridges take one species", s); return MDFT_E_ARG; }
         if (h->ct.ncoef != h0->ct.ncoef) { set_error("species %d has another c(k) coefficient count", s); return MDFT_E_ARG; }
         const double x = mole_fraction[s];
         if (!(x > 0.0 && x <= 1.0)) { set_error("mole fraction of species %d is %g, outside (0, 1]", s, x); return MDFT_E_ARG; }
@@ -173,7 +173,7 @@ int mdft_mixture_energy_and_gradient_device(mdft_mixture *m, const double *d_xi,
     if (rc) return rc;
     if (!d_xi || !f) { set_error("null argument"); return MDFT_E_ARG; }
     for (const mdft_handle *h : m->sp)
-        if (h->cgb) { set_error("a species handle has a bridge term; the reference's bridges take one species"); return MDFT_E_STATE; }
+        if (has_bridge(h)) { set_error("a species handle has a bridge term; the reference's bridges take one species"); return MDFT_E_STATE; }
     if ((rc = mixture_launch(m, d_xi, d_df))) {
         for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
         return rc;

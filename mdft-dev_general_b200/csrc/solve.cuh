@@ -1152,7 +1152,7 @@ int pressure_impl(mdft_handle *h, const double *d_xi, double ftot, double lj_tai
     double f0 = 0.0;
     f0 = f0 + fid + fext;
     f0 = f0 + fexc;
-    f0 = f0 + (h->cgb ? h->h_sums[6] : 0.0);  // the bridge term of the empty box
+    f0 = f0 + (has_bridge(h) ? h->h_sums[6] : 0.0);  // the bridge term of the empty box
     const double pbulk = f0 / (g.lx * g.ly * g.lz);
     const double pmv = -deltaN / g.n0 * pbulk;
     out[0] = ftot + pmv + lj_tail;

@@ -146,6 +146,8 @@ SIGNATURES = {
     "mdft_set_bridge_cgb": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]),
     "mdft_cgb_c00": (C.c_int, [C.c_char_p, C.c_int, _DP]),
     "mdft_bridge_energy": (C.c_int, [C.c_void_p, _DP, _DP, _DP]),
+    "mdft_set_bridge_fmt": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "mdft_get_bridge_fmt_params": (C.c_int, [C.c_void_p, _DP]),
     # multi-species solvent
     "mdft_mixture_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, _DP, C.POINTER(C.c_void_p)]),
     "mdft_mixture_destroy": (C.c_int, [C.c_void_p]),
@@ -294,6 +296,16 @@ class Engine:
             _check(lib().mdft_cgb_c00(solvent.encode(), int(self.sizes.ntheta - 1 if mmax is None else mmax), _p(v)))
             c00 = float(v[0])
         _check(lib().mdft_set_bridge_cgb(self.h, int(version), float(B6), float(sigma), float(c00 or 0.0)))
+
+    def set_bridge_fmt(self, functional, radius=1.4):
+        """bridge = "hard_sphere": functional 1 PY, 2 CS, 0 removes any bridge; radius hs_radius."""
+        _check(lib().mdft_set_bridge_fmt(self.h, int(functional), float(radius)))
+
+    def bridge_fmt_params(self):
+        """(radius, mu_exc0, Fexc0, nb_k) of the hard-sphere bridge."""
+        p = np.zeros(4)
+        _check(lib().mdft_get_bridge_fmt_params(self.h, _p(p)))
+        return p
 
     def bridge_energy(self, xi, df=None):
         """energy_bridge(fb, df): returns F_b; adds the bridge gradient to df (in place) when given."""

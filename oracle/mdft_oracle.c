@@ -374,6 +374,12 @@ typedef struct orc {
     /* bridge = "cgb" (0: none, 1: 'sla', 2: 'wda') and its parameters */
     int cgb;
     double cgb_B6, cgb_sigma, cgb_c00;
+    /* bridge = "hard_sphere" (0: none, 1: PY, 2: CS): radius, bulk excess chemical potential
+       and grand potential, and the hard-sphere c(k) on nb_k points of step dq */
+    int fmt;
+    double hs_R, hs_mu, hs_fexc0;
+    int hs_nbk;
+    double *hs_cs;
     cplx *drho; /* [N][np] */
 } orc;
 
@@ -400,7 +406,7 @@ void orc_destroy(orc *o)
     free(o->thetaof); free(o->wthetaof); free(o->phiof); free(o->psiof); free(o->w);
     free(o->kx); free(o->ky); free(o->kz); free(o->rotm);
     free(o->p3m); free(o->p3mup); free(o->p3mu); free(o->p3p); free(o->wig); free(o->ef); free(o->eb);
-    free(o->c); free(o->vext); free(o->drho);
+    free(o->c); free(o->vext); free(o->drho); free(o->hs_cs);
     free(o);
 }
 
@@ -1052,6 +1058,7 @@ static void ideal_and_external(const orc *o, const double *xi, double *fid, doub
 /* energy_and_gradient: module_energy_and_gradient.f90:36-240.               */
 /* terms = {F_id, F_ext, F_exc, corrections}                                  */
 static int bridge_cgb(const orc *o, const double *xi, double *fb, double *df);
+static int bridge_fmt(const orc *o, const double *xi, double *fb, double *df);
 
 int orc_energy_grad(orc *o, const double *xi, double *f, double *df, double *terms)
 {
@@ -1060,6 +1067,7 @@ int orc_energy_grad(orc *o, const double *xi, double *f, double *df, double *ter
     ideal_and_external(o, xi, &fid, &fext, df);
     if (excess(o, xi, &fexc, df)) return -1;
     if (o->cgb && bridge_cgb(o, xi, &fb, df)) return -1; /* energy_bridge :166-175, :246-275 */
+    if (o->fmt && bridge_fmt(o, xi, &fb, df)) return -1;
     double ff = 0.0;
     ff = ff + fid + fext;
     ff = ff + fexc;
@@ -1235,8 +1243,288 @@ int orc_set_bridge_cgb(orc *o, int version, double B6, double sigma, double c00)
 int orc_bridge_energy(orc *o, const double *xi, double *fb, double *df)
 {
     *fb = 0.0;
-    if (!o->cgb) return 0;
-    return bridge_cgb(o, xi, fb, df);
+    if (o->cgb) return bridge_cgb(o, xi, fb, df);
+    if (o->fmt) return bridge_fmt(o, xi, fb, df);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Hard-sphere bridge, bridge = "hard_sphere" (one species): module_fmt.f90:5-317 with the   */
+/* Kierlik-Rosinberg weights of module_hardspheres.f90:40-73, the bulk parameters of        */
+/* :83-189 and the hard-sphere c(k) of cs_of_k_hard_sphere.f90:3-166.                      */
+
+/* w_alpha(k), module_hardspheres.f90:56-70 */
+static void hs_weights(double R, double k, double w[4])
+{
+    const double fourpi = 4.0 * ORC_PI;
+    if (fabs(k) > EPSDP) {
+        const double kR = k * R, sk = sin(kR), ck = cos(kR);
+        w[3] = fourpi * (sk - kR * ck) / (k * k * k);
+        w[2] = fourpi * R * sk / k;
+        w[1] = (sk + kR * ck) / (2 * k);
+        w[0] = ck + kR * sk / 2;
+    } else {
+        w[3] = fourpi / 3 * (R * R * R);
+        w[2] = fourpi * (R * R);
+        w[1] = R;
+        w[0] = 1;
+    }
+}
+
+/* functional 1 PY, 2 CS; 0 removes the term.  dq: the c(k) file's step, as module_grid's dq
+   after energy_cproj_mrso (module_energy_cproj_mrso.f90:369). */
+int orc_set_bridge_fmt(orc *o, int functional, double R)
+{
+    free(o->hs_cs);
+    o->hs_cs = NULL;
+    o->fmt = 0;
+    if (functional == 0) return 0;
+    if (functional < 0 || functional > 2 || !(R > 0.0)) { set_err("bad hard-sphere parameters"); return -1; }
+    if (!o->c) { set_err("c(k) table not loaded"); return -1; }
+    const double pi = ORC_PI, kT = o->kT, n0b = o->n0;
+    /* packing fraction (:19-28, fourthird = 4./3. in single precision) and its limit (:113-120) */
+    const double pf = (double)(4.0f / 3.0f) * pi * n0b * (R * R * R);
+    if (pf >= 0.74) { set_err("hard-sphere packing fraction above 0.74"); return -1; }
+    /* excess chemical potential and bulk grand potential (:136-187) */
+    const double n0 = n0b, n1 = n0 * R, n2 = n0 * 4 * pi * (R * R), n3 = n0 * 4 * pi * (R * R * R) / 3;
+    double dphi[4];
+    if (functional == 1) {
+        dphi[0] = -log(1 - n3);
+        dphi[1] = n2 / (1 - n3);
+        dphi[2] = n1 / (1 - n3) + (n2 * n2) / (8 * pi * ((1 - n3) * (1 - n3)));
+        dphi[3] = n0 / (1 - n3) + n1 * n2 / ((1 - n3) * (1 - n3)) + (n2 * n2 * n2) / (12 * pi * ((1 - n3) * (1 - n3) * (1 - n3)));
+    } else {
+        const double m1 = n3 - 1;
+        dphi[0] = -log(1 - n3);
+        dphi[1] = n2 / (1 - n3);
+        dphi[2] = (n3 * ((n2 * n2) - 12 * n1 * m1 * n3 * pi) + (n2 * n2) * (m1 * m1) * log(1 - n3)) / (12 * pi * (m1 * m1) * (n3 * n3));
+        dphi[3] = (n3 * ((n2 * n2 * n2) * (2 - 5 * n3 + (n3 * n3)) + 36 * n1 * n2 * m1 * (n3 * n3) * pi - 36 * n0 * (m1 * m1) * (n3 * n3) * pi) -
+                   2 * (n2 * n2 * n2) * (m1 * m1 * m1) * log(1 - n3)) /
+                  (36 * pi * (m1 * m1 * m1) * (n3 * n3 * n3));
+    }
+    const double dndrho[4] = {1, R, 4 * pi * (R * R), 4 * pi * (R * R * R) / 3.0};
+    double acc = 0.0;
+    for (int a = 0; a < 4; ++a) acc += dphi[a] * dndrho[a];
+    const double mu = kT * acc;
+    double fexc0;
+    if (functional == 1)
+        fexc0 = kT * (-n0 * log(1 - n3) + n1 * n2 / (1 - n3) + (n2 * n2 * n2) / (24 * pi * ((1 - n3) * (1 - n3))));
+    else
+        fexc0 = kT * (((1.0 / (36 * pi)) * (n2 * n2 * n2) / (n3 * n3) - n0) * log(1 - n3) + n1 * n2 / (1 - n3) +
+                      (1.0 / (36 * pi)) * (n2 * n2 * n2) / (((1 - n3) * (1 - n3)) * n3));
+    fexc0 = (fexc0 - mu * n0b) * (o->lx * o->ly * o->lz);
+    /* the hard-sphere c(k) (cs_of_k_hard_sphere.f90:56-157) */
+    const double kxm = o->kx[o->nx / 2], kym = o->ky[o->ny / 2], kzm = o->kz[o->nz / 2];
+    const int nbk = (int)(sqrt(kxm * kxm + kym * kym + kzm * kzm) / o->dq) + 1;
+    double *cs = malloc(sizeof(double) * nbk);
+    if (!cs) { set_err("out of memory"); return -1; }
+    double b0 = 0, b1 = 0, b2 = 0, b3 = 0; /* the bulk weighted densities, set at k = 0 */
+    for (int i = 0; i < nbk; ++i) {
+        const double k = i * o->dq;
+        double w[4];
+        if (fabs(k) <= EPSDP) {
+            w[0] = 1.0; w[1] = R; w[2] = 4.0 * pi * (R * R); w[3] = 4.0 * pi / 3.0 * (R * R * R);
+            b0 = n0b * w[0]; b1 = n0b * w[1]; b2 = n0b * w[2]; b3 = n0b * w[3];
+        } else {
+            const double kR = k * R, sk = sin(kR), ck = cos(kR);
+            w[0] = ck + kR * sk / 2.0;
+            w[1] = (sk + kR * ck) / (2.0 * k);
+            w[2] = (4.0 * pi * R * sk) / k;
+            w[3] = 4.0 * pi * (sk - kR * ck) / (k * k * k);
+        }
+        if (fabs(b3 - 1) <= EPSDP) { free(cs); set_err("n3 = 1 in the hard-sphere c(k)"); return -1; }
+        double d[4][4] = {{0}};
+        const double u = 1.0 - b3;
+        if (functional == 1) {
+            d[0][3] = 1.0 / u;
+            d[1][2] = 1.0 / u;
+            d[1][3] = b2 / (u * u);
+            d[2][1] = d[1][2];
+            d[2][2] = b2 / (4 * pi * (u * u));
+            d[2][3] = b1 / (u * u) + (b2 * b2) / (4 * pi * (u * u * u));
+            d[3][0] = d[0][3];
+            d[3][1] = d[1][3];
+            d[3][2] = d[2][3];
+            d[3][3] = (2.0 * b1 * b2) / (u * u * u) + b0 / (u * u) + (b2 * b2 * b2) / (4.0 * pi * ((u * u) * (u * u)));
+        } else {
+            const double m1 = -1.0 + b3;
+            d[0][3] = 1.0 / (1 - b3);
+            d[1][2] = 1.0 / (1.0 - b3);
+            d[1][3] = b2 / ((1.0 - b3) * (1.0 - b3));
+            d[2][1] = d[1][2];
+            d[2][2] = b2 / (6.0 * ((1.0 - b3) * (1.0 - b3)) * b3 * pi) + (b2 * log(1.0 - b3)) / (6.0 * (b3 * b3) * pi);
+            d[2][3] = (b3 * ((b2 * b2) * (2.0 - 5.0 * b3 + (b3 * b3)) + 12.0 * b1 * m1 * (b3 * b3) * pi) -
+                       2.0 * (b2 * b2) * (m1 * m1 * m1) * log(1 - b3)) /
+                      (12.0 * (m1 * m1 * m1) * (b3 * b3 * b3) * pi);
+            d[3][0] = d[0][3];
+            d[3][1] = d[1][3];
+            d[3][2] = d[2][3];
+            d[3][3] = (b3 * ((b2 * b2 * b2) * (6.0 - 21.0 * b3 + 26.0 * (b3 * b3) - 5.0 * (b3 * b3 * b3)) -
+                             72.0 * b1 * b2 * m1 * (b3 * b3 * b3) * pi + 36.0 * b0 * (m1 * m1) * (b3 * b3 * b3) * pi) +
+                       6.0 * (b2 * b2 * b2) * ((m1 * m1) * (m1 * m1)) * log(1.0 - b3)) /
+                      (36.0 * ((m1 * m1) * (m1 * m1)) * ((b3 * b3) * (b3 * b3)) * pi);
+        }
+        double sum = 0.0;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) sum += d[a][b] * w[a] * w[b];
+        cs[i] = -sum;
+    }
+    o->fmt = functional;
+    o->hs_R = R;
+    o->hs_mu = mu;
+    o->hs_fexc0 = fexc0;
+    o->hs_nbk = nbk;
+    o->hs_cs = cs;
+    return 0;
+}
+
+int orc_fmt_params(const orc *o, double *out /* R, mu, Fexc0, nb_k */)
+{
+    out[0] = o->hs_R; out[1] = o->hs_mu; out[2] = o->hs_fexc0; out[3] = o->hs_nbk;
+    return o->fmt ? 0 : -1;
+}
+
+/* energy_bridge_fmt (module_fmt.f90:5-317) for one species (mole fraction 1).  Real-to-complex
+   transforms run as complex FFTs of real data; the multipliers depend on |k| only. */
+static int bridge_fmt(const orc *o, const double *xi, double *fb_out, double *df)
+{
+    const long N = o->N;
+    const int no = o->no, nx = o->nx, ny = o->ny, nz = o->nz;
+    const double kT = o->kT, dv = o->dv, rho0 = o->rho0, pi = ORC_PI, R = o->hs_R, mu = o->hs_mu;
+    /* empty box (:46-49) */
+    int empty = 1;
+    for (long i = 0; i < N * no && empty; ++i)
+        if (fabs(xi[i]) > EPSDP) empty = 0;
+    if (empty) { *fb_out = -o->hs_fexc0; return 0; }
+    cplx *rk = malloc(sizeof(cplx) * N), *wd = malloc(sizeof(cplx) * 4 * N), *gk = malloc(sizeof(cplx) * N);
+    double *rho = calloc(N, sizeof(double)), *kn = malloc(sizeof(double) * N);
+    if (!rk || !wd || !gk || !rho || !kn) {
+        free(rk); free(wd); free(gk); free(rho); free(kn);
+        set_err("out of memory");
+        return -1;
+    }
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                const double kx = o->kx[ix], ky = o->ky[iy], kz = o->kz[iz];
+                kn[((long)iz * ny + iy) * nx + ix] = sqrt(kx * kx + ky * ky + kz * kz);
+            }
+    /* rho(r) = sum_io xi^2 w (:51-63) and the molecule count (:66-68) */
+    double srho = 0.0;
+    for (long r = 0; r < N; ++r) {
+        double a = 0.0;
+        for (int io = 0; io < no; ++io) a = a + xi[r * no + io] * xi[r * no + io] * o->w[io];
+        rho[r] = a;
+        srho += a;
+    }
+    const double nmol = srho * dv * rho0 * 1.0;
+    /* weighted densities (:84-91) */
+    for (long r = 0; r < N; ++r) rk[r] = rho[r];
+    fft3d(rk, nx, ny, nz, -1);
+    for (int a = 0; a < 4; ++a) {
+        cplx *p = wd + a * N;
+        for (long r = 0; r < N; ++r) {
+            double w[4];
+            hs_weights(R, kn[r], w);
+            /* cmplx(w_k, 0) without KIND is single precision (:88) */
+            p[r] = rk[r] * rho0 * 1.0 * (double)(float)w[a];
+        }
+        fft3d(p, nx, ny, nz, +1);
+        for (long r = 0; r < N; ++r) p[r] = creal(p[r]) / (double)(nx * ny * nz);
+    }
+#define WD(a, r) creal(wd[(a) * N + (r)])
+    int rc = 0;
+    double s1 = 0, s2 = 0, s3 = 0;
+    for (long r = 0; r < N; ++r) {
+        const double w0 = WD(0, r), w1 = WD(1, r), w2 = WD(2, r), w3 = WD(3, r);
+        if (w3 >= 1) { rc = -1; set_err("1 - w3 <= 0 in the hard-sphere bridge"); break; }
+        if (o->fmt == 1) {
+            s1 += w0 * log(1 - w3);
+            s2 += w1 * w2 / (1 - w3);
+            s3 += (w2 * w2 * w2) / ((1 - w3) * (1 - w3));
+        } else {
+            if (w3 <= EPSDP) { rc = -1; set_err("w3 <= 0 in the hard-sphere bridge"); break; }
+            s1 += w1 * w2 / (1 - w3);
+            s2 += ((1.0 / (36.0 * pi)) * (w2 * w2 * w2) / (w3 * w3) - w0) * log(1 - w3);
+            s3 += (1.0 / (36.0 * pi)) * (w2 * w2 * w2) / (w3 * ((1 - w3) * (1 - w3)));
+        }
+    }
+    double ffmt = 0.0;
+    if (!rc) {
+        ffmt = o->fmt == 1 ? -s1 + s2 + s3 / (24 * pi) : s1 + s2 + s3;
+        ffmt = ffmt * kT * dv - mu * nmol - o->hs_fexc0 * 1.0;
+    }
+    /* gradient (:128-219): dPhi/dw_alpha, transformed, weighted, summed, back */
+    if (!rc && df) {
+        for (long r = 0; r < N && !rc; ++r) {
+            const double w0 = WD(0, r), w1 = WD(1, r), w2 = WD(2, r), w3 = WD(3, r);
+            /* :131, :138-139 */
+            if ((1 - w3) <= EPSDP || (o->fmt == 2 && fabs(w3) <= EPSDP)) { rc = -1; set_err("1 - w3 or w3 at 0 in the hard-sphere bridge"); break; }
+            double d[4];
+            if (o->fmt == 1) {
+                d[0] = -log(1 - w3);
+                d[1] = w2 / (1 - w3);
+                d[2] = w1 / (1 - w3) + (1.0 / (8.0 * pi)) * (d[1] * d[1]);
+                d[3] = (w0 + w1 * d[1]) / (1 - w3) + (1.0 / (12.0 * pi)) * (d[1] * d[1] * d[1]);
+            } else {
+                const double q23 = w2 / w3;
+                d[0] = -log((1 - w3));
+                d[1] = w2 / (1 - w3);
+                d[2] = -(1.0 / (12.0 * pi)) * (q23 * q23) * d[0] + w1 / (1 - w3) + (1.0 / (12.0 * pi)) * (d[1] * d[1]) / w3;
+                d[3] = (1.0 / (18.0 * pi)) * d[0] * (q23 * q23 * q23) - ((1.0 / (36.0 * pi)) * (w2 * w2 * w2) / (w3 * w3) - w0) / (1 - w3) +
+                       w1 * d[1] / (1 - w3) +
+                       (1.0 / (36.0 * pi)) * (w2 * w2 * w2) / (w3 * w3) * (3.0 * w3 - 1.0) / ((1 - w3) * (1 - w3) * (1 - w3));
+            }
+            for (int a = 0; a < 4; ++a) wd[a * N + r] = d[a];
+        }
+        if (rc) goto out;
+        for (int a = 0; a < 4; ++a) fft3d(wd + a * N, nx, ny, nz, -1);
+        for (long r = 0; r < N; ++r) {
+            double w[4];
+            hs_weights(R, kn[r], w);
+            gk[r] = wd[r] * w[0] + wd[N + r] * w[1] + wd[2 * N + r] * w[2] + wd[3 * N + r] * w[3];
+        }
+        fft3d(gk, nx, ny, nz, +1);
+        for (long r = 0; r < N; ++r) {
+            const double dfex = creal(gk[r]) / (double)(nx * ny * nz);
+            for (int io = 0; io < no; ++io) {
+                const double psi = xi[r * no + io];
+                df[r * no + io] = df[r * no + io] + 2 * psi * rho0 * (kT * dfex - mu) * o->w[io];
+            }
+        }
+    }
+#undef WD
+    /* minus the hard-sphere c(k)'s quadratic part (:223-282) */
+    if (!rc) {
+        const double shift = ((2.0 * pi) * (4.0 * pi)) / (double)o->mrso; /* twopi*fourpi/mrso */
+        for (long r = 0; r < N; ++r) rk[r] = rho[r] - shift;
+        fft3d(rk, nx, ny, nz, -1);
+        for (long r = 0; r < N; ++r) {
+            int ki = (int)(kn[r] / o->dq) + 1;
+            if (ki > o->hs_nbk) ki = o->hs_nbk;
+            rk[r] = rk[r] * o->hs_cs[ki - 1];
+        }
+        fft3d(rk, nx, ny, nz, +1);
+        const double fact = dv * rho0;
+        double fint = 0.0;
+        for (int ix = 0; ix < nx; ++ix)
+            for (int iy = 0; iy < ny; ++iy)
+                for (int iz = 0; iz < nz; ++iz) {
+                    const long r = ((long)iz * ny + iy) * nx + ix;
+                    const double gam = creal(rk[r]) / (double)(nx * ny * nz);
+                    const double vint = -kT * rho0 * gam;
+                    for (int io = 0; io < no; ++io) {
+                        const double psi = xi[r * no + io];
+                        fint = fint + o->w[io] * fact * 0.5 * (psi * psi - 1.0) * vint;
+                        if (df) df[r * no + io] = df[r * no + io] - 2.0 * psi * o->w[io] * fact * vint / dv;
+                    }
+                }
+        ffmt = ffmt - fint;
+    }
+out:
+    free(rk); free(wd); free(gk); free(rho); free(kn);
+    *fb_out = ffmt;
+    return rc;
 }
 
 /* Charged-solute corrections: module_energy_and_gradient.f90:281-344.        */

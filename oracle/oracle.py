@@ -65,6 +65,8 @@ def lib():
         L.orc_mixture_energy_grad.argtypes = [C.POINTER(C.c_void_p), C.c_int, dp, dp, dp, dp, dp]
         L.orc_set_bridge_cgb.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_bridge_energy.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_set_bridge_fmt.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.orc_fmt_params.argtypes = [C.c_void_p, dp]
     return _LIB
 
 
@@ -181,6 +183,15 @@ class Oracle:
         """bridge = "cgb": version 0 none, 1 'sla', 2 'wda'; c00 the solvent's c(k=0)."""
         if lib().orc_set_bridge_cgb(self.h, version, B6, sigma, c00) != 0:
             raise RuntimeError(lib().orc_last_error().decode())
+
+    def set_bridge_fmt(self, functional, radius=1.4):
+        """bridge = "hard_sphere": functional 1 PY, 2 CS, 0 removes it; radius hs_radius."""
+        if lib().orc_set_bridge_fmt(self.h, functional, radius) != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def fmt_params(self):
+        """(radius, excess chemical potential, bulk grand potential Fexc0, nb_k)."""
+        p = np.zeros(4); lib().orc_fmt_params(self.h, _p(p)); return p
 
     def bridge_energy(self, xi, df=None):
         """energy_bridge(fb, df): returns fb; adds the bridge gradient to df when given."""

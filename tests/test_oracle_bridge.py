@@ -73,3 +73,54 @@ def test_energy_and_gradient_adds_the_bridge(tmp_path, version):
     o.set_bridge_cgb(0)
     f2, _, _ = o.energy_grad(xi)
     assert f2 == f0
+
+
+# ---- bridge = "hard_sphere" (src/module_fmt.f90) ------------------------------------------
+
+@pytest.mark.parametrize("functional", [1, 2])
+def test_fmt_bulk_parameters_match_the_closed_forms(tmp_path, functional):
+    # the Kierlik-Rosinberg functional reproduces the Percus-Yevick (compressibility) and
+    # Carnahan-Starling equations of state: beta mu_exc and the excess free energy per
+    # particle in closed form in the packing fraction eta
+    o, _ = system(tmp_path)
+    R = 1.4
+    o.set_bridge_fmt(functional, R)
+    r, mu, fexc0, nbk = o.fmt_params()
+    eta = 4.0 / 3.0 * np.pi * SV.n0 * R ** 3
+    if functional == 1:
+        bmu = -np.log(1 - eta) + eta * (14 - 13 * eta + 5 * eta ** 2) / (2 * (1 - eta) ** 3)
+        bf = -np.log(1 - eta) + 3 * eta * (2 - eta) / (2 * (1 - eta) ** 2)
+    else:
+        bmu = eta * (8 - 9 * eta + 3 * eta ** 2) / (1 - eta) ** 3
+        bf = eta * (4 - 3 * eta) / (1 - eta) ** 2
+    assert abs(mu / SV.kT - bmu) <= 1e-12 * bmu
+    V = 8.0 ** 3
+    # Fexc0 = (f_exc - mu n0) V, so f_exc / n0 = Fexc0 / (V n0) + mu
+    assert abs((fexc0 / (V * SV.n0) + mu) / SV.kT - bf) <= 1e-12 * bf
+    assert nbk > 1
+
+
+@pytest.mark.parametrize("functional", [1, 2])
+def test_fmt_gradient_is_the_derivative(tmp_path, functional):
+    # the energy's weights are the reference's single-precision cmplx(w_k, 0), the gradient's
+    # are not (module_fmt.f90:88 against :170-174): agreement to 1e-5, not to rounding
+    o, xi = system(tmp_path)
+    o.set_bridge_fmt(functional, 1.4)
+    fd, an = fd_check(o, xi, h=1e-4)
+    assert abs(fd - an) <= 1e-5 * abs(fd), (fd, an)
+
+
+@pytest.mark.parametrize("functional", [1, 2])
+def test_fmt_bulk_and_empty_box(tmp_path, functional):
+    o, _ = system(tmp_path)
+    o.set_bridge_fmt(functional, 1.4)
+    fexc0 = o.fmt_params()[2]
+    # bulk: the functional is shifted to vanish there (up to the single-precision weights)
+    assert abs(o.bridge_energy(np.ones(o.shape))) < 1e-4
+    # empty box (every |xi| <= epsilon): -Fexc0 and no gradient (:46-49)
+    g = np.zeros(o.shape)
+    assert o.bridge_energy(np.zeros(o.shape), g) == -fexc0
+    assert not g.any()
+    # a weighted density n3 >= 1 stops the reference; the oracle reports it
+    with pytest.raises(RuntimeError, match="w3"):
+        o.bridge_energy(3.0 * np.ones(o.shape))
