@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(kBrThreads) k_cgb_finish(const double *__restr
 //   F_int, df -= the quadratic part of the hard-sphere c(k) (:223-282): gamma = IFFT(FFT(rho -
 //   8 pi^2 / mrso) c_hs(k bin)) / N, F_int = sum w dv rho0 0.5 (xi^2 - 1) (-kT rho0 gamma),
 //   df -= 2 xi w dv rho0 (-kT rho0 gamma) / dv.
-// fl(): the reference's cmplx(w_k, 0) is single precision (:88).  Planes (N complex each):
+// fl(): the reference's cmplx(w_k, 0) is single precision (:92).  Planes (N complex each):
 // 0 rho, 1 rho - 8 pi^2/mrso (then gamma), 2-5 wd_a (then dPhi/dwd_a), 6 the gradient sum.
 struct FmtArgs {
     long long N;

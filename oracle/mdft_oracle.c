@@ -1426,7 +1426,7 @@ static int bridge_fmt(const orc *o, const double *xi, double *fb_out, double *df
         for (long r = 0; r < N; ++r) {
             double w[4];
             hs_weights(R, kn[r], w);
-            /* cmplx(w_k, 0) without KIND is single precision (:88) */
+            /* cmplx(w_k, 0) without KIND is single precision (:92) */
             p[r] = rk[r] * rho0 * 1.0 * (double)(float)w[a];
         }
         fft3d(p, nx, ny, nz, +1);

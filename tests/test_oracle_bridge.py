@@ -103,7 +103,7 @@ def test_fmt_bulk_parameters_match_the_closed_forms(tmp_path, functional):
 @pytest.mark.parametrize("functional", [1, 2])
 def test_fmt_gradient_is_the_derivative(tmp_path, functional):
     # the energy's weights are the reference's single-precision cmplx(w_k, 0), the gradient's
-    # are not (module_fmt.f90:88 against :170-174): agreement to 1e-5, not to rounding
+    # are not (module_fmt.f90:92 against :170-174): agreement to 1e-5, not to rounding
     o, xi = system(tmp_path)
     o.set_bridge_fmt(functional, 1.4)
     fd, an = fd_check(o, xi, h=1e-4)
