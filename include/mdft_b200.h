@@ -445,6 +445,10 @@ int mdft_mixture_destroy(mdft_mixture *m);
 int mdft_mixture_energy_and_gradient(mdft_mixture *m, const double *xi, double *f, double *df, double *terms);
 /* Device arrays (d_df may be NULL: energy only). */
 int mdft_mixture_energy_and_gradient_device(mdft_mixture *m, const double *d_xi, double *d_df, double *f, double *terms);
+/* energy_minimization of a mixture: the L-BFGS of mdft_minimize (FP64 only) over every
+ * species' xi at once (xi: [nspec][N][no] host array, updated in place); the reference's
+ * minimiser runs on the vector of all species. */
+int mdft_mixture_minimize(mdft_mixture *m, double *xi, const mdft_minimize_opts *opts, mdft_minimize_result *res);
 
 #ifdef __cplusplus
 }

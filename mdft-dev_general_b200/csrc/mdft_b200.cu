@@ -61,6 +61,9 @@ using namespace mdft;
 
 struct mdft_handle {
     Grid g;
+    // set on species 0's handle while mdft_mixture_minimize runs: the minimiser's vectors
+    // span every species and its evaluations are the mixture's
+    mdft_mixture *mix = nullptr;
     CTable ct;
     int precision = MDFT_PREC_FP64;
     int device = 0;

@@ -28,8 +28,9 @@ struct mdft_mixture {
     DevBuf<int> oz_ints;
     DevBuf<double> oz_dbls;
     int oz_grid = 0;
-    DevBuf<double> xi, df;  // staging of the host entry point, [nspec][N][no]
-    std::vector<cudaEvent_t> ev_fwd;
+    DevBuf<double> xi, df;  // staging of the host entry point and the minimiser's gradient, [nspec][N][no]
+    std::vector<cudaEvent_t> ev_fwd, ev_done;  // per species: forward FFTs done, gather done
+    cudaEvent_t ev_start = nullptr;            // species 0's stream: the point is ready
 };
 
 namespace {
@@ -40,11 +41,17 @@ int mixture_check(const mdft_mixture *m) {
 }
 
 // Launches one evaluation; leaves each species' sums on its handle (finish_sums reads them).
-int mixture_launch(mdft_mixture *m, const double *d_xi, double *d_df) {
+// The point may come from work on species 0's stream (the minimiser's trial point): every
+// species stream starts after it, and species 0's stream continues after every gather.
+// dvec (may be null): the gathers also form df.dvec, as in single-species evaluations.
+int mixture_launch(mdft_mixture *m, const double *d_xi, double *d_df, const double *dvec = nullptr) {
     const int ns = (int)m->sp.size();
     const Grid &g = m->sp[0]->g;
     const size_t n = (size_t)g.N * g.no;
     int rc;
+    if ((rc = check_cuda(cudaEventRecord(m->ev_start, m->sp[0]->stream), "event record"))) return rc;
+    for (int s = 1; s < ns; ++s)
+        if ((rc = check_cuda(cudaStreamWaitEvent(m->sp[s]->stream, m->ev_start, 0), "stream wait"))) return rc;
     for (int s = 0; s < ns; ++s) {
         mdft_handle *h = m->sp[s];
         const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
@@ -70,16 +77,78 @@ int mixture_launch(mdft_mixture *m, const double *d_xi, double *d_df) {
         }
         const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
         if ((rc = launch_fft_t<double>(h, gam, tw, -1))) return rc;
-        const GatherArgs ga = gather_args(h, d_df ? 1 : 0, 1, nullptr, m->x[s2]);
-        const bool tma = h->gt_ncol64 > 0 && ((uintptr_t)(d_xi + s2 * n) & 15u) == 0;
+        const double *dv = dvec ? dvec + s2 * n : nullptr;
+        const GatherArgs ga = gather_args(h, d_df ? 1 : 0, 1, dv, m->x[s2]);
+        const bool tma = h->gt_ncol64 > 0 && ((uintptr_t)(d_xi + s2 * n) & 15u) == 0 && ((uintptr_t)dv & 15u) == 0;
         const long long rows = launch_gather_cc<double>(h, gam, h->B.p, d_xi + s2 * n, d_df ? d_df + s2 * n : nullptr, ga,
                                                         tma ? h->gt_ncol64 : 0);
         if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
         k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, rows, h->sums.p);
         if ((rc = check_cuda(cudaGetLastError(), "reduce launch"))) return rc;
         h->launches += ns + 2;
+        if ((rc = check_cuda(cudaEventRecord(m->ev_done[s2], h->stream), "event record"))) return rc;
+    }
+    for (int s = 1; s < ns; ++s)
+        if ((rc = check_cuda(cudaStreamWaitEvent(m->sp[0]->stream, m->ev_done[s], 0), "stream wait"))) return rc;
+    return MDFT_OK;
+}
+
+// Reads every species' sums (synchronising its stream): F, and with the gradient's
+// reductions summed over species {df.dvec, max|df|, sum w df dv}; fscale the terms' sizes.
+int mixture_finish(mdft_mixture *m, double *f, double *terms, double *gd, double *gmax, double *guni, double *fscale) {
+    double fid = 0.0, fext = 0.0, sexc = 0.0, gdv = 0.0, gmx = 0.0, gun = 0.0;
+    int first = 0;
+    for (mdft_handle *h : m->sp) {
+        double a = 0, b = 0, c = 0;
+        const int r = finish_sums(h, &a, &b, &c);  // synchronises the species' stream
+        if (r && !first) first = r;
+        // src/module_energy_ideal_and_external.f90:46-72 sums F_id and F_ext over species in
+        // order; F_exc = 0.5 dv sum_{s2} (...) (src/module_energy_cproj_mrso_mixture.f90:788-809)
+        fid += a;
+        fext += b;
+        sexc += h->h_sums[2];
+        gdv += h->h_sums[3];
+        gmx = std::max(gmx, h->h_sums[4]);
+        gun += h->h_sums[5];
+    }
+    if (first) return first;
+    const mdft_handle *h0 = m->sp[0];
+    const double fexc = sexc * 0.5 * h0->g.dv;
+    *f = combine(h0, fid, fext, fexc);
+    if (terms) {
+        terms[0] = fid;
+        terms[1] = fext;
+        terms[2] = fexc;
+        terms[3] = h0->const_corr;
+    }
+    if (gd) *gd = gdv;
+    if (gmax) *gmax = gmx;
+    if (guni) *guni = gun * h0->g.dv;
+    if (fscale) *fscale = std::fabs(fid) + std::fabs(fext) + std::fabs(fexc) + std::fabs(h0->const_corr);
+    if (!std::isfinite(gdv) || !std::isfinite(gmx) || !std::isfinite(gun)) {
+        set_error("non-finite gradient");
+        return MDFT_E_NUMERIC;
     }
     return MDFT_OK;
+}
+
+long long mixture_len(const mdft_mixture *m) { return (long long)m->sp.size() * m->sp[0]->g.N * m->sp[0]->g.no; }
+
+double *mixture_grad(mdft_mixture *m) {
+    const size_t n = (size_t)mixture_len(m);
+    if (!m->df.p && alloc_check(m->df.alloc(n), "mixture df", n * 8)) return nullptr;
+    return m->df.p;
+}
+
+int mixture_eval_launch(mdft_mixture *m, const double *x, double *g, const double *dvec) {
+    const int rc = mixture_launch(m, x, g, dvec);
+    if (rc)
+        for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
+    return rc;
+}
+
+int mixture_eval_finish(mdft_mixture *m, double *f, double *gd, double *gmax, double *guni, double *fscale) {
+    return mixture_finish(m, f, nullptr, gd, gmax, guni, fscale);
 }
 
 }  // namespace
@@ -147,12 +216,24 @@ int mdft_mixture_create(mdft_handle *const *species, int nspec, const double *mo
     const long long groups = (nk + h0->oz_warps - 1) / h0->oz_warps;
     m->oz_grid = (int)std::min<long long>(groups, (long long)std::max(1, per_sm) * h0->nsm);
     m->ev_fwd.assign(nspec, nullptr);
+    m->ev_done.assign(nspec, nullptr);
+    auto drop_events = [&]() {
+        for (cudaEvent_t e : m->ev_fwd)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : m->ev_done)
+            if (e) cudaEventDestroy(e);
+        if (m->ev_start) cudaEventDestroy(m->ev_start);
+    };
     for (int s = 0; s < nspec; ++s)
-        if ((rc = check_cuda(cudaEventCreateWithFlags(&m->ev_fwd[s], cudaEventDisableTiming), "event create"))) {
-            for (cudaEvent_t e : m->ev_fwd)
-                if (e) cudaEventDestroy(e);
+        if ((rc = check_cuda(cudaEventCreateWithFlags(&m->ev_fwd[s], cudaEventDisableTiming), "event create")) ||
+            (rc = check_cuda(cudaEventCreateWithFlags(&m->ev_done[s], cudaEventDisableTiming), "event create"))) {
+            drop_events();
             return rc;
         }
+    if ((rc = check_cuda(cudaEventCreateWithFlags(&m->ev_start, cudaEventDisableTiming), "event create"))) {
+        drop_events();
+        return rc;
+    }
     *out = m.release();
     return MDFT_OK;
 }
@@ -163,6 +244,9 @@ int mdft_mixture_destroy(mdft_mixture *m) {
     for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
     for (cudaEvent_t e : m->ev_fwd)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : m->ev_done)
+        if (e) cudaEventDestroy(e);
+    if (m->ev_start) cudaEventDestroy(m->ev_start);
     m->gam.free(); m->oz_ints.free(); m->oz_dbls.free(); m->xi.free(); m->df.free();
     delete m;
     return MDFT_OK;
@@ -178,29 +262,7 @@ int mdft_mixture_energy_and_gradient_device(mdft_mixture *m, const double *d_xi,
         for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
         return rc;
     }
-    // src/module_energy_ideal_and_external.f90:46-72 sums F_id and F_ext over species in
-    // order; F_exc = 0.5 dv sum_{s2} (...) (src/module_energy_cproj_mrso_mixture.f90:788-809)
-    double fid = 0.0, fext = 0.0, sexc = 0.0;
-    int first = 0;
-    for (mdft_handle *h : m->sp) {
-        double a = 0, b = 0, c = 0;
-        const int r = finish_sums(h, &a, &b, &c);  // synchronises the species' stream
-        if (r && !first) first = r;
-        fid += a;
-        fext += b;
-        sexc += h->h_sums[2];
-    }
-    if (first) return first;
-    const mdft_handle *h0 = m->sp[0];
-    const double fexc = sexc * 0.5 * h0->g.dv;
-    *f = combine(h0, fid, fext, fexc);
-    if (terms) {
-        terms[0] = fid;
-        terms[1] = fext;
-        terms[2] = fexc;
-        terms[3] = h0->const_corr;
-    }
-    return MDFT_OK;
+    return mixture_finish(m, f, terms, nullptr, nullptr, nullptr, nullptr);
 }
 
 int mdft_mixture_energy_and_gradient(mdft_mixture *m, const double *xi, double *f, double *df, double *terms) {
@@ -220,6 +282,34 @@ int mdft_mixture_energy_and_gradient(mdft_mixture *m, const double *xi, double *
         if ((rc = check_cuda(cudaStreamSynchronize(st), "df download"))) return rc;
     }
     return MDFT_OK;
+}
+
+// energy_minimization over every species' xi at once (the reference's L-BFGS on the vector of
+// all species): the FP64 minimiser of mdft_minimize with the mixture's evaluations.
+int mdft_mixture_minimize(mdft_mixture *m, double *xi, const mdft_minimize_opts *o, mdft_minimize_result *res) {
+    int rc = mixture_check(m);
+    if (rc) return rc;
+    if (!xi || !o || !res) { set_error("null argument"); return MDFT_E_ARG; }
+    if ((rc = check_min_opts(o))) return rc;
+    if (o->precision != MDFT_PREC_FP64) { set_error("mixtures are minimised in FP64"); return MDFT_E_ARG; }
+    for (const mdft_handle *h : m->sp)
+        if (has_bridge(h)) { set_error("a species handle has a bridge term; the reference's bridges take one species"); return MDFT_E_STATE; }
+    mdft_handle *h0 = m->sp[0];
+    struct Bind {  // species 0's handle runs the minimiser on the mixture while this lives
+        mdft_handle *h;
+        Bind(mdft_handle *hh, mdft_mixture *mm) : h(hh) { h->mix = mm; }
+        ~Bind() { h->mix = nullptr; }
+    } bind(h0, m);
+    if (!mixture_grad(m)) return MDFT_E_NOMEM;
+    if ((rc = lbfgs_alloc(h0, o->m))) return rc;
+    LbfgsState &L = h0->lb;
+    if ((rc = check_cuda(cudaMemcpyAsync(L.x.p, xi, L.n * 8, cudaMemcpyHostToDevice, h0->stream), "xi upload"))) return rc;
+    if ((rc = solve_phases(h0, o, res))) {
+        for (mdft_handle *h : m->sp) cudaStreamSynchronize(h->stream);
+        return rc;
+    }
+    if ((rc = check_cuda(cudaMemcpyAsync(xi, L.x.p, L.n * 8, cudaMemcpyDeviceToHost, h0->stream), "xi download"))) return rc;
+    return check_cuda(cudaStreamSynchronize(h0->stream), "xi download");
 }
 
 }  // extern "C"

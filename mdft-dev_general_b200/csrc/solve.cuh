@@ -10,14 +10,23 @@ constexpr double kQfact = 1.602176565e-19 * 1.602176565e-19 * 1.0e-3 * 6.0221412
 
 inline unsigned vec_grid() { return kRedBlocks; }
 
+// multi-species minimisation (mixture.cuh): vector length, gradient buffer and the two
+// halves of an evaluation of every species
+long long mixture_len(const mdft_mixture *m);
+double *mixture_grad(mdft_mixture *m);
+int mixture_eval_launch(mdft_mixture *m, const double *x, double *g, const double *dvec);
+int mixture_eval_finish(mdft_mixture *m, double *f, double *gd, double *gmax, double *guni, double *fscale);
+
 // Evaluation in two halves so that more work can be queued before the synchronise:
 // eval_launch queues the pipeline at x (gradient into g; with dvec also g.dvec and max|g|
 // from the gather pass), eval_finish waits and reads f, g.dvec, max|g| and sum w g dv.
 int eval_launch(mdft_handle *h, const void *x, double *g, const void *dvec, bool v32 = false, bool x32 = false) {
+    if (h->mix) return mixture_eval_launch(h->mix, static_cast<const double *>(x), g, static_cast<const double *>(dvec));
     return run_pipeline(h, x, g, 1, 1, dvec, v32, x32);
 }
 
 int eval_finish(mdft_handle *h, double *f, double *gd, double *gmax, double *guni = nullptr, double *fscale = nullptr) {
+    if (h->mix) return mixture_eval_finish(h->mix, f, gd, gmax, guni, fscale);
     double fid, fext, fexc;
     int rc = finish_sums(h, &fid, &fext, &fexc);
     if (rc) return rc;
@@ -165,7 +174,7 @@ int autotune_at_create(mdft_handle *h) {
 
 int lbfgs_alloc(mdft_handle *h, int m) {
     LbfgsState &L = h->lb;
-    const long long n = h->g.N * h->g.no;
+    const long long n = h->mix ? mixture_len(h->mix) : h->g.N * h->g.no;
     if (L.n == n && L.m == m) return 0;
     lbfgs_free(L);
     L.n = n;
@@ -856,7 +865,8 @@ int minimize_impl(mdft_handle *h, const mdft_minimize_opts *o, mdft_minimize_res
     const int m = o->m;
     cudaStream_t st = h->stream;
     if (H.m != m) H.reset(m, H.low);
-    double *xc = L.x.p, *xt = L.t.p, *gc = h->df.p, *gt = L.r.p;  // gc, gt and L.d hold TV values
+    double *const g0 = h->mix ? mixture_grad(h->mix) : h->df.p;  // the gradient's home buffer
+    double *xc = L.x.p, *xt = L.t.p, *gc = g0, *gt = L.r.p;  // gc, gt and L.d hold TV values
     const bool v32 = H.low;  // mixed solves: FP32 gradient and direction vectors
     // FP32 phase of a mixed solve: the point too is FP32 (xc, xt then hold floats); the FP64
     // start point in L.x is converted into L.t first, and the result back into L.x at the end
@@ -1020,7 +1030,7 @@ done:
     } else if (xc != L.x.p) {
         cudaMemcpyAsync(L.x.p, xc, n * 8, cudaMemcpyDeviceToDevice, st);
     }
-    if (gc != h->df.p) cudaMemcpyAsync(h->df.p, gc, n * (v32 ? 4 : 8), cudaMemcpyDeviceToDevice, st);
+    if (gc != g0) cudaMemcpyAsync(g0, gc, n * (v32 ? 4 : 8), cudaMemcpyDeviceToDevice, st);
     if ((rc = check_cuda(cudaStreamSynchronize(st), "minimize"))) return rc;
     res->f = f;
     res->pgnorm = sbgnrm;

@@ -153,6 +153,7 @@ SIGNATURES = {
     "mdft_mixture_destroy": (C.c_int, [C.c_void_p]),
     "mdft_mixture_energy_and_gradient": (C.c_int, [C.c_void_p, _DP, _DP, _DP, _DP]),
     "mdft_mixture_energy_and_gradient_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _DP, _DP]),
+    "mdft_mixture_minimize": (C.c_int, [C.c_void_p, _DP, C.POINTER(_MinOpts), C.POINTER(_MinRes)]),
 }
 
 
@@ -490,6 +491,15 @@ class Mixture:
         df = np.empty(self.shape) if want_grad else None
         _check(lib().mdft_mixture_energy_and_gradient(self.h, _p(x), _p(f), _p(df), _p(terms)))
         return float(f[0]), df, terms
+
+    def minimize(self, xi, m=5, pgtol=1e-6, ftol_abs=1e-3, itermax=1000, guni_tol=0.0):
+        """L-BFGS over every species' xi (FP64); returns (xi, result dict) like Engine.minimize."""
+        x = np.array(xi, dtype=np.float64, copy=True).reshape(self.shape)
+        o = _MinOpts(m, pgtol, ftol_abs, itermax, PREC_FP64, 0.0, 1, guni_tol)
+        r = _MinRes()
+        _check(lib().mdft_mixture_minimize(self.h, _p(x), C.byref(o), C.byref(r)))
+        return x, dict(f=r.f, pgnorm=r.pgnorm, iterations=r.iterations, evaluations=r.evaluations, status=r.status,
+                       guni=r.guni)
 
     def energy_and_gradient_device(self, xi_ptr: int, df_ptr: int | None):
         f = np.zeros(1)

@@ -1948,11 +1948,47 @@ static double amax_(long n, const double *a)
     return s;
 }
 
+/* The objective of a minimisation: F and its gradient at x (vectors of n). */
+typedef int (*objective_fn)(void *ctx, const double *x, double *f, double *g);
+
+static int lbfgs_core(objective_fn eval, void *ctx, long n, double *x, int m, double pgtol, double tol, int itermax,
+                      double *f_out, int *nfg_out, int *iter_out, int *status_out);
+
+static int single_objective(void *ctx, const double *x, double *f, double *g)
+{
+    return orc_energy_grad((orc *)ctx, x, f, g, NULL);
+}
+
 /* result: status 0=pgtol convergence, 1=f-reduction convergence, 2=abnormal line search, 3=itermax */
 int orc_minimize(orc *o, double *x, int m, double pgtol, double tol, int itermax, double *f_out, int *nfg_out,
                  int *iter_out, int *status_out)
 {
-    const long n = o->N * o->no;
+    return lbfgs_core(single_objective, o, o->N * o->no, x, m, pgtol, tol, itermax, f_out, nfg_out, iter_out, status_out);
+}
+
+typedef struct { orc *const *sp; int ns; const double *x; } mixture_ctx;
+
+static int mixture_objective(void *ctx, const double *x, double *f, double *g)
+{
+    const mixture_ctx *c = (const mixture_ctx *)ctx;
+    return orc_mixture_energy_grad(c->sp, c->ns, c->x, x, f, g, NULL);
+}
+
+/* The same L-BFGS over every species' xi at once, x = [ns][N][no] (energy_minimization's
+   vector of all species). */
+int orc_mixture_minimize(orc *const *sp, int ns, const double *xfrac, double *x, int m, double pgtol, double tol, int itermax,
+                         double *f_out, int *nfg_out, int *iter_out, int *status_out)
+{
+    mixture_ctx c = {sp, ns, xfrac};
+    return lbfgs_core(mixture_objective, &c, sp[0]->N * sp[0]->no * ns, x, m, pgtol, tol, itermax, f_out, nfg_out, iter_out,
+                      status_out);
+}
+
+/* L-BFGS-B without bounds: module_lbfgs_nocedal_mdft.f90:136-534 (mainlb), the compact
+   update of :1287-1318 and the line search of :1653-1959. */
+static int lbfgs_core(objective_fn eval, void *ctx, long n, double *x, int m, double pgtol, double tol, int itermax,
+                      double *f_out, int *nfg_out, int *iter_out, int *status_out)
+{
     double *g = malloc(sizeof(double) * n), *d = malloc(sizeof(double) * n), *t = malloc(sizeof(double) * n);
     double *r = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n);
     double *S = malloc(sizeof(double) * n * m), *Y = malloc(sizeof(double) * n * m);
@@ -1961,7 +1997,7 @@ int orc_minimize(orc *o, double *x, int m, double pgtol, double tol, int itermax
     const double ftol = (double)0.001f, gtol = (double)0.9f, xtol = (double)0.1f, big = 1.0 + 10;
     double f, fold = 0, theta = 1.0, stp = 0, gd = 0, gdold = 0, dtd, dnorm, stpmx;
     int col = 0, head = 0, itail = 0, iupdat = 0, iter = 0, nfgv = 0, status = 3;
-    if (orc_energy_grad(o, x, &f, g, NULL)) goto fail;
+    if (eval(ctx, x, &f, g)) goto fail;
     nfgv = 1;
     double sbgnrm = amax_(n, g);
     if (sbgnrm <= pgtol) { status = 0; goto done; }
@@ -2012,7 +2048,7 @@ int orc_minimize(orc *o, double *x, int m, double pgtol, double tol, int itermax
             if (iback >= 20) break;
             if (stp == 1.0) memcpy(x, z, sizeof(double) * n);
             else for (long i = 0; i < n; ++i) x[i] = stp * d[i] + t[i];
-            if (orc_energy_grad(o, x, &f, g, NULL)) goto fail;
+            if (eval(ctx, x, &f, g)) goto fail;
         }
         if (info != 0 || iback >= 20) {
             memcpy(x, t, sizeof(double) * n);

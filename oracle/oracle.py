@@ -66,6 +66,8 @@ def lib():
         L.orc_set_bridge_cgb.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_bridge_energy.argtypes = [C.c_void_p, dp, dp, dp]
         L.orc_set_bridge_fmt.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.orc_mixture_minimize.argtypes = [C.POINTER(C.c_void_p), C.c_int, dp, dp, C.c_int, C.c_double, C.c_double, C.c_int,
+                                           dp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_fmt_params.argtypes = [C.c_void_p, dp]
     return _LIB
 
@@ -266,3 +268,18 @@ def mixture_energy_grad(species, mole_fractions, xi, want_grad=True):
     if rc != 0:
         raise RuntimeError(lib().orc_last_error().decode())
     return float(f[0]), df, terms
+
+
+def mixture_minimize(species, mole_fractions, xi, m=5, pgtol=1e-6, tol=1e-3, itermax=1000):
+    """L-BFGS over every species' xi at once; returns (xi, f, evaluations, iterations, status)."""
+    ns = len(species)
+    shape = (ns,) + tuple(species[0].shape)
+    x = np.ascontiguousarray(xi, dtype=np.float64).reshape(shape).copy()
+    fr = np.ascontiguousarray(mole_fractions, dtype=np.float64)
+    hs = (C.c_void_p * ns)(*[o.h for o in species])
+    f = np.zeros(1); nfg = C.c_int(); it = C.c_int(); st = C.c_int()
+    rc = lib().orc_mixture_minimize(hs, ns, _p(fr), _p(x), m, pgtol, tol, itermax, _p(f), C.byref(nfg), C.byref(it),
+                                    C.byref(st))
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return x, float(f[0]), nfg.value, it.value, st.value

@@ -4,11 +4,13 @@ energy_cproj_mrso_mixture restatement, through the C-ABI.
 Tolerances as the single-species FP64 path: F <= 1e-10 relative, each term <= 1e-10 of
 |F|, gradient max|df_gpu - df_oracle| <= 1e-8 * max|df_oracle| over all species.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from mdft_b200 import Engine, Mixture, MdftError, PREC_MIXED, synth
+from mdft_b200 import Engine, Mixture, MdftError, PREC_MIXED, engine, synth
 import cases
 
 pytestmark = pytest.mark.gpu
@@ -100,4 +102,30 @@ def test_mixture_refusals(tmp_path):
     with pytest.raises(MdftError, match="FP64"):
         Mixture([engines[0], mixed], fr)
     for e in engines + [other, mixed]:
+        e.close()
+
+
+def test_mixture_minimize_trajectory_parity(tmp_path):
+    # the L-BFGS over both species' xi: the same trajectory as the oracle's for 25 iterations
+    c, oracles, engines, fr, _ = build(tmp_path, "walk5_16_m2")
+    x0 = np.stack([o.guess_density() for o in oracles])
+    xo, fo, nfo, ito, sto = O.mixture_minimize(oracles, fr, x0, m=5, pgtol=1e-12, tol=-1.0, itermax=25)
+    with Mixture(engines, fr) as mix:
+        xg, r = mix.minimize(x0, m=5, pgtol=1e-12, ftol_abs=-1.0, itermax=25)
+        assert (r["iterations"], r["evaluations"], r["status"]) == (ito, nfo, sto)
+        assert abs(r["f"] - fo) <= 1e-9 * abs(fo)
+        assert np.abs(xg - xo).max() <= 1e-6
+        # the result is a point of the mixture's functional
+        f1, _, _ = mix.energy_and_gradient(xg)
+        assert abs(f1 - r["f"]) <= 1e-12 * abs(f1)
+        # a mixed-precision minimisation is refused (the binding always asks for FP64)
+        o = engine._MinOpts(5, 1e-6, 1e-3, 5, PREC_MIXED, 0.0, 1, 0.0)
+        res = engine._MinRes()
+        x = np.ascontiguousarray(x0)
+        with pytest.raises(MdftError, match="FP64"):
+            engine._check(engine.lib().mdft_mixture_minimize(mix.h, engine._p(x), ctypes.byref(o), ctypes.byref(res)))
+    # species 0's handle minimises on its own afterwards
+    x1, r1 = engines[0].minimize(oracles[0].guess_density(), m=5, pgtol=1e-12, ftol_abs=-1.0, itermax=3)
+    assert r1["iterations"] == 3
+    for e in engines:
         e.close()
