@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--prof-grid", type=int, default=0,
                     help="with --evals: evaluations of a config-2-style cluster on this grid (0.375 A spacing) instead")
     ap.add_argument("--prof-mmax", type=int, default=5, help="with --prof-grid: the angular order")
+    ap.add_argument("--terms-compare", action="store_true",
+                    help="time one FP64 evaluation plain, with each bridge term and as a two-species mixture")
     ap.add_argument("--fft-compare", action="store_true",
                     help="timing comparison: the engine's FFT stages against cuFFT (torch.fft) on the same planes")
     return ap.parse_args()
@@ -319,6 +321,57 @@ def fft_compare(n, box, ck, sv, sol, rvdw, device):
     print(json.dumps(res))
 
 
+def terms_compare(n, box, ck, sv, sol, rvdw, device, evals=20):
+    """Device time of one FP64 evaluation (energy and gradient) of the bench workload at a
+    perturbed bulk density: plain, with bridge = cgb ('sla'), with bridge = hard_sphere (PY,
+    R = 1.4 A), and as a mixture of two species (x = 0.5 each) through mdft_mixture_*.
+    CUDA events on species 0's stream around `evals` evaluations after 3 untimed ones; each
+    evaluation ends with the host reading its sums, so the gaps between them are included."""
+    import torch
+    from mdft_b200 import Engine, Mixture, PREC_FP64
+
+    def timed(stream_ptr, fn):
+        st = torch.cuda.ExternalStream(stream_ptr)
+        for _ in range(3):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(evals):
+            fn()
+        b.record(st)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / evals
+
+    res = {"metric": "FP64 evaluation time with the optional terms", "unit": "ms per evaluation",
+           "workload": WORKLOAD % (N_GRID, BOX, MMAX, NSITE), "evaluations": evals}
+    e = Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0, device=device, precision=PREC_FP64)
+    e.compute_vext(sol, sv, rvdw=rvdw)
+    rng = np.random.default_rng(5)
+    xi_h = np.clip(1.0 + 0.1 * rng.standard_normal(e.shape), 0.0, None)
+    xi = torch.from_numpy(xi_h).to(device)
+    df = torch.empty_like(xi)
+    run = lambda: e.energy_and_gradient_device(xi.data_ptr(), df.data_ptr())
+    res["plain_ms"] = timed(e.stream, run)
+    e.set_bridge_cgb(1, B6=5.0, sigma=1.0, c00=-13.665)
+    res["cgb_sla_ms"] = timed(e.stream, run)
+    e.set_bridge_fmt(1, 1.4)
+    res["hard_sphere_py_ms"] = timed(e.stream, run)
+    e.set_bridge_fmt(0)
+    e.close()
+    sp = [Engine(n, box, MMAX, ck, temperature=sv.temperature, n0=sv.n0 * 0.5, device=device, precision=PREC_FP64)
+          for _ in range(2)]
+    for h in sp:
+        h.compute_vext(sol, sv, rvdw=rvdw)
+    xm = torch.cat([xi.reshape(-1), xi.reshape(-1)])
+    dm = torch.empty_like(xm)
+    with Mixture(sp, [0.5, 0.5]) as mix:
+        res["mixture_2_species_ms"] = timed(sp[0].stream, lambda: mix.energy_and_gradient_device(xm.data_ptr(), dm.data_ptr()))
+    for h in sp:
+        h.close()
+    print(json.dumps(res))
+
+
 def median(xs):
     return float(np.median(np.asarray(xs, dtype=np.float64)))
 
@@ -420,6 +473,9 @@ def main():
 
     if args.fft_compare:
         fft_compare(n, box, ck, sv, sols[0], rvdw, local)
+        return
+    if args.terms_compare:
+        terms_compare(n, box, ck, sv, sols[0], rvdw, local)
         return
 
     if args.evals and args.prof_grid:
