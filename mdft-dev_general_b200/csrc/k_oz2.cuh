@@ -137,7 +137,6 @@ struct Oz2Args {
     int mmax, np, ncoef, nq;
     double dq, twopi_lx, twopi_ly, twopi_lz;
     int quirks;  // FP64 path: FP32 rounding of the flushed entries and the gamma flush, as the reference
-    int accumulate;  // Mode 1: add the results to out instead of storing them
     int n_ints, n_dbls, nrot;
     int fwd_off, fwd_terms, oz_off, oz_terms, bwd_off, bwd_terms, sign, lvl_off, rec_int;
 };
@@ -155,23 +154,35 @@ template <typename C> __device__ __forceinline__ void cfmac(C &acc, C a, C b) { 
     acc.y += a.y * b.x - a.x * b.y;
 }
 
+// The source species of a multi-species step (Mode 1): their planes, in order.
+constexpr int kOzMaxSpecies = 8;
+struct OzMix {
+    const void *p[kOzMaxSpecies];
+    int ns;
+};
+
+// per warp: R, ceff and 6 np complex (8 np in Mode 1: the gamma accumulators)
 template <typename T>
-inline size_t oz2_smem_bytes(const Oz2Args &a, int W) {
-    const size_t per_warp = (size_t)(a.nrot + 1) + a.ncoef + 6 * a.np;
+inline size_t oz2_smem_bytes(const Oz2Args &a, int W, int mode = 0) {
+    const size_t per_warp = (size_t)(a.nrot + 1) + a.ncoef + (mode == 1 ? 8 : 6) * a.np;
     return ((a.n_ints * 4 + 15) / 16) * 16 + ((a.n_dbls * sizeof(T) + 15) / 16) * 16 + 32 +
            sizeof(typename Cplx<T>::t) * per_warp * W;
 }
 
 // smem: ints | coefficients (T) | flags[2W] | per warp: R[nrot+1], ceff[ncoef], dq, dmq, rq, rmq, gq, gmq
-// Mode 0: the single-species step, in place on planes (out unused).  Mode 1: the
-// multi-species step (src/module_energy_cproj_mrso_mixture.f90:491-721) of one (s, s2) pair:
-// reads species s's planes, stores (a.accumulate: adds) gamma_{s2} to out; at self-conjugate
-// points it keeps the q result (:685-709); with tables built with mix = true.
+// (Mode 1: and the accumulators aq, amq)
+// Mode 0: the single-species step, in place on planes (out and mi unused).  Mode 1: the
+// multi-species step (src/module_energy_cproj_mrso_mixture.f90:491-721) for one receiving
+// species s2 (c = ctab): gamma_{s2} = sum_s OZ(drho_s) over the source species' planes
+// mi.p[s], each source's gamma flushed as the reference does before the sum; R(q) and c are
+// formed once per pair and the sum is back-rotated once (the reference back-rotates each
+// source's gamma and then sums: the same up to rounding).  Stores gamma_{s2} to out; at
+// self-conjugate points it keeps the q result (:685-709); with tables built with mix = true.
 template <typename T, int Mode = 0>
 __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ planes,
                                              const typename Cplx<T>::t *__restrict__ ctab, const int *__restrict__ gints,
                                              const double *__restrict__ gdbls, Oz2Args a,
-                                             typename Cplx<T>::t *__restrict__ out) {
+                                             typename Cplx<T>::t *__restrict__ out, OzMix mi) {
     using C = typename Cplx<T>::t;
     extern __shared__ __align__(16) unsigned char oz2_smem[];
     const int W = blockDim.x >> 5;
@@ -181,26 +192,15 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
     unsigned char *flags = reinterpret_cast<unsigned char *>(sd) + ((a.n_dbls * sizeof(T) + 15) / 16) * 16;
     C *wbase = reinterpret_cast<C *>(flags + 32);
     const int np = a.np;
-    const int per_warp = (a.nrot + 1) + a.ncoef + 6 * np;
+    const int per_warp = (a.nrot + 1) + a.ncoef + (Mode == 1 ? 8 : 6) * np;
     for (int i = threadIdx.x; i < a.n_ints; i += blockDim.x) si[i] = gints[i];
     for (int i = threadIdx.x; i < a.n_dbls; i += blockDim.x) sd[i] = (T)gdbls[i];
     // persistent: the tables are staged once, then the CTA walks groups of W points
     for (long long k0 = (long long)blockIdx.x * W; k0 < a.nk; k0 += (long long)gridDim.x * W) {
-    __syncthreads();  // tables staged / the previous group's stores have read wbase
-    // coalesced load of the W points (side 0) and their partners (side 1)
-    for (int e = threadIdx.x; e < 2 * np * W; e += blockDim.x) {
-        const int side = e / (np * W), rem = e % (np * W), ip = rem / W, j = rem % W;
-        const long long kk = k0 + j;
-        if (kk >= a.nk) continue;
-        const int ix = (int)(kk % a.nx), iy = (int)((kk / a.nx) % a.ny), iz = (int)(kk / ((long long)a.nx * a.ny));
-        long long kidx;
-        if (side == 0) kidx = ((long long)iz * a.ny + iy) * a.nx + ix;
-        else kidx = ((long long)((a.nz - iz) % a.nz) * a.ny + (a.ny - iy) % a.ny) * a.nx + (a.nx - ix) % a.nx;
-        wbase[(size_t)j * per_warp + (a.nrot + 1) + a.ncoef + side * np + ip] = planes[(size_t)ip * a.N + kidx];
-    }
     C *Rw = wbase + (size_t)warp * per_warp;
     C *ceff = Rw + (a.nrot + 1);
     C *dq = ceff + a.ncoef, *dmq = dq + np, *rq = dmq + np, *rmq = rq + np, *gq = rmq + np, *gmq = gq + np;
+    C *aq = gmq + np, *amq = aq + np;  // Mode 1 only
     const long long kk = k0 + warp;
     bool active = kk < a.nk;
     int ix = 0, iy = 0, iz = 0, ixm = 0, iym = 0, izm = 0;
@@ -216,12 +216,28 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
     }
     const bool selfconj = active && (ix == ixm && iy == iym && iz == izm);
     const bool nyq = (2 * ix == a.nx) || (2 * iy == a.ny) || (2 * iz == a.nz);
-    if (lane == 0) {
+    const int nsrc = Mode == 1 ? mi.ns : 1;
+    for (int src = 0; src < nsrc; ++src) {
+    __syncthreads();  // tables staged / the previous group's stores (or source's products) have read wbase
+    // coalesced load of the W points (side 0) and their partners (side 1)
+    const C *pin = Mode == 1 ? static_cast<const C *>(mi.p[src]) : planes;
+    for (int e = threadIdx.x; e < 2 * np * W; e += blockDim.x) {
+        const int side = e / (np * W), rem = e % (np * W), ip = rem / W, j = rem % W;
+        const long long kk = k0 + j;
+        if (kk >= a.nk) continue;
+        const int ix = (int)(kk % a.nx), iy = (int)((kk / a.nx) % a.ny), iz = (int)(kk / ((long long)a.nx * a.ny));
+        long long kidx;
+        if (side == 0) kidx = ((long long)iz * a.ny + iy) * a.nx + ix;
+        else kidx = ((long long)((a.nz - iz) % a.nz) * a.ny + (a.ny - iy) % a.ny) * a.nx + (a.nx - ix) % a.nx;
+        wbase[(size_t)j * per_warp + (a.nrot + 1) + a.ncoef + side * np + ip] = pin[(size_t)ip * a.N + kidx];
+    }
+    if (src == 0 && lane == 0) {  // after the barrier above: the previous group's stores have read them
         flags[warp] = active ? 1 : 0;
         flags[W + warp] = selfconj ? 1 : 0;
     }
     __syncthreads();
     if (active) {
+      if (src == 0) {  // R(q) and c at |q| do not depend on the source species
         const double qx = (ix <= a.nx / 2 ? ix : ix - a.nx) * a.twopi_lx;
         const double qy = (iy <= a.ny / 2 ? iy : iy - a.ny) * a.twopi_ly;
         const double qz = (iz <= a.nz / 2 ? iz : iz - a.nz) * a.twopi_lz;
@@ -317,6 +333,7 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
             ceff[i] = v;
         }
         __syncwarp();
+      }
         const int *sign = si + a.sign;
         // forward rotation (:505-523)
         {
@@ -370,6 +387,23 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
             }
         }
         __syncwarp();
+        if (Mode == 1) {  // sum the flushed gamma of every source species
+            for (int o = lane; o < np; o += 32) {
+                if (src == 0) {
+                    aq[o] = gq[o];
+                    amq[o] = gmq[o];
+                } else {
+                    aq[o].x += gq[o].x; aq[o].y += gq[o].y;
+                    amq[o].x += gmq[o].x; amq[o].y += gmq[o].y;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    }  // source loop
+    if (active) {
+        const int *sign = si + a.sign;
+        const C *bq = Mode == 1 ? aq : gq, *bmq = Mode == 1 ? amq : gmq;
         // back rotation with conj(R) (:611-641); results replace dq / dmq
         {
             const int *off = si + a.bwd_off, *tm = si + a.bwd_terms;
@@ -378,8 +412,8 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
                 s.x = s.y = t.x = t.y = 0;
                 for (int k = off[o]; k < off[o + 1]; ++k) {
                     const int tt = tm[k], jp = tt & 255, r1i = (tt >> 8) & 2047, r2i = tt >> 19;
-                    cfmac(s, gq[jp], Rw[r1i]);
-                    cfmac(t, gmq[jp], Rw[r2i]);
+                    cfmac(s, bq[jp], Rw[r1i]);
+                    cfmac(t, bmq[jp], Rw[r2i]);
                 }
                 const T sg = (T)sign[o];
                 t.x *= sg;
@@ -402,16 +436,8 @@ __global__ void __launch_bounds__(256) k_oz2(typename Cplx<T>::t *__restrict__ p
         if (side == 0) kidx = ((long long)jz * a.ny + jy) * a.nx + jx;
         else kidx = ((long long)((a.nz - jz) % a.nz) * a.ny + (a.ny - jy) % a.ny) * a.nx + (a.nx - jx) % a.nx;
         const C v = wbase[(size_t)j * per_warp + (a.nrot + 1) + a.ncoef + side * np + ip];
-        if (Mode == 0) {
-            planes[(size_t)ip * a.N + kidx] = v;
-        } else if (a.accumulate) {
-            C o = out[(size_t)ip * a.N + kidx];
-            o.x += v.x;
-            o.y += v.y;
-            out[(size_t)ip * a.N + kidx] = o;
-        } else {
-            out[(size_t)ip * a.N + kidx] = v;
-        }
+        if (Mode == 0) planes[(size_t)ip * a.N + kidx] = v;
+        else out[(size_t)ip * a.N + kidx] = v;
     }
     }  // group loop
 }

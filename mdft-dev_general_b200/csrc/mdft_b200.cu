@@ -619,7 +619,7 @@ int run_pipeline_t(mdft_handle *h, const void *xin, double *d_df, int do_ideal, 
         launch_ozp(h, (float2 *)planes, (const float2 *)ctab, oz);
     else
         k_oz2<T><<<dbl ? h->oz_grid : h->oz_grid32, 32 * ozw, dbl ? h->oz_smem : h->oz_smem32, h->stream>>>(planes, ctab, h->oz_ints.p,
-                                                                                                           h->oz_dbls.p, oz, nullptr);
+                                                                                                           h->oz_dbls.p, oz, nullptr, OzMix{});
     if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
     stage_mark(h, 3);
     if ((rc = launch_fft_t<T>(h, planes, tw, -1))) return rc;

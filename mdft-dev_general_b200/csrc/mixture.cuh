@@ -9,9 +9,8 @@
 //   * species s, on its handle's stream: the S1 projection of rho0_s (xi_s^2 - 1) into the
 //     handle's planes and their forward FFT (src/module_energy_cproj_mrso_mixture.f90:283-344);
 //   * species s2, on its stream once every forward FFT is done:
-//     gamma_{s2} = sum_s OZ_{c(s2)}(drho_s) by nspec launches of k_oz2<double, 1> (the first
-//     stores, the others add, in the reference's order over s, :491-721), the inverse FFT of
-//     gamma_{s2} (:746-779), then the gather of species s2 with its ideal and external terms
+//     gamma_{s2} = sum_s OZ_{c(s2)}(drho_s) by one launch of k_oz2<double, 1> over every
+//     source species' planes (:491-721), the inverse FFT of gamma_{s2} (:746-779), then the gather of species s2 with its ideal and external terms
 //     and the excess prefactor times x_{s2} (:788-809,
 //     src/module_energy_ideal_and_external.f90:46-72).
 // The mixture owns the gamma planes (nspec x np x N complex) and the OZ term tables of the
@@ -27,7 +26,9 @@ struct mdft_mixture {
     DevBuf<double2> gam;  // [nspec][np][N]
     DevBuf<int> oz_ints;
     DevBuf<double> oz_dbls;
-    int oz_grid = 0;
+    int oz_grid = 0, oz_warps = 0;
+    size_t oz_smem = 0;
+    OzMix srcs{};  // every species' planes
     DevBuf<double> xi, df;  // staging of the host entry point and the minimiser's gradient, [nspec][N][no]
     std::vector<cudaEvent_t> ev_fwd, ev_done;  // per species: forward FFTs done, gather done
     cudaEvent_t ev_start = nullptr;            // species 0's stream: the point is ready
@@ -69,12 +70,9 @@ int mixture_launch(mdft_mixture *m, const double *d_xi, double *d_df, const doub
             if ((rc = check_cuda(cudaStreamWaitEvent(h->stream, m->ev_fwd[s], 0), "stream wait"))) return rc;
         Oz2Args oz = h->oz;  // this species' c table: nq, dq
         oz.quirks = 1;
-        for (int s = 0; s < ns; ++s) {
-            oz.accumulate = s > 0 ? 1 : 0;
-            k_oz2<double, 1><<<m->oz_grid, 32 * h->oz_warps, h->oz_smem, h->stream>>>(m->sp[s]->planes.p, h->ctab.p, m->oz_ints.p,
-                                                                                     m->oz_dbls.p, oz, gam);
-            if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
-        }
+        k_oz2<double, 1><<<m->oz_grid, 32 * m->oz_warps, m->oz_smem, h->stream>>>(nullptr, h->ctab.p, m->oz_ints.p, m->oz_dbls.p,
+                                                                                 oz, gam, m->srcs);
+        if ((rc = check_cuda(cudaGetLastError(), "oz launch"))) return rc;
         const void *tw[3] = {h->tw64[0].p, h->tw64[1].p, h->tw64[2].p};
         if ((rc = launch_fft_t<double>(h, gam, tw, -1))) return rc;
         const double *dv = dvec ? dvec + s2 * n : nullptr;
@@ -85,7 +83,7 @@ int mixture_launch(mdft_mixture *m, const double *d_xi, double *d_df, const doub
         if ((rc = check_cuda(cudaGetLastError(), "gather launch"))) return rc;
         k_reduce_sums<<<1, 256, 0, h->stream>>>(h->partial.p, rows, h->sums.p);
         if ((rc = check_cuda(cudaGetLastError(), "reduce launch"))) return rc;
-        h->launches += ns + 2;
+        h->launches += 3;
         if ((rc = check_cuda(cudaEventRecord(m->ev_done[s2], h->stream), "event record"))) return rc;
     }
     for (int s = 1; s < ns; ++s)
@@ -158,8 +156,9 @@ extern "C" {
 int mdft_mixture_create(mdft_handle *const *species, int nspec, const double *mole_fraction, mdft_mixture **out) {
     if (!species || !mole_fraction || !out) { set_error("null argument"); return MDFT_E_ARG; }
     *out = nullptr;
-    if (nspec < 2) {
-        set_error("a mixture needs at least two species (one species uses the handle itself)");
+    if (nspec < 2 || nspec > kOzMaxSpecies) {
+        set_error(nspec < 2 ? "a mixture needs at least two species (one species uses the handle itself)"
+                            : "a mixture takes at most %d species", kOzMaxSpecies);
         return MDFT_E_ARG;
     }
     const mdft_handle *h0 = species[0];
@@ -210,11 +209,18 @@ int mdft_mixture_create(mdft_handle *const *species, int nspec, const double *mo
     if ((rc = check_cuda(cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, m->device), "device attribute")))
         return rc;
     if ((rc = allow_smem((const void *)k_oz2<double, 1>, maxsmem))) return rc;
+    // warps per CTA: as many of 8 as fit with the two gamma accumulators per warp
+    m->oz_warps = 8;
+    while (m->oz_warps > 1 && oz2_smem_bytes<double>(h0->oz, m->oz_warps, 1) > (size_t)maxsmem) m->oz_warps /= 2;
+    m->oz_smem = oz2_smem_bytes<double>(h0->oz, m->oz_warps, 1);
+    if (m->oz_smem > (size_t)maxsmem) { set_error("multi-species OZ tile does not fit in shared memory"); return MDFT_E_ARG; }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oz2<double, 1>, 32 * h0->oz_warps, h0->oz_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oz2<double, 1>, 32 * m->oz_warps, m->oz_smem);
     const long long nk = (long long)g0.nx * g0.ny * (g0.nz / 2 + 1);
-    const long long groups = (nk + h0->oz_warps - 1) / h0->oz_warps;
+    const long long groups = (nk + m->oz_warps - 1) / m->oz_warps;
     m->oz_grid = (int)std::min<long long>(groups, (long long)std::max(1, per_sm) * h0->nsm);
+    m->srcs.ns = nspec;
+    for (int s = 0; s < nspec; ++s) m->srcs.p[s] = m->sp[s]->planes.p;
     m->ev_fwd.assign(nspec, nullptr);
     m->ev_done.assign(nspec, nullptr);
     auto drop_events = [&]() {
