@@ -8,7 +8,10 @@
  *   procedure pointer excess_energy(ff, df)    src/module_proc_ptrs.f90:3-21
  *
  * and the set-up and callers those need (vext, guess_density, the L-BFGS
- * loop of energy_minimization, pressure_correction).  A Fortran host binds
+ * loop of energy_minimization, pressure_correction), with the functionals
+ * beside the excess term on the same path: the bridges of energy_bridge
+ * (src/module_energy_and_gradient.f90:246-275) and the multi-species excess
+ * energy_cproj_mrso_mixture.  A Fortran host binds
  * these entry points with ISO_C_BINDING (one bind(C) interface per entry point,
  * with the structs below as bind(C) derived types).
  *
