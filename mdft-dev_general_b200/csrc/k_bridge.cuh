@@ -77,16 +77,22 @@ __global__ void k_cgb_cmul(double2 *__restrict__ p, const double2 *__restrict__ 
     }
 }
 
-// n(r) into dens and into the real part of plane (one thread per grid point)
+// n(r) into dens and into the real part of plane: one warp per grid point, the lanes
+// striding over its orientations (coalesced), summed by shuffles
 __global__ void __launch_bounds__(kBrThreads) k_cgb_density(const double *__restrict__ xi, const double *__restrict__ w, CgbArgs a,
                                                             double *__restrict__ dens, double2 *__restrict__ plane) {
-    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < a.N; r += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.N; r += nw) {
         const double *x = xi + r * a.no;
         double s = 0.0;
-        for (int io = 0; io < a.no; ++io) s += x[io] * x[io] * a.rho0 * w[io];
-        const double n = s / a.n0;
-        dens[r] = n;
-        plane[r] = make_double2(n, 0.0);
+        for (int io = lane; io < a.no; io += 32) s += x[io] * x[io] * a.rho0 * w[io];
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+        if (lane == 0) {
+            const double n = s / a.n0;
+            dens[r] = n;
+            plane[r] = make_double2(n, 0.0);
+        }
     }
 }
 
@@ -237,21 +243,27 @@ __device__ __forceinline__ void fmt_weights(double R, double k, double w[4]) {
     }
 }
 
-// planes 0, 1 <- rho, rho - shift; part[2 blk] = {sum rho, max |xi|}
+// planes 0, 1 <- rho, rho - shift; part[2 blk] = {sum rho, max |xi|}.  One warp per grid
+// point, the lanes striding over its orientations (coalesced), summed by shuffles.
 __global__ void __launch_bounds__(kBrThreads) k_fmt_density(const double *__restrict__ xi, const double *__restrict__ w, FmtArgs a,
                                                             double2 *__restrict__ pl, double *__restrict__ part) {
     __shared__ double sh[kBrThreads / 32];
     double srho = 0.0, mx = 0.0;
-    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < a.N; r += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < a.N; r += nw) {
         const double *x = xi + r * a.no;
         double s = 0.0;
-        for (int io = 0; io < a.no; ++io) {
+        for (int io = lane; io < a.no; io += 32) {
             s = s + x[io] * x[io] * w[io];
             mx = fmax(mx, fabs(x[io]));
         }
-        pl[r] = make_double2(s, 0.0);
-        pl[a.N + r] = make_double2(s - a.shift, 0.0);
-        srho += s;
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+        if (lane == 0) {
+            pl[r] = make_double2(s, 0.0);
+            pl[a.N + r] = make_double2(s - a.shift, 0.0);
+            srho += s;
+        }
     }
     const double t = block_sum(srho, sh);
     __syncthreads();
