@@ -317,11 +317,13 @@ int dcsrch(double f, double g, double &stp, double ftol, double gtol, double xto
     return LS_FG;
 }
 
-// Launch a batched FFT over `nplanes` planes starting at `data`.
+// Launch a batched FFT over `nplanes` planes starting at `data`: the specialised plane (xy)
+// and column (z) kernels of the evaluation pipeline where they exist for the grid's
+// lengths, the generic per-axis kernel otherwise.
 int launch_fft_planes(mdft_handle *h, double2 *data, int nplanes, int sign) {
     const Grid &g = h->g;
     const int dims[3] = {g.nx, g.ny, g.nz};
-    for (int ax = 0; ax < 3; ++ax) {
+    auto axis = [&](int ax) {
         FftAxisArgs a = h->fft[ax].args;
         a.nplanes = nplanes;
         a.sign = sign;
@@ -331,6 +333,25 @@ int launch_fft_planes(mdft_handle *h, double2 *data, int nplanes, int sign) {
         size_t smem = fft_smem_bytes<double>(dims[ax], a.TL);
         k_fft_axis<double><<<(unsigned)(nlines / a.TL), kFftThreads, smem, h->stream>>>(data, (const double2 *)h->fft[ax].tw, a);
         h->launches += 1;
+    };
+    bool xy_done = false;
+    if (g.nx == g.ny && sizeof(double2) * (size_t)g.nx * (g.nx + 2) <= 200 * 1024) {
+        const cudaError_t e = fft_xy<double>(g.nx, data, (long long)nplanes * g.nz, h->tw64[0].p, sign, h->stream, false,
+                                             h->xy_grid_cap64, h->kerr.p);
+        if (e == cudaSuccess) { xy_done = true; h->launches += 1; }
+        else if (e != cudaErrorNotSupported) return check_cuda(e, "fft xy launch");
+        else cudaGetLastError();
+    }
+    if (!xy_done) {
+        axis(0);
+        axis(1);
+    }
+    const cudaError_t e = fft_z<double>(g.nz, data, nplanes, g.nx, g.ny, h->tw64[2].p, sign, h->stream, false);
+    if (e == cudaSuccess) h->launches += 1;
+    else if (e != cudaErrorNotSupported) return check_cuda(e, "fft z launch");
+    else {
+        cudaGetLastError();
+        axis(2);
     }
     return check_cuda(cudaGetLastError(), "fft launch");
 }
