@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--prof-grid", type=int, default=0,
                     help="with --evals: evaluations of a config-2-style cluster on this grid (0.375 A spacing) instead")
     ap.add_argument("--prof-mmax", type=int, default=5, help="with --prof-grid: the angular order")
+    ap.add_argument("--prof-solve", action="store_true",
+                    help="with --prof-grid: full solves of the packed cluster (mixed and FP64 at the bench's stop "
+                         "rule, FP64 to max|df| <= 1e-6) and their dG")
     ap.add_argument("--terms-compare", action="store_true",
                     help="time one FP64 evaluation plain, with each bridge term and as a two-species mixture")
     ap.add_argument("--fft-compare", action="store_true",
@@ -476,6 +479,30 @@ def main():
         return
     if args.terms_compare:
         terms_compare(n, box, ck, sv, sols[0], rvdw, local)
+        return
+
+    if args.prof_solve and args.prof_grid:
+        # the packed cluster of the profiling mode, solved: the mixed form and plain FP64 at the
+        # bench's stop rule, and FP64 to max|df| <= 1e-6 as the reference dG
+        pn, pbox = args.prof_grid, 0.375 * args.prof_grid
+        rad = min(20.0, 0.4 * pbox)
+        cl = synth.packed_cluster_solute(max(20, int(540 * (rad / 20.0) ** 3)), seed=2026, radius=rad)
+        cl.xyz = synth.center_solute(cl.xyz, (pbox,) * 3)
+        ckp = ck_file(args.prof_mmax, kmax=15.0)
+        out = {"grid": pn, "box": pbox, "mmax": args.prof_mmax, "sites": len(cl.q)}
+        forms = (("mixed", PREC_MIXED, dict(pgtol=PGTOL, guni_tol=GUNI_TOL)),
+                 ("fp64", PREC_FP64, dict(pgtol=PGTOL, guni_tol=GUNI_TOL)),
+                 ("fp64_ref", PREC_FP64, dict(pgtol=PGTOL_REF, guni_tol=0.01)))
+        for name, prec, stop in forms:
+            eng = Engine(pn, pbox, args.prof_mmax, ckp, temperature=sv.temperature, n0=sv.n0, device=local, precision=prec)
+            t0 = time.time()
+            r = eng.solve(cl, sv, rvdw=min(RVDW, 0.45 * pbox), m=5, ftol_abs=-1.0, itermax=3000, precision=prec, **stop)
+            out[name] = {"dG": r["dG"], "evaluations": r["evaluations"], "status": r["status"], "pgnorm": r["pgnorm"],
+                         "guni": r["guni"], "seconds": time.time() - t0}
+            eng.close()
+        out["dG_error_mixed"] = abs(out["mixed"]["dG"] - out["fp64_ref"]["dG"])
+        out["dG_error_fp64"] = abs(out["fp64"]["dG"] - out["fp64_ref"]["dG"])
+        print(json.dumps(out))
         return
 
     if args.evals and args.prof_grid:
