@@ -124,4 +124,8 @@ def test_bridge_and_mixture_host_checks_without_gpu():
     assert b"at least two" in L.mdft_last_error()
     assert L.mdft_mixture_create(hs, 2, x, ctypes.byref(m)) == -1
     assert b"null species" in L.mdft_last_error()
+    hs9 = (ctypes.c_void_p * 9)(*([None] * 9))
+    x9 = (ctypes.c_double * 9)(*([1.0 / 9] * 9))
+    assert L.mdft_mixture_create(hs9, 9, x9, ctypes.byref(m)) == -1
+    assert b"at most 8" in L.mdft_last_error()
     assert L.mdft_mixture_destroy(None) == 0
