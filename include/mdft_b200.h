@@ -425,7 +425,7 @@ int mdft_bridge_energy(mdft_handle *h, const double *xi, double *fb, double *df)
  * src/module_energy_cproj_mrso_mixture.f90:67-850) with the ideal and external terms summed
  * over species (src/module_energy_ideal_and_external.f90:46-72).
  *
- * Each species is an FP64 handle on one grid, mmax, mrso, temperature and device, created
+ * Up to 8 species.  Each species is an FP64 handle on one grid, mmax, mrso, temperature and device, created
  * with that species' n0 already multiplied by its mole fraction (as the reference stores
  * it, src/module_solvent.f90:221-222) and its own c(k) file, with its vext set
  * (mdft_set_vext or mdft_compute_vext with its own sites).  mole_fraction[s] must lie in
